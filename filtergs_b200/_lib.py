@@ -1,0 +1,104 @@
+"""ctypes binding of libfiltergs_b200.so (the C ABI declared in include/filtergs_b200.h).
+
+The library is built in-tree by filtergs_b200/build.py.  There is no fallback:
+if the shared library is missing or does not load, every entry point raises.
+"""
+import ctypes as C
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libfiltergs_b200.so")
+
+FGS_OK = 0
+FGS_ERR_ARG = 1
+FGS_ERR_CUDA = 2
+FGS_ERR_TIMEOUT = 3
+FGS_ERR_PREFILTERED = 4
+FGS_ERR_CAPACITY = 5
+FGS_ERR_OVERFLOW = 6
+FGS_BACKWARD_REF_COMPAT = 0
+FGS_BACKWARD_CONSISTENT = 1
+FGS_STATS_SLOTS = 64
+
+vp = C.c_void_p
+i32 = C.c_int
+f32 = C.c_float
+i64 = C.c_longlong
+sz = C.c_size_t
+
+
+class RasterArgs(C.Structure):
+    """Mirror of struct fgs_raster_args."""
+    _fields_ = [
+        ("P", i32), ("D", i32), ("M", i32), ("width", i32), ("height", i32),
+        ("background", vp), ("means3D", vp), ("shs", vp), ("colors_precomp", vp), ("opacities", vp),
+        ("scales", vp), ("scale_modifier", f32), ("rotations", vp), ("cov3D_precomp", vp),
+        ("viewmatrix", vp), ("projmatrix", vp), ("campos", vp), ("tan_fovx", f32), ("tan_fovy", f32),
+        ("prefiltered", i32), ("use_filter", i32),
+        ("ogfs_epsilon_scale", f32), ("ogfs_epsilon_max", f32), ("ogfs_energy_floor", f32),
+        ("ogfs_radius_ratio_min", f32), ("ogfs_enable_stats", i32), ("filter3d_scale", f32),
+    ]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "fgs_status_string": (C.c_char_p, [i32]),
+    "fgs_version": (C.c_char_p, []),
+    "fgs_geom_bytes": (sz, [i32]),
+    "fgs_image_bytes": (sz, [i32, i32]),
+    "fgs_binning_bytes": (sz, [i64, i32]),
+    "fgs_forward_preprocess": (i32, [C.POINTER(RasterArgs), vp, vp, vp, C.POINTER(i64), vp]),
+    "fgs_forward_render": (i32, [C.POINTER(RasterArgs), vp, vp, vp, i64, vp, vp, vp, vp, vp, vp, i32, vp]),
+    "fgs_backward": (i32, [C.POINTER(RasterArgs), vp, vp, vp, i64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                           i32, vp]),
+    "fgs_check": (i32, [vp, vp]),
+    "fgs_mark_visible": (i32, [i32, vp, vp, vp, vp, vp]),
+    "fgs_compute_radius": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, f32, f32, vp, vp]),
+    "fgs_compute_radius_v2": (i32, [i32, vp, vp, vp, vp, vp, f32, f32, f32, f32, vp, vp]),
+    "fgs_visibility_radius": (i32, [i32, vp, vp, vp, vp, vp, vp, vp, i32, f32, f32, f32, f32, f32, f32, f32,
+                                    vp, vp, vp, vp]),
+    "fgs_sorted_pairs": (i32, [vp, vp, i32, i64, vp, vp, vp]),
+    "fgs_preprocess_outputs": (i32, [vp, i32, vp, vp, vp, vp, vp, vp]),
+    "fgs_image_outputs": (i32, [vp, i32, i32, vp, vp, vp, vp]),
+}
+
+_lib = None
+
+
+class FgsError(RuntimeError):
+    def __init__(self, status, where):
+        self.status = status
+        text = status_string(status) if _lib is not None else str(status)
+        super().__init__(f"{where}: {text} (status {status})")
+
+
+def lib():
+    """Load the shared library once; raise loudly when it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"filtergs_b200 CUDA library not built: {LIB_PATH} is missing "
+                               "(run `python -m filtergs_b200.build`)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def status_string(status):
+    return lib().fgs_status_string(int(status)).decode()
+
+
+def check(status, where):
+    if status != FGS_OK:
+        raise FgsError(status, where)
+
+
+def call(name, *args):
+    """Call an int-returning entry point and raise FgsError on failure."""
+    st = getattr(lib(), name)(*args)
+    check(st, name)
+    return st

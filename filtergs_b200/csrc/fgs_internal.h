@@ -1,0 +1,108 @@
+// Internal host-side declarations shared by the .cu translation units.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/filtergs_b200.h"
+
+namespace fgs {
+
+struct PairRecord;
+
+// Per-call forward parameters after validation (device pointers).
+struct PreParams {
+    int P, D, M, W, H;
+    const float* means;       // [P,3]
+    const float* scales;      // [P,3] or null
+    const float* rots;        // [P,4] or null
+    const float* opac;        // [P]
+    const float* shs;         // [P,M,3] or null
+    const float* cov3D;       // [P,6] or null (precomputed)
+    const float* colors;      // [P,3] or null (precomputed)
+    const float* view;        // [16]
+    const float* proj;        // [16]
+    const float* campos;      // [3]
+    float scale_mod, tanx, tany, fx, fy;
+    int prefiltered, use_filter;
+    float eps_scale, eps_max, energy_floor, ratio_min;
+    float filter3d;
+    int aligned;              // means/scales/rots/opac 16-byte aligned: stage with float4 loads
+};
+
+// Geometry workspace views (per-Gaussian state kept from forward to backward).
+struct GeomState {
+    PairRecord* grec;          // [P] render record per Gaussian
+    int* radii;                // [P] internal radii (when the caller passes none)
+    uint32_t* tiles;           // [P] tiles touched
+    uint8_t* clamped;          // [P] SH clamp bits
+    uint32_t* depth_key;       // [P] depth bits (0xffffffff = culled)
+    uint32_t* sort_ids_a;      // [P] depth-sorted ids (ping)
+    uint32_t* sort_ids_b;      // [P] (pong)
+    uint32_t* sort_keys_b;     // [P]
+    uint32_t* hist;            // [8][256] radix histograms: 4 depth passes + up to 4 tile passes
+    uint32_t* status;          // lookback status words, depth passes
+    uint32_t* counters;        // [16] chunk counters / misc
+    unsigned long long* total; // [4]: 0 = K (pairs), 1 = V (visible count)
+    unsigned int* err;         // error bit set
+    size_t status_words;
+};
+GeomState geom_views(void* base, int P);
+size_t geom_bytes(int P);
+
+struct ImageState {
+    float* final_T;     // [N]
+    uint32_t* n_contrib; // [N]
+    uint2* ranges;      // [tiles]
+};
+ImageState image_views(void* base, int W, int H);
+size_t image_bytes(int W, int H);
+
+struct BinState {
+    uint32_t* tile_a;   // [K]
+    uint32_t* tile_b;   // [K]
+    uint32_t* val_a;    // [K]
+    uint32_t* val_b;    // [K] final point list
+    PairRecord* rec;    // [K]
+    uint32_t* status;   // lookback words, tile passes
+    uint32_t* scan_status; // lookback words of the fused scan
+    float* kv_sum;      // [K] (stats)
+    uint32_t* kv_cnt;   // [K] (stats)
+    size_t status_words, scan_words;
+};
+BinState bin_views(void* base, long long K, int P);
+size_t bin_bytes(long long K, int P);
+
+// ---------------------------------------------------------------- launchers
+void launch_preprocess(const PreParams& p, const GeomState& g, int* radii, cudaStream_t s);
+void launch_depth_sort(const GeomState& g, int P, cudaStream_t s);
+void launch_duplicate(const GeomState& g, const BinState& b, uint32_t V, uint32_t K, int W, int H, int tile_bits,
+                      cudaStream_t s);
+int sort_chunk_size();
+void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int tile_bits, cudaStream_t s);
+void launch_ranges(const BinState& b, const ImageState& im, long long K, int num_tiles, cudaStream_t s);
+void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, const float* bg, float* out_color,
+                       int* point_id, float* pw_pixel, float* point_weight, bool stats, unsigned* err,
+                       cudaStream_t s);
+void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, const float* bg,
+                       const float* dL_dpix, float* dmean2D, float* dconic, float* dopac, float* dcolor,
+                       int consistent, unsigned* err, cudaStream_t s);
+void launch_preprocess_bwd(const PreParams& p, const int* radii, const GeomState& g, const float* dmean2D,
+                           const float* dconic, const float* dcolor, float* dopac, float* dmean3D,
+                           float* dcov3D, float* dsh, float* dscale, float* drot, int consistent,
+                           cudaStream_t s);
+void launch_kpc_stats(const BinState& b, const ImageState& im, int num_tiles, float used_thresh, double* dev_out,
+                      cudaStream_t s);
+
+// radius / visibility helpers
+void launch_compute_radius(int variant, int P, const float* means, const float* scales, const float* rots,
+                           const float* view, const float* proj, float fx, float fy, float tanx, float tany,
+                           float* radius, cudaStream_t s);
+void launch_mark_visible(int P, const float* means, const float* view, uint8_t* present, cudaStream_t s);
+void launch_visibility_radius(int P, const float* means, const float* lscales, const float* rots,
+                              const float* proj, const float* view, const int32_t* node_index,
+                              const int32_t* ancestors, int L, float fx, float fy, float tanx, float tany,
+                              float padding, float radius_max, float radius_filter, uint8_t* mask, float* radius2d,
+                              float* depth, cudaStream_t s);
+
+}  // namespace fgs

@@ -1,0 +1,366 @@
+// Per-Gaussian forward preprocess and the radius / visibility kernels.
+//
+// preprocess: antialias/cuda_rasterizer/forward.cu:266-401 (EWA projection,
+// 2D dilation, OGFS opacity-aware radius, tile rectangle, SH degree<=3
+// colour), plus the optional 3D filter.  Each 256-thread block stages its
+// slice of the AoS parameter arrays through shared memory with coalesced
+// float4 loads, then every thread works on one Gaussian in registers.  The
+// kernel writes a 48-byte render record per Gaussian, the depth sort key,
+// and accumulates the pair count K and visible count V on the device.
+#include "fgs_common.cuh"
+#include "fgs_internal.h"
+
+namespace fgs {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// Copy rows [row0, row0+rows) of an NF-float-per-row array into shared memory.
+template <int NF>
+__device__ __forceinline__ void stage_rows(const float* __restrict__ g, int row0, int rows, float* s, bool vec)
+{
+    const float* src = g + (size_t)row0 * NF;
+    const int nf = rows * NF;
+    if (vec) {
+        const int nv = nf >> 2;
+        const float4* s4 = reinterpret_cast<const float4*>(src);
+        float4* d4 = reinterpret_cast<float4*>(s);
+        for (int v = threadIdx.x; v < nv; v += kThreads) d4[v] = __ldg(s4 + v);
+        for (int f = (nv << 2) + threadIdx.x; f < nf; f += kThreads) s[f] = __ldg(src + f);
+    } else {
+        for (int f = threadIdx.x; f < nf; f += kThreads) s[f] = __ldg(src + f);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomState g, int* __restrict__ radii_out)
+{
+    __shared__ __align__(16) float s_mean[kThreads * 3];
+    __shared__ __align__(16) float s_scale[kThreads * 3];
+    __shared__ __align__(16) float s_rot[kThreads * 4];
+    __shared__ __align__(16) float s_opac[kThreads];
+    __shared__ unsigned long long s_sum[2];
+
+    const int row0 = blockIdx.x * kThreads;
+    const int rows = min(kThreads, p.P - row0);
+    const bool vec = p.aligned != 0;
+    stage_rows<3>(p.means, row0, rows, s_mean, vec);
+    stage_rows<1>(p.opac, row0, rows, s_opac, vec);
+    if (p.scales) stage_rows<3>(p.scales, row0, rows, s_scale, vec);
+    if (p.rots) stage_rows<4>(p.rots, row0, rows, s_rot, vec);
+    if (threadIdx.x < 2) s_sum[threadIdx.x] = 0;
+    __syncthreads();
+
+    const int t = threadIdx.x;
+    const int idx = row0 + t;
+    uint32_t tiles = 0;
+    if (idx < p.P) {
+        int radius_px = 0;
+        uint32_t key = 0xffffffffu;
+        uint8_t clamp_bits = 0;
+        PairRecord rec;
+        rec.a = make_float4(0.f, 0.f, 0.f, 0.f);
+        rec.b = rec.a;
+        rec.c = make_float4(0.f, __int_as_float(idx), 0.f, 0.f);
+        const float3 p_orig = {s_mean[3 * t], s_mean[3 * t + 1], s_mean[3 * t + 2]};
+        // auxiliary.h:139-164 (near plane at view z = 0.2)
+        const float4 p_hom = xform_point4x4(p_orig, p.proj);
+        const float p_w = 1.0f / (p_hom.w + 0.0000001f);
+        const float3 p_proj = {p_hom.x * p_w, p_hom.y * p_w, p_hom.z * p_w};
+        const float3 p_view = xform_point4x3(p_orig, p.view);
+        bool live = true;
+        if (p_view.z <= 0.2f) {
+            live = false;
+            if (p.prefiltered) set_error(g.err, FGS_ERR_PREFILTERED);
+        }
+        float cov3D[6];
+        if (live) {
+            if (p.cov3D) {
+#pragma unroll
+                for (int k = 0; k < 6; k++) cov3D[k] = __ldg(p.cov3D + (size_t)idx * 6 + k);
+            } else {
+                const float4 q = {s_rot[4 * t], s_rot[4 * t + 1], s_rot[4 * t + 2], s_rot[4 * t + 3]};
+                cov3d_from_scale_rot(s_scale[3 * t], s_scale[3 * t + 1], s_scale[3 * t + 2], p.scale_mod, q, cov3D);
+            }
+            if (p.filter3d > 0.f) {
+                // 3D filter: isotropic variance of a sigma = s * z / focal blur.
+                const float sf = p.filter3d * p_view.z / p.fx;
+                const float v = sf * sf;
+                cov3D[0] += v; cov3D[3] += v; cov3D[5] += v;
+            }
+            float3 cov = ewa_cov2d(p_orig, p.fx, p.fy, p.tanx, p.tany, cov3D, p.view);
+            if (p.use_filter) {
+                cov.x = dilate_max(cov.x);
+                cov.z = dilate_max(cov.z);
+            }
+            const float det = (cov.x * cov.z - cov.y * cov.y);
+            if (det == 0.0f) live = false;
+            if (live) {
+                const float det_inv = 1.f / det;
+                const float3 conic = {cov.z * det_inv, -cov.y * det_inv, cov.x * det_inv};
+                // forward.cu:345-369: OGFS radius
+                const float opacity = fmaxf(s_opac[t], 1e-6f);
+                const float epsilon_pix = 1.0f / 255.0f;
+                const float eps_base = fmaxf(0.0f, 1.0f - epsilon_pix);
+                const float lambda_G_raw = 1.0f - powf(eps_base, static_cast<float>(kOgfsBlockArea));
+                float lambda_G = epsilon_pix + p.eps_scale * (lambda_G_raw - epsilon_pix);
+                lambda_G = fminf(fmaxf(lambda_G, epsilon_pix), p.eps_max);
+                const float log_lambda_G = logf(lambda_G);
+                const float log_opacity = logf(opacity);
+                const float radius_energy = log_opacity - log_lambda_G;
+                const float energy_clamped = fmaxf(radius_energy, p.energy_floor);
+                const float mid = 0.5f * (cov.x + cov.z);
+                const float disc = fmaxf(0.0f, mid * mid - det);
+                const float sqrt_disc = sqrtf(disc);
+                const float lambda1 = mid + sqrt_disc;
+                const float lambda2 = mid - sqrt_disc;
+                const float max_lambda = fmaxf(fmaxf(lambda1, lambda2), 1e-6f);
+                const float radius_base = 3.0f * sqrtf(max_lambda);
+                float radius_major = sqrtf(2.0f * energy_clamped * max_lambda);
+                radius_major = fminf(radius_major, radius_base);
+                radius_major = fmaxf(radius_major, p.ratio_min * radius_base);
+                const float radius_f = radius_major + 1.0f;
+                const int rpx = max(1, static_cast<int>(ceilf(radius_f)));
+                const float px = ndc_to_pix(p_proj.x, p.W), py = ndc_to_pix(p_proj.y, p.H);
+                const int gx = (p.W + kTileX - 1) / kTileX, gy = (p.H + kTileY - 1) / kTileY;
+                int x0, y0, x1, y1;
+                tile_rect(px, py, rpx, gx, gy, kTileX, kTileY, x0, y0, x1, y1);
+                const int extent = (x1 - x0) * (y1 - y0);
+                if (extent != 0) {
+                    float3 rgb;
+                    if (p.colors) {
+                        rgb = {__ldg(p.colors + 3 * (size_t)idx), __ldg(p.colors + 3 * (size_t)idx + 1),
+                               __ldg(p.colors + 3 * (size_t)idx + 2)};
+                    } else {
+                        // SH row: 12 float4 loads when the row is 16-byte aligned.
+                        float sh[48];
+                        const int nf = p.M * 3;
+                        const float* row = p.shs + (size_t)idx * nf;
+                        const int ncoef = (p.D + 1) * (p.D + 1);
+                        const int need = min(nf, ncoef * 3);
+                        if (vec && (nf & 3) == 0) {
+                            const float4* r4 = reinterpret_cast<const float4*>(row);
+#pragma unroll
+                            for (int v = 0; v < 12; v++)
+                                if (4 * v < need) {
+                                    const float4 q = __ldg(r4 + v);
+                                    sh[4 * v] = q.x; sh[4 * v + 1] = q.y; sh[4 * v + 2] = q.z; sh[4 * v + 3] = q.w;
+                                }
+                        } else {
+#pragma unroll
+                            for (int f = 0; f < 48; f++)
+                                if (f < need) sh[f] = __ldg(row + f);
+                        }
+                        const float3 cam = {__ldg(p.campos), __ldg(p.campos + 1), __ldg(p.campos + 2)};
+                        rgb = sh_to_rgb(p.D, sh, p_orig, cam, clamp_bits);
+                    }
+                    radius_px = rpx;
+                    tiles = (uint32_t)extent;
+                    key = __float_as_uint(p_view.z);
+                    rec.a = make_float4(px, py, conic.x, conic.y);
+                    rec.b = make_float4(conic.z, opacity, rgb.x, rgb.y);
+                    rec.c = make_float4(rgb.z, __int_as_float(idx), p_view.z, 0.f);
+                }
+            }
+        }
+        g.grec[idx] = rec;
+        g.tiles[idx] = tiles;
+        g.depth_key[idx] = key;
+        g.clamped[idx] = clamp_bits;
+        g.radii[idx] = radius_px;
+        if (radii_out) radii_out[idx] = radius_px;
+    }
+    // K (pairs) and V (visible) totals: warp reduce, then one shared atomic per warp.
+    unsigned long long k = tiles;
+    unsigned v = tiles ? 1u : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        k += __shfl_xor_sync(0xffffffffu, k, o);
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&s_sum[0], k);
+        atomicAdd(&s_sum[1], (unsigned long long)v);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_sum[0]) atomicAdd(&g.total[0], s_sum[0]);
+        if (s_sum[1]) atomicAdd(&g.total[1], s_sum[1]);
+    }
+}
+
+// forward.cu:187-263 (variant 0) and compute_radius_kernel_v2.cu:180-229 (variant 1)
+__global__ void compute_radius_kernel(int variant, int P, const float* __restrict__ means,
+                                      const float* __restrict__ scales, const float* __restrict__ rots,
+                                      const float* __restrict__ view, const float* __restrict__ proj, float fx,
+                                      float fy, float tanx, float tany, float* __restrict__ radius)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= P) return;
+    radius[idx] = 0;
+    const float3 p_orig = {means[3 * idx], means[3 * idx + 1], means[3 * idx + 2]};
+    const float4 p_hom = xform_point4x4(p_orig, proj);
+    const float p_w = 1.0f / (p_hom.w + 0.0000001f);
+    const float3 p_proj = {p_hom.x * p_w, p_hom.y * p_w, p_hom.z * p_w};
+    if (variant == 0) {
+        const float3 p_view = xform_point4x3(p_orig, view);
+        if (p_view.z <= 0.2f) return;
+    }
+    if (p_proj.x < -1.3 || p_proj.x > 1.3 || p_proj.y < -1.3 || p_proj.y > 1.3) return;
+    float cov3D[6];
+    const float4 q = {rots[4 * idx], rots[4 * idx + 1], rots[4 * idx + 2], rots[4 * idx + 3]};
+    cov3d_from_scale_rot(scales[3 * idx], scales[3 * idx + 1], scales[3 * idx + 2], 1.f, q, cov3D);
+    float3 cov = ewa_cov2d(p_orig, fx, fy, tanx, tany, cov3D, view);
+    if (variant == 1) {
+        cov.x = dilate_max(cov.x);
+        cov.z = dilate_max(cov.z);
+    }
+    const float det = (cov.x * cov.z - cov.y * cov.y);
+    if (det == 0.0f) return;
+    const float mid = 0.5f * (cov.x + cov.z);
+    const float lambda1 = mid + sqrtf(fmaxf(0.1f, mid * mid - det));
+    const float lambda2 = mid - sqrtf(fmaxf(0.1f, mid * mid - det));
+    radius[idx] = 3.f * sqrtf(fmaxf(lambda1, lambda2));
+}
+
+// rasterizer_impl.cu:97-109
+__global__ void mark_visible_kernel(int P, const float* __restrict__ means, const float* __restrict__ view,
+                                    uint8_t* __restrict__ present)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= P) return;
+    const float3 p = {means[3 * idx], means[3 * idx + 1], means[3 * idx + 2]};
+    present[idx] = xform_point4x3(p, view).z > 0.2f;
+}
+
+// compute_radius_kernel_v2.cu:109-169
+__device__ __forceinline__ bool vis_radius_point(int idx, const float* __restrict__ means,
+                                                 const float* __restrict__ lscales, const float* __restrict__ rots,
+                                                 const float* __restrict__ proj, const float* __restrict__ view,
+                                                 float fx, float fy, float tanx, float tany, float padding,
+                                                 float& depth_out, float& radius_out)
+{
+    const float3 p_orig = {means[3 * idx], means[3 * idx + 1], means[3 * idx + 2]};
+    const float4 p_hom = xform_point4x4(p_orig, proj);
+    const float p_w = 1.0f / (p_hom.w + 0.0000001f);
+    const float3 p_proj = {p_hom.x * p_w, p_hom.y * p_w, p_hom.z * p_w};
+    depth_out = p_proj.z;
+    const bool visible = (p_proj.z > 0.0f) && (p_proj.z < 1.0f) && (p_proj.x > -1.0f - padding) &&
+                         (p_proj.x < 1.0f + padding) && (p_proj.y > -1.0f - padding) && (p_proj.y < 1.0f + padding);
+    if (!visible) {
+        radius_out = 0.0f;
+        return false;
+    }
+    const float sx = expf(lscales[3 * idx]), sy = expf(lscales[3 * idx + 1]), sz = expf(lscales[3 * idx + 2]);
+    float4 q = {rots[4 * idx], rots[4 * idx + 1], rots[4 * idx + 2], rots[4 * idx + 3]};
+    const float rn = sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    if (rn > 0.f) {
+        q.x = q.x / rn; q.y = q.y / rn; q.z = q.z / rn; q.w = q.w / rn;
+    } else {
+        q = {1.f, 0.f, 0.f, 0.f};
+    }
+    float cov3D[6];
+    cov3d_from_scale_rot(sx, sy, sz, 1.f, q, cov3D);
+    float3 cov = ewa_cov2d(p_orig, fx, fy, tanx, tany, cov3D, view);
+    cov.x = dilate_max(cov.x);
+    cov.z = dilate_max(cov.z);
+    const float det = (cov.x * cov.z - cov.y * cov.y);
+    if (det <= 0.0f) {
+        radius_out = 0.0f;
+        return true;
+    }
+    const float mid = 0.5f * (cov.x + cov.z);
+    const float disc = fmaxf(0.1f, mid * mid - det);
+    const float root = sqrtf(disc);
+    const float lambda1 = mid + root;
+    const float lambda2 = mid - root;
+    radius_out = 3.f * sqrtf(fmaxf(lambda1, lambda2));
+    return true;
+}
+
+// Phase 1 of compute_radius_kernel_v2.cu:231-353: every node's visibility,
+// radius and NDC depth.  Each node's radius is a pure function of the node,
+// so computing all of them first and applying the tree rule in phase 2 gives
+// the same mask as the reference's lazily computed ancestor radii.
+__global__ void visibility_phase1(int P, const float* __restrict__ means, const float* __restrict__ lscales,
+                                  const float* __restrict__ rots, const float* __restrict__ proj,
+                                  const float* __restrict__ view, float fx, float fy, float tanx, float tany,
+                                  float padding, uint8_t* __restrict__ mask, float* __restrict__ radius2d,
+                                  float* __restrict__ depth)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= P) return;
+    float r = 0.f, d = 0.f;
+    const bool vis = vis_radius_point(idx, means, lscales, rots, proj, view, fx, fy, tanx, tany, padding, d, r);
+    depth[idx] = d;
+    radius2d[idx] = r;
+    mask[idx] = vis ? 1 : 0;  // phase 2 turns this into the keep decision
+}
+
+// Phase 2: the LoD keep rule (compute_radius_kernel_v2.cu:281-352).
+__global__ void visibility_phase2(int P, const int32_t* __restrict__ node_index, const int32_t* __restrict__ anc,
+                                  int L, float radius_max, float radius_filter, uint8_t* __restrict__ mask,
+                                  const float* __restrict__ radius2d)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= P) return;
+    if (!mask[idx]) return;
+    const float r = radius2d[idx];
+    bool keep = true;
+    if (node_index[idx] != -1) {
+        keep = r <= radius_max;
+    } else {
+        const int32_t* row = anc + (size_t)idx * L;
+        for (int l = 0; l < L; ++l) {
+            const int32_t a = __ldg(row + l);
+            if (a < 0) break;
+            if (a == idx || a >= P) continue;  // (an id past the node table is not a node)
+            if (__ldg(node_index + a) == -1) continue;
+            const float ar = radius2d[a];
+            if (ar > 0.f && ar <= radius_max) {
+                keep = false;
+                break;
+            }
+        }
+    }
+    if (keep && radius_filter > 0.0f && r > radius_filter) keep = false;
+    mask[idx] = keep ? 1 : 0;
+}
+
+}  // namespace
+
+void launch_preprocess(const PreParams& p, const GeomState& g, int* radii, cudaStream_t s)
+{
+    if (p.P <= 0) return;
+    preprocess_kernel<<<(p.P + kThreads - 1) / kThreads, kThreads, 0, s>>>(p, g, radii);
+}
+
+void launch_compute_radius(int variant, int P, const float* means, const float* scales, const float* rots,
+                           const float* view, const float* proj, float fx, float fy, float tanx, float tany,
+                           float* radius, cudaStream_t s)
+{
+    if (P <= 0) return;
+    compute_radius_kernel<<<(P + 255) / 256, 256, 0, s>>>(variant, P, means, scales, rots, view, proj, fx, fy,
+                                                           tanx, tany, radius);
+}
+
+void launch_mark_visible(int P, const float* means, const float* view, uint8_t* present, cudaStream_t s)
+{
+    if (P <= 0) return;
+    mark_visible_kernel<<<(P + 255) / 256, 256, 0, s>>>(P, means, view, present);
+}
+
+void launch_visibility_radius(int P, const float* means, const float* lscales, const float* rots,
+                              const float* proj, const float* view, const int32_t* node_index,
+                              const int32_t* ancestors, int L, float fx, float fy, float tanx, float tany,
+                              float padding, float radius_max, float radius_filter, uint8_t* mask, float* radius2d,
+                              float* depth, cudaStream_t s)
+{
+    if (P <= 0) return;
+    visibility_phase1<<<(P + 255) / 256, 256, 0, s>>>(P, means, lscales, rots, proj, view, fx, fy, tanx, tany,
+                                                       padding, mask, radius2d, depth);
+    visibility_phase2<<<(P + 255) / 256, 256, 0, s>>>(P, node_index, ancestors, L, radius_max, radius_filter,
+                                                       mask, radius2d);
+}
+
+}  // namespace fgs

@@ -1,0 +1,457 @@
+// Tile compositing, forward and backward
+// (antialias/cuda_rasterizer/forward.cu:406-567, backward.cu:399-557).
+//
+// One CTA per 16x16 tile.  The tile's sorted pairs are contiguous 48-byte
+// records (written by the last sort pass), so each 256-record batch is ONE
+// bulk copy (cp.async.bulk, the TMA engine's 1-D form) into shared memory,
+// completed on an mbarrier.  Three record buffers keep two batches in flight
+// while the current one is composited.  A thread owns PPT pixels of one
+// column (16 x 2*PPT pixels per warp); a warp whose pixels have all
+// saturated (T < 1e-4) stops evaluating and only joins the per-batch barrier.
+//
+// Per-Gaussian outputs that the reference updates from every pixel (the
+// racy out_point_weight max, the KPC statistics, the backward's 9 gradient
+// atomics) are reduced across the warp first, then across the CTA in shared
+// memory, and leave the CTA once per (tile, pair).
+#include "fgs_common.cuh"
+#include "fgs_internal.h"
+
+namespace fgs {
+
+namespace {
+
+constexpr int kBatch = 256;
+constexpr int kBufs = 3;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false (and an error bit) if the copy never lands.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned* err)
+{
+    long long spins = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++spins > kSpinLimit) {
+            set_error(err, FGS_ERR_TIMEOUT);
+            return false;
+        }
+    }
+    return true;
+}
+// 1-D bulk copy global -> shared, completion counted on `bar`.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Issue the bulk copy of records [first, first+count) into buffer `buf`.
+__device__ __forceinline__ void issue_batch(PairRecord* sbuf, uint64_t* bar, const PairRecord* recs, uint32_t first,
+                                            uint32_t count)
+{
+    const uint32_t bytes = count * (uint32_t)sizeof(PairRecord);
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(sbuf, recs + first, bytes, bar);
+}
+
+__device__ __forceinline__ float warp_sum(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ---------------------------------------------------------------- forward
+template <int PPT>
+__global__ void __launch_bounds__(256 / PPT)
+    render_fwd_kernel(const uint2* __restrict__ ranges, const PairRecord* __restrict__ recs, int W, int H,
+                      const float* __restrict__ bg, float* __restrict__ out_color, float* __restrict__ final_T,
+                      uint32_t* __restrict__ n_contrib, int* __restrict__ out_point_id,
+                      float* __restrict__ out_pw_pixel, float* __restrict__ out_point_weight,
+                      float* __restrict__ kv_sum, uint32_t* __restrict__ kv_cnt, unsigned* err)
+{
+    constexpr int NT = 256 / PPT;
+    __shared__ __align__(128) PairRecord s_rec[kBufs][kBatch];
+    __shared__ __align__(8) uint64_t s_bar[kBufs];
+    __shared__ uint32_t s_wmax[2][kBatch];
+    __shared__ float s_ksum[2][kBatch];
+    __shared__ uint32_t s_kcnt[2][kBatch];
+
+    const int tid = threadIdx.x;
+    const int gx = (W + kTileX - 1) / kTileX;
+    const int tile = blockIdx.x;
+    const int bx = tile % gx, by = tile / gx;
+    const int lx = tid & 15, ly0 = (tid >> 4) * PPT;
+    const int px = bx * kTileX + lx;
+    const uint2 range = ranges[tile];
+    const uint32_t n = range.y - range.x;
+    const int nb = (int)((n + kBatch - 1) / kBatch);
+    const bool stats = kv_sum != nullptr;
+
+    for (int e = tid; e < 2 * kBatch; e += NT) {
+        (&s_wmax[0][0])[e] = 0;
+        (&s_ksum[0][0])[e] = 0.f;
+        (&s_kcnt[0][0])[e] = 0;
+    }
+    if (tid == 0) {
+        for (int i = 0; i < kBufs; i++) mbar_init(&s_bar[i], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int b = 0; b < 2 && b < nb; b++)
+            issue_batch(s_rec[b], &s_bar[b], recs, range.x + b * kBatch, min((uint32_t)kBatch, n - b * kBatch));
+    }
+
+    float T[PPT], C[PPT][3], wmax[PPT];
+    uint32_t last[PPT];
+    int maxid[PPT];
+    bool done[PPT];
+    float pyf[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+        T[k] = 1.0f;
+        C[k][0] = C[k][1] = C[k][2] = 0.f;
+        wmax[k] = 0.f;
+        last[k] = 0;
+        maxid[k] = -1;
+        const int py = by * kTileY + ly0 + k;
+        done[k] = !(px < W && py < H);
+        pyf[k] = (float)py;
+    }
+    const float pxf = (float)px;
+    bool all_done = true;
+#pragma unroll
+    for (int k = 0; k < PPT; k++) all_done = all_done && done[k];
+
+    uint32_t contributor = 0;
+    for (int b = 0; b < nb; b++) {
+        const int buf = b % kBufs;
+        const int acc = b & 1;
+        const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
+        if (!mbar_wait(&s_bar[buf], (uint32_t)((b / kBufs) & 1), err)) all_done = true;
+        const PairRecord* R = s_rec[buf];
+        const bool warp_live = !__all_sync(0xffffffffu, all_done);
+        if (warp_live) {
+            for (uint32_t j = 0; j < cnt; j++) {
+                if (__all_sync(0xffffffffu, all_done)) break;
+                const uint32_t position = contributor + j + 1;
+                const float4 ra = R[j].a;
+                const float4 rb = R[j].b;
+                float wj = 0.f, ksum = 0.f;
+                uint32_t kc = 0;
+#pragma unroll
+                for (int k = 0; k < PPT; k++) {
+                    if (done[k]) continue;
+                    const float2 d = {ra.x - pxf, ra.y - pyf[k]};
+                    const float power = -0.5f * (ra.z * d.x * d.x + rb.x * d.y * d.y) - ra.w * d.x * d.y;
+                    if (power > 0.0f) continue;
+                    const float alpha = min(0.99f, rb.y * exp(power));
+                    if (alpha < 1.0f / 255.0f) continue;
+                    const float test_T = T[k] * (1 - alpha);
+                    if (test_T < 0.0001f) {
+                        done[k] = true;
+                        continue;
+                    }
+                    const float4 rc = R[j].c;
+                    C[k][0] += rb.z * alpha * T[k];
+                    C[k][1] += rb.w * alpha * T[k];
+                    C[k][2] += rc.x * alpha * T[k];
+                    const float w = T[k] * alpha;
+                    if (w > wmax[k]) {
+                        wmax[k] = w;
+                        maxid[k] = __float_as_int(rc.y);
+                    }
+                    wj = fmaxf(wj, w);
+                    ksum += w;
+                    kc += 1;
+                    T[k] = test_T;
+                    last[k] = position;
+                }
+                bool ad = true;
+#pragma unroll
+                for (int k = 0; k < PPT; k++) ad = ad && done[k];
+                all_done = ad;
+                // per-Gaussian max weight (and statistics): warp, then CTA
+                if (__any_sync(0xffffffffu, wj > 0.f)) {
+                    const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(wj));
+                    float ks = 0.f;
+                    uint32_t kcs = 0;
+                    if (stats) {
+                        ks = warp_sum(ksum);
+                        kcs = __reduce_add_sync(0xffffffffu, kc);
+                    }
+                    if ((tid & 31) == 0) {
+                        atomicMax(&s_wmax[acc][j], wm);
+                        if (stats) {
+                            atomicAdd(&s_ksum[acc][j], ks);
+                            atomicAdd(&s_kcnt[acc][j], kcs);
+                        }
+                    }
+                }
+            }
+        }
+        contributor += cnt;
+        const int ndone = __syncthreads_count(all_done);
+        for (uint32_t e = tid; e < cnt; e += NT) {
+            const uint32_t wm = s_wmax[acc][e];
+            if (wm) {
+                const int id = __float_as_int(R[e].c.y);
+                atomicMax(reinterpret_cast<unsigned*>(out_point_weight) + id, wm);
+                s_wmax[acc][e] = 0;
+            }
+            if (stats) {
+                kv_sum[range.x + b * kBatch + e] = s_ksum[acc][e];
+                kv_cnt[range.x + b * kBatch + e] = s_kcnt[acc][e];
+                s_ksum[acc][e] = 0.f;
+                s_kcnt[acc][e] = 0;
+            }
+        }
+        if (ndone == NT) {
+            // drain the copy still in flight before the CTA's shared memory goes away
+            if (tid == 0 && b + 1 < nb) mbar_wait(&s_bar[(b + 1) % kBufs], (uint32_t)(((b + 1) / kBufs) & 1), err);
+            if (stats) {
+                // pairs never reached contribute nothing
+                for (uint32_t e = (b + 1) * kBatch + tid; e < n; e += NT) {
+                    kv_sum[range.x + e] = 0.f;
+                    kv_cnt[range.x + e] = 0;
+                }
+            }
+            break;
+        }
+        if (tid == 0 && b + 2 < nb) {
+            const int nbuf = (b + 2) % kBufs;
+            issue_batch(s_rec[nbuf], &s_bar[nbuf], recs, range.x + (b + 2) * kBatch,
+                        min((uint32_t)kBatch, n - (b + 2) * kBatch));
+        }
+    }
+
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+        const int py = by * kTileY + ly0 + k;
+        if (px < W && py < H) {
+            const int pix = W * py + px;
+            final_T[pix] = T[k];
+            n_contrib[pix] = last[k];
+            out_color[pix] = C[k][0] + T[k] * bg[0];
+            out_color[H * W + pix] = C[k][1] + T[k] * bg[1];
+            out_color[2 * H * W + pix] = C[k][2] + T[k] * bg[2];
+            out_point_id[pix] = maxid[k];
+            out_pw_pixel[pix] = wmax[k];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- backward
+template <int PPT>
+__global__ void __launch_bounds__(256 / PPT)
+    render_bwd_kernel(const uint2* __restrict__ ranges, const PairRecord* __restrict__ recs, int W, int H,
+                      const float* __restrict__ bg, const float* __restrict__ final_Ts,
+                      const uint32_t* __restrict__ n_contrib, const float* __restrict__ dL_dpixels,
+                      float* __restrict__ dL_dmean2D, float* __restrict__ dL_dconic, float* __restrict__ dL_dopacity,
+                      float* __restrict__ dL_dcolors, int consistent, unsigned* err)
+{
+    constexpr int NT = 256 / PPT;
+    constexpr int NG = 9;  // dcolor r,g,b ; dmean2D x,y ; dconic x,y,w ; dopacity
+    __shared__ __align__(128) PairRecord s_rec[kBufs][kBatch];
+    __shared__ __align__(8) uint64_t s_bar[kBufs];
+    __shared__ float s_acc[NG][kBatch];
+    __shared__ uint32_t s_max_last;
+
+    const int tid = threadIdx.x;
+    const int gx = (W + kTileX - 1) / kTileX;
+    const int tile = blockIdx.x;
+    const int bx = tile % gx, by = tile / gx;
+    const int lx = tid & 15, ly0 = (tid >> 4) * PPT;
+    const int px = bx * kTileX + lx;
+    const uint2 range = ranges[tile];
+
+    float T[PPT], T_final[PPT], dpix[PPT][3], accum[PPT][3], last_color[PPT][3], last_alpha[PPT], pyf[PPT];
+    uint32_t last[PPT];
+    float bg_dot[PPT];
+    const float bg0 = bg[0], bg1 = bg[1], bg2 = bg[2];
+    uint32_t my_max = 0;
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+        const int py = by * kTileY + ly0 + k;
+        const bool inside = px < W && py < H;
+        const int pix = W * py + px;
+        T_final[k] = inside ? final_Ts[pix] : 0.f;
+        T[k] = T_final[k];
+        last[k] = inside ? n_contrib[pix] : 0;
+        my_max = max(my_max, last[k]);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            dpix[k][c] = inside ? dL_dpixels[c * H * W + pix] : 0.f;
+            accum[k][c] = 0.f;
+            last_color[k][c] = 0.f;
+        }
+        last_alpha[k] = 0.f;
+        bg_dot[k] = bg0 * dpix[k][0] + bg1 * dpix[k][1] + bg2 * dpix[k][2];
+        pyf[k] = (float)py;
+    }
+    const float pxf = (float)px;
+    const float ddelx_dx = 0.5 * W;
+    const float ddely_dy = 0.5 * H;
+
+    if (tid == 0) {
+        s_max_last = 0;
+        for (int i = 0; i < kBufs; i++) mbar_init(&s_bar[i], 1);
+        mbar_fence_init();
+    }
+    for (int e = tid; e < NG * kBatch; e += NT) (&s_acc[0][0])[e] = 0.f;
+    __syncthreads();
+    const uint32_t wm = __reduce_max_sync(0xffffffffu, my_max);
+    if ((tid & 31) == 0) atomicMax(&s_max_last, wm);
+    __syncthreads();
+    // Entries at or beyond the largest n_contrib of the tile touch no pixel.
+    const uint32_t n = min(range.y - range.x, s_max_last);
+    const int nb = (int)((n + kBatch - 1) / kBatch);
+    // batch b holds entries [lo_b, hi_b) with hi_b = n - b*kBatch (back to front)
+    if (tid == 0) {
+        for (int b = 0; b < 2 && b < nb; b++) {
+            const uint32_t hi = n - b * kBatch, lo = hi > (uint32_t)kBatch ? hi - kBatch : 0;
+            issue_batch(s_rec[b], &s_bar[b], recs, range.x + lo, hi - lo);
+        }
+    }
+
+    for (int b = 0; b < nb; b++) {
+        const int buf = b % kBufs;
+        const uint32_t hi = n - b * kBatch, lo = hi > (uint32_t)kBatch ? hi - kBatch : 0;
+        const uint32_t cnt = hi - lo;
+        mbar_wait(&s_bar[buf], (uint32_t)((b / kBufs) & 1), err);
+        const PairRecord* R = s_rec[buf];
+        for (int j = (int)cnt - 1; j >= 0; j--) {
+            const uint32_t contributor = lo + (uint32_t)j;  // 0-based position in the tile list
+            const float4 ra = R[j].a;
+            const float4 rb = R[j].b;
+            float g[NG];
+#pragma unroll
+            for (int q = 0; q < NG; q++) g[q] = 0.f;
+            bool any = false;
+#pragma unroll
+            for (int k = 0; k < PPT; k++) {
+                if (contributor >= last[k]) continue;
+                const float2 d = {ra.x - pxf, ra.y - pyf[k]};
+                const float power = -0.5f * (ra.z * d.x * d.x + rb.x * d.y * d.y) - ra.w * d.x * d.y;
+                if (power > 0.0f) continue;
+                const float G = exp(power);
+                const float alpha = min(0.99f, rb.y * G);
+                if (alpha < 1.0f / 255.0f) continue;
+                T[k] = T[k] / (1.f - alpha);
+                const float dchannel_dcolor = alpha * T[k];
+                const float col[3] = {rb.z, rb.w, R[j].c.x};
+                float dL_dalpha = 0.0f;
+#pragma unroll
+                for (int ch = 0; ch < 3; ch++) {
+                    const float c = col[ch];
+                    accum[k][ch] = last_alpha[k] * last_color[k][ch] + (1.f - last_alpha[k]) * accum[k][ch];
+                    last_color[k][ch] = c;
+                    dL_dalpha += (c - accum[k][ch]) * dpix[k][ch];
+                    g[ch] += dchannel_dcolor * dpix[k][ch];
+                }
+                dL_dalpha *= T[k];
+                last_alpha[k] = alpha;
+                dL_dalpha += (-T_final[k] / (1.f - alpha)) * bg_dot[k];
+                if (consistent && rb.y * G > 0.99f) dL_dalpha = 0.f;
+                const float dL_dG = rb.y * dL_dalpha;
+                const float gdx = G * d.x;
+                const float gdy = G * d.y;
+                const float dG_ddelx = -gdx * ra.z - gdy * ra.w;
+                const float dG_ddely = -gdy * rb.x - gdx * ra.w;
+                g[3] += dL_dG * dG_ddelx * ddelx_dx;
+                g[4] += dL_dG * dG_ddely * ddely_dy;
+                g[5] += -0.5f * gdx * d.x * dL_dG;
+                g[6] += -0.5f * gdx * d.y * dL_dG;
+                g[7] += -0.5f * gdy * d.y * dL_dG;
+                g[8] += G * dL_dalpha;
+                any = true;
+            }
+            if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+                for (int q = 0; q < NG; q++) g[q] = warp_sum(g[q]);
+                if ((tid & 31) == 0) {
+#pragma unroll
+                    for (int q = 0; q < NG; q++) atomicAdd(&s_acc[q][j], g[q]);
+                }
+            }
+        }
+        __syncthreads();
+        for (uint32_t e = tid; e < cnt; e += NT) {
+            const int id = __float_as_int(R[e].c.y);
+            float v[NG];
+#pragma unroll
+            for (int q = 0; q < NG; q++) {
+                v[q] = s_acc[q][e];
+                s_acc[q][e] = 0.f;
+            }
+            if (v[0] != 0.f) atomicAdd(dL_dcolors + 3 * id, v[0]);
+            if (v[1] != 0.f) atomicAdd(dL_dcolors + 3 * id + 1, v[1]);
+            if (v[2] != 0.f) atomicAdd(dL_dcolors + 3 * id + 2, v[2]);
+            if (v[3] != 0.f) atomicAdd(dL_dmean2D + 3 * id, v[3]);
+            if (v[4] != 0.f) atomicAdd(dL_dmean2D + 3 * id + 1, v[4]);
+            if (v[5] != 0.f) atomicAdd(dL_dconic + 4 * id, v[5]);
+            if (v[6] != 0.f) atomicAdd(dL_dconic + 4 * id + 1, v[6]);
+            if (v[7] != 0.f) atomicAdd(dL_dconic + 4 * id + 3, v[7]);
+            if (v[8] != 0.f) atomicAdd(dL_dopacity + id, v[8]);
+        }
+        if (tid == 0 && b + 2 < nb) {
+            const int nbuf = (b + 2) % kBufs;
+            const uint32_t hi2 = n - (b + 2) * kBatch, lo2 = hi2 > (uint32_t)kBatch ? hi2 - kBatch : 0;
+            issue_batch(s_rec[nbuf], &s_bar[nbuf], recs, range.x + lo2, hi2 - lo2);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, const float* bg, float* out_color,
+                       int* point_id, float* pw_pixel, float* point_weight, bool stats, unsigned* err,
+                       cudaStream_t s)
+{
+    const int gx = (W + kTileX - 1) / kTileX, gy = (H + kTileY - 1) / kTileY;
+    constexpr int PPT = 2;
+    render_fwd_kernel<PPT><<<gx * gy, 256 / PPT, 0, s>>>(im.ranges, b.rec, W, H, bg, out_color, im.final_T,
+                                                          im.n_contrib, point_id, pw_pixel, point_weight,
+                                                          stats ? b.kv_sum : nullptr, stats ? b.kv_cnt : nullptr, err);
+}
+
+void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, const float* bg,
+                       const float* dL_dpix, float* dmean2D, float* dconic, float* dopac, float* dcolor,
+                       int consistent, unsigned* err, cudaStream_t s)
+{
+    const int gx = (W + kTileX - 1) / kTileX, gy = (H + kTileY - 1) / kTileY;
+    constexpr int PPT = 2;
+    render_bwd_kernel<PPT><<<gx * gy, 256 / PPT, 0, s>>>(im.ranges, b.rec, W, H, bg, im.final_T, im.n_contrib,
+                                                          dL_dpix, dmean2D, dconic, dopac, dcolor, consistent, err);
+}
+
+}  // namespace fgs

@@ -1,0 +1,153 @@
+/*
+ * filtergs_b200 -- C ABI of the B200 (sm_100a) FilterGS rasterizer.
+ *
+ * Plain device pointers, sizes and a cudaStream_t passed as void*.  No torch
+ * types.  Every entry point returns an FGS_* status.  All pointers named in
+ * an argument list are device pointers unless the comment says "host".
+ *
+ * The reference interface each entry point replaces is cited beside it
+ * (paths inside the reference project xenon-w/FilterGS).
+ */
+#ifndef FILTERGS_B200_H
+#define FILTERGS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define FGS_OK 0
+#define FGS_ERR_ARG 1          /* invalid argument (shape, null pointer, size)          */
+#define FGS_ERR_CUDA 2         /* a CUDA runtime call or launch failed                  */
+#define FGS_ERR_TIMEOUT 3      /* a bounded device-side wait gave up                    */
+#define FGS_ERR_PREFILTERED 4  /* prefiltered set, yet a Gaussian failed the near test   */
+#define FGS_ERR_CAPACITY 5     /* a preallocated capacity was exceeded                  */
+#define FGS_ERR_OVERFLOW 6     /* more tile/Gaussian pairs than the binning supports    */
+
+#define FGS_BACKWARD_REF_COMPAT 0 /* reproduce the reference backward (+0.3 dilation)    */
+#define FGS_BACKWARD_CONSISTENT 1 /* differentiate exactly what the forward computed     */
+
+#define FGS_STATS_SLOTS 64        /* RenderStats::MAX_KPC_BINS (rasterizer.h:24)        */
+
+/* Human-readable text of a status code (static storage). */
+const char *fgs_status_string(int status);
+/* Library version string. */
+const char *fgs_version(void);
+
+/* ------------------------------------------------------------------ arguments
+ * One rasterizer call.  Mirrors the argument list of
+ * RasterizeGaussiansCUDA (antialias/rasterize_points.cu:36-62) after the
+ * binding resolved its empty tensors to null pointers (:112-135).          */
+typedef struct fgs_raster_args {
+    int P;                       /* number of Gaussians                                   */
+    int D;                       /* active SH degree                                     */
+    int M;                       /* SH coefficients per channel (0 when shs is null)      */
+    int width, height;           /* image size in pixels                                  */
+    const float *background;     /* [3]                                                   */
+    const float *means3D;        /* [P,3]                                                 */
+    const float *shs;            /* [P,M,3] or null                                       */
+    const float *colors_precomp; /* [P,3]  or null (exactly one of shs / colors_precomp)  */
+    const float *opacities;      /* [P]                                                   */
+    const float *scales;         /* [P,3]  or null                                        */
+    float scale_modifier;
+    const float *rotations;      /* [P,4] (r,x,y,z) or null                               */
+    const float *cov3D_precomp;  /* [P,6]  or null (exactly one of scale+rot / cov3D)     */
+    const float *viewmatrix;     /* [16] column-major world->view                         */
+    const float *projmatrix;     /* [16] column-major world->clip                         */
+    const float *campos;         /* [3]                                                   */
+    float tan_fovx, tan_fovy;
+    int prefiltered;             /* reference traps on a violation; here FGS_ERR_PREFILTERED */
+    int use_filter;              /* 2D dilation: cov2D diagonal = max(., 0.3)             */
+    float ogfs_epsilon_scale, ogfs_epsilon_max, ogfs_energy_floor, ogfs_radius_ratio_min;
+    int ogfs_enable_stats;       /* compute the KPC/GTC statistics vector                 */
+    float filter3d_scale;        /* 3D filter: cov3D += (s * z_view / focal_x)^2 I; 0 = off (no reference counterpart) */
+} fgs_raster_args;
+
+/* ------------------------------------------------------------------ workspaces
+ * The three opaque byte buffers of the reference forward/backward
+ * (geomBuffer / imageBuffer / binningBuffer, rasterizer_impl.cu:211-250).
+ * Their layout is private to this library; they only need the returned size
+ * and 256-byte alignment, and are passed unchanged from forward to backward. */
+size_t fgs_geom_bytes(int P);
+size_t fgs_image_bytes(int width, int height);
+size_t fgs_binning_bytes(long long num_rendered, int P);
+
+/* ------------------------------------------------------------------ forward
+ * CudaRasterizer::Rasterizer::forward (rasterizer.h:49-76,
+ * rasterizer_impl.cu:254-563), split at the point where the reference copies
+ * num_rendered to the host (rasterizer_impl.cu:367):
+ *   1. fgs_forward_preprocess: preprocess + depth ordering; synchronises the
+ *      stream once and returns num_rendered (host long long) and writes radii
+ *      ([P] int, may be null).
+ *   2. the caller allocates fgs_binning_bytes(num_rendered, P);
+ *   3. fgs_forward_render: binning, sort, tile ranges, compositing.
+ * Outputs are fully written (no zero-initialisation needed):
+ *   out_color [3,H,W], out_point_id [H,W], out_point_weight_pixel [H,W],
+ *   out_point_weight [P].  When ogfs_enable_stats is set, stats_host (host,
+ *   stats_len doubles) receives the reference's statistics vector
+ *   (rasterize_points.cu:138-177): 9 + 2*FGS_STATS_SLOTS + 2*tiles values,
+ *   and the call synchronises the stream.                                   */
+int fgs_forward_preprocess(const fgs_raster_args *a, void *geom, void *image, int *radii,
+                           long long *num_rendered, void *stream);
+int fgs_forward_render(const fgs_raster_args *a, void *geom, void *image, void *binning, long long num_rendered,
+                       const int *radii, float *out_color, int *out_point_id, float *out_point_weight_pixel,
+                       float *out_point_weight, double *stats_host, int stats_len, void *stream);
+
+/* ------------------------------------------------------------------ backward
+ * CudaRasterizer::Rasterizer::backward (rasterizer.h:82-111,
+ * rasterizer_impl.cu:582-676) and RasterizeGaussiansBackwardCUDA
+ * (rasterize_points.cu:181-260).  All gradient outputs are fully written:
+ *   dL_dmeans2D [P,3], dL_dconic [P,4], dL_dopacity [P], dL_dcolors [P,3],
+ *   dL_dmeans3D [P,3], dL_dcov3D [P,6], dL_dsh [P,M,3] (may be null when M==0),
+ *   dL_dscales [P,3], dL_drotations [P,4] (both may be null when scales is null).
+ * backward_mode: FGS_BACKWARD_REF_COMPAT or FGS_BACKWARD_CONSISTENT.        */
+int fgs_backward(const fgs_raster_args *a, const void *geom, const void *image, const void *binning,
+                 long long num_rendered, const int *radii, const float *dL_dout_color, float *dL_dmeans2D,
+                 float *dL_dconic, float *dL_dopacity, float *dL_dcolors, float *dL_dmeans3D, float *dL_dcov3D,
+                 float *dL_dsh, float *dL_dscales, float *dL_drotations, int backward_mode, void *stream);
+
+/* Synchronise `stream` and return the first error recorded by device code in
+ * `geom` (FGS_OK when none).  The debug flag of the Python API calls this. */
+int fgs_check(const void *geom, void *stream);
+
+/* ------------------------------------------------------------------ utilities
+ * markVisible (rasterizer_impl.cu:197-209, rasterize_points.cu:299-318): present[P] bytes 0/1. */
+int fgs_mark_visible(int P, const float *means3D, const float *viewmatrix, const float *projmatrix,
+                     uint8_t *present, void *stream);
+/* _C.compute_radius (forward.cu:208-263, rasterize_points.cu:263-296): 3-sigma radius, float[P]. */
+int fgs_compute_radius(int P, int height, int width, const float *means3D, const float *scales,
+                       const float *rotations, const float *viewmatrix, const float *projmatrix, float tan_fovx,
+                       float tan_fovy, float *radii, void *stream);
+/* FilterGS compute_radius_v2.compute_radius (compute_radius_kernel_v2.cu:180-229,355-380). */
+int fgs_compute_radius_v2(int P, const float *means3D, const float *scales, const float *rotations,
+                          const float *projmatrix, const float *viewmatrix, float focal_x, float focal_y,
+                          float tan_fovx, float tan_fovy, float *radii, void *stream);
+/* FilterGS compute_visibility_radius (compute_radius_kernel_v2.cu:231-353,382-430):
+ * mask[P] bytes, radius2d[P], depth[P].  ancestor_path is [P, max_level] int32. */
+int fgs_visibility_radius(int P, const float *means3D, const float *log_scales, const float *rotations,
+                          const float *projmatrix, const float *viewmatrix, const int32_t *tree_node_index,
+                          const int32_t *ancestor_path, int max_level, float focal_x, float focal_y,
+                          float tan_fovx, float tan_fovy, float padding, float radius_max,
+                          float radius_filter_threshold, uint8_t *mask, float *radius2d, float *depth,
+                          void *stream);
+
+/* ------------------------------------------------------------------ test accessors
+ * Sorted (tile|depth) keys and Gaussian ids of a forward, in the reference's
+ * 64-bit key format (rasterizer_impl.cu:139-141).  keys/vals: [num_rendered]. */
+int fgs_sorted_pairs(const void *geom, const void *binning, int P, long long num_rendered, uint64_t *keys,
+                     uint32_t *vals, void *stream);
+/* Per-Gaussian preprocess outputs kept in geom: means2D [P,2], depth [P],
+ * conic_opacity [P,4], rgb [P,3], tiles_touched [P] (any may be null). */
+int fgs_preprocess_outputs(const void *geom, int P, float *means2D, float *depths, float *conic_opacity,
+                           float *rgb, uint32_t *tiles_touched, void *stream);
+/* Per-pixel state kept in image: final transmittance [H*W], n_contrib [H*W], ranges [tiles,2]. */
+int fgs_image_outputs(const void *image, int width, int height, float *final_T, uint32_t *n_contrib,
+                      uint32_t *ranges, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FILTERGS_B200_H */
