@@ -60,7 +60,13 @@ SIGNATURES = {
     "fgs_sorted_pairs": (i32, [vp, vp, i32, i64, vp, vp, vp]),
     "fgs_preprocess_outputs": (i32, [vp, i32, vp, vp, vp, vp, vp, vp]),
     "fgs_image_outputs": (i32, [vp, i32, i32, vp, vp, vp, vp]),
+    "fgs_profile_enable": (i32, [i32]),
+    "fgs_profile_read": (i32, [vp, vp, i32]),
+    "fgs_launch_count": (i64, []),
 }
+
+STAGES = ["preprocess", "depth_sort", "duplicate", "tile_sort", "ranges", "render_fwd", "stats", "render_bwd",
+          "preprocess_bwd"]
 
 _lib = None
 
@@ -95,6 +101,24 @@ def status_string(status):
 def check(status, where):
     if status != FGS_OK:
         raise FgsError(status, where)
+
+
+def profile_enable(on=True):
+    lib().fgs_profile_enable(int(bool(on)))
+
+
+def profile_read(reset=True):
+    """Per-stage (milliseconds summed, calls) recorded since the last reset."""
+    import numpy as np
+    ms = np.zeros(len(STAGES), np.float64)
+    calls = np.zeros(len(STAGES), np.int64)
+    check(lib().fgs_profile_read(ms.ctypes.data_as(vp), calls.ctypes.data_as(vp), int(bool(reset))),
+          "fgs_profile_read")
+    return {n: (float(ms[i]), int(calls[i])) for i, n in enumerate(STAGES)}
+
+
+def launch_count():
+    return int(lib().fgs_launch_count())
 
 
 def call(name, *args):

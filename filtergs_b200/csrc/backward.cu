@@ -301,6 +301,7 @@ void launch_preprocess_bwd(const PreParams& p, const int* radii, const GeomState
     if (p.P <= 0) return;
     preprocess_bwd_kernel<<<(p.P + 255) / 256, 256, 0, s>>>(p, radii, g.clamped, dmean2D, dconic, dcolor, dopac,
                                                              dmean3D, dcov3D, dsh, dscale, drot, consistent);
+    note_launches(1);
 }
 
 }  // namespace fgs

@@ -311,6 +311,7 @@ void launch_depth_sort(const GeomState& g, int P, cudaStream_t s)
     const uint32_t hb0 = (n + 1023) / 1024;
     const int hb = (int)(hb0 < 1184u ? hb0 : 1184u);
     depth_hist_kernel<<<hb, 256, 0, s>>>(g.depth_key, n, g.hist);
+    note_launches(5);
     // ping-pong: depth_key -> sort_keys_b -> depth_key -> sort_keys_b ; ids a/b
     const uint32_t* kin[4] = {g.depth_key, g.sort_keys_b, g.depth_key, g.sort_keys_b};
     uint32_t* kout[4] = {g.sort_keys_b, g.depth_key, g.sort_keys_b, nullptr};
@@ -336,6 +337,7 @@ void launch_duplicate(const GeomState& g, const BinState& b, uint32_t V, uint32_
     duplicate_kernel<<<chunks_of(V, 256), 256, 0, s>>>(g.sort_ids_b, g.tiles, g.grec, g.radii, V, gx, gy, tout,
                                                        vout, K, b.scan_status, g.counters + 8, g.hist + 4 * kRadix,
                                                        passes, g.err);
+    note_launches(1);
 }
 
 void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int tile_bits, cudaStream_t s)
@@ -357,6 +359,7 @@ void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int ti
         ki = ko;
         vi = vo;
     }
+    note_launches(passes);
 }
 
 void launch_ranges(const BinState& b, const ImageState& im, long long K, int num_tiles, cudaStream_t s)
@@ -364,6 +367,7 @@ void launch_ranges(const BinState& b, const ImageState& im, long long K, int num
     cudaMemsetAsync(im.ranges, 0, sizeof(uint2) * (size_t)num_tiles, s);
     if (K <= 0) return;
     ranges_kernel<<<chunks_of(K, 256), 256, 0, s>>>(b.tile_b, (uint32_t)K, im.ranges);
+    note_launches(1);
 }
 
 }  // namespace fgs

@@ -1,8 +1,11 @@
 // extern "C" entry points (include/filtergs_b200.h): argument checks,
 // workspace carving, kernel sequencing on the caller's stream.
+#include <atomic>
 #include <cerrno>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "fgs_common.cuh"
 #include "fgs_internal.h"
@@ -206,6 +209,52 @@ __global__ void pre_outputs_kernel(const PairRecord* __restrict__ grec, const ui
 
 }  // namespace
 
+// ---------------------------------------------------------------- profiling
+namespace {
+struct EventPair {
+    int stage;
+    cudaEvent_t a, b;
+};
+std::atomic<long long> g_launches{0};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<EventPair> g_prof_live;
+std::vector<cudaEvent_t> g_prof_pool;
+
+cudaEvent_t pool_event()
+{
+    if (!g_prof_pool.empty()) {
+        cudaEvent_t e = g_prof_pool.back();
+        g_prof_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+}  // namespace
+
+void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+StageTimer::StageTimer(int st, cudaStream_t s) : stage(st), stream(s), slot(nullptr)
+{
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    if (!g_prof_on) return;
+    EventPair* ep = new EventPair{st, pool_event(), pool_event()};
+    cudaEventRecord(ep->a, s);
+    slot = ep;
+}
+
+StageTimer::~StageTimer()
+{
+    if (!slot) return;
+    EventPair* ep = static_cast<EventPair*>(slot);
+    cudaEventRecord(ep->b, stream);
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof_live.push_back(*ep);
+    delete ep;
+}
+
 GeomState geom_views(void* base, int P) { return carve_geom(base, P).g; }
 size_t geom_bytes(int P) { return carve_geom(nullptr, P).total; }
 
@@ -285,8 +334,14 @@ int fgs_forward_preprocess(const fgs_raster_args* a, void* geom, void* image, in
     }
     GeomCarve gc = carve_geom(geom, p.P);
     cudaMemsetAsync(gc.zero_begin, 0, gc.zero_bytes, s);
-    launch_preprocess(p, gc.g, radii, s);
-    launch_depth_sort(gc.g, p.P, s);
+    {
+        StageTimer t(FGS_STAGE_PREPROCESS, s);
+        launch_preprocess(p, gc.g, radii, s);
+    }
+    {
+        StageTimer t(FGS_STAGE_DEPTH_SORT, s);
+        launch_depth_sort(gc.g, p.P, s);
+    }
     if ((st = check_launch())) return st;
     unsigned long long* tot = reinterpret_cast<unsigned long long*>(pin + 8);
     cudaMemcpyAsync(tot, gc.g.total, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
@@ -325,12 +380,22 @@ int fgs_forward_render(const fgs_raster_args* a, void* geom, void* image, void* 
     if (K > 0) {
         cudaMemsetAsync(bc.b.status, 0, sizeof(uint32_t) * (bc.b.status_words + bc.b.scan_words), s);
         // V lives on the device (g.total[1]); every Gaussian beyond it has no pairs.
-        launch_duplicate(g, bc.b, (uint32_t)p.P, (uint32_t)K, W, H, tbits, s);
+        {
+            StageTimer t(FGS_STAGE_DUPLICATE, s);
+            launch_duplicate(g, bc.b, (uint32_t)p.P, (uint32_t)K, W, H, tbits, s);
+        }
+        StageTimer t(FGS_STAGE_TILE_SORT, s);
         launch_tile_sort(g, bc.b, K, tbits, s);
     }
-    launch_ranges(bc.b, im, K, num_tiles, s);
-    launch_render_fwd(W, H, im, bc.b, a->background, out_color, out_point_id, out_point_weight_pixel,
-                      out_point_weight, stats && K > 0, g.err, s);
+    {
+        StageTimer t(FGS_STAGE_RANGES, s);
+        launch_ranges(bc.b, im, K, num_tiles, s);
+    }
+    {
+        StageTimer t_render(FGS_STAGE_RENDER_FWD, s);
+        launch_render_fwd(W, H, im, bc.b, a->background, out_color, out_point_id, out_point_weight_pixel,
+                          out_point_weight, stats && K > 0, g.err, s);
+    }
     if ((st = check_launch())) return st;
     unsigned int* pin = pinned_words();
     if (stats && stats_host) {
@@ -345,6 +410,7 @@ int fgs_forward_render(const fgs_raster_args* a, void* geom, void* image, void* 
             // device scratch for the statistics: the tail of the pair-record buffer is free
             // only when it is large enough; otherwise use a temporary allocation.
             if (cudaMallocAsync(reinterpret_cast<void**>(&dev), nd * sizeof(double), s) != cudaSuccess) return FGS_ERR_CUDA;
+            StageTimer t(FGS_STAGE_STATS, s);
             launch_kpc_stats(bc.b, im, num_tiles, kpc_used_thresh(), dev, s);
         }
         double* host = static_cast<double*>(std::malloc(nd * sizeof(double)));
@@ -424,12 +490,17 @@ int fgs_backward(const fgs_raster_args* a, const void* geom, const void* image, 
     }
     if (!p.shs && dL_dsh && a->M > 0) cudaMemsetAsync(dL_dsh, 0, sizeof(float) * 3 * (size_t)a->M * p.P, s);
     const int consistent = backward_mode == FGS_BACKWARD_CONSISTENT;
-    if (num_rendered > 0)
+    if (num_rendered > 0) {
+        StageTimer t(FGS_STAGE_RENDER_BWD, s);
         launch_render_bwd(p.W, p.H, im, b, a->background, dL_dout_color, dL_dmeans2D, dL_dconic, dL_dopacity,
                           dL_dcolors, consistent, g.err, s);
-    launch_preprocess_bwd(p, rad, g, dL_dmeans2D, dL_dconic, dL_dcolors, dL_dopacity, dL_dmeans3D, dL_dcov3D,
-                          p.shs ? dL_dsh : nullptr, p.scales ? dL_dscales : nullptr,
-                          p.scales ? dL_drotations : nullptr, consistent, s);
+    }
+    {
+        StageTimer t_pb(FGS_STAGE_PREPROCESS_BWD, s);
+        launch_preprocess_bwd(p, rad, g, dL_dmeans2D, dL_dconic, dL_dcolors, dL_dopacity, dL_dmeans3D, dL_dcov3D,
+                              p.shs ? dL_dsh : nullptr, p.scales ? dL_dscales : nullptr,
+                              p.scales ? dL_drotations : nullptr, consistent, s);
+    }
     if ((st = check_launch())) return st;
     unsigned int* pin = pinned_words();
     cudaMemcpyAsync(pin + 4, g.err, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
@@ -540,5 +611,46 @@ int fgs_image_outputs(const void* image, int width, int height, float* final_T, 
     if (ranges) cudaMemcpyAsync(ranges, im.ranges, T * sizeof(uint2), cudaMemcpyDeviceToDevice, s);
     return check_launch();
 }
+
+int fgs_profile_enable(int on)
+{
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    g_prof_on = on != 0;
+    return FGS_OK;
+}
+
+int fgs_profile_read(double* ms, long long* calls, int reset)
+{
+    std::vector<EventPair> live;
+    {
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        live = g_prof_live;
+        if (reset) g_prof_live.clear();
+    }
+    for (int i = 0; i < FGS_NUM_STAGES; i++) {
+        if (ms) ms[i] = 0.0;
+        if (calls) calls[i] = 0;
+    }
+    int st = FGS_OK;
+    for (const EventPair& e : live) {
+        if (cudaEventSynchronize(e.b) != cudaSuccess) st = FGS_ERR_CUDA;
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, e.a, e.b) != cudaSuccess) st = FGS_ERR_CUDA;
+        if (e.stage >= 0 && e.stage < FGS_NUM_STAGES) {
+            if (ms) ms[e.stage] += t;
+            if (calls) calls[e.stage] += 1;
+        }
+    }
+    if (reset) {
+        std::lock_guard<std::mutex> lk(g_prof_mu);
+        for (const EventPair& e : live) {
+            g_prof_pool.push_back(e.a);
+            g_prof_pool.push_back(e.b);
+        }
+    }
+    return st;
+}
+
+long long fgs_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 }  // extern "C"

@@ -105,4 +105,14 @@ void launch_visibility_radius(int P, const float* means, const float* lscales, c
                               float padding, float radius_max, float radius_filter, uint8_t* mask, float* radius2d,
                               float* depth, cudaStream_t s);
 
+// Kernel-launch accounting (fgs_launch_count) and per-stage event timing.
+void note_launches(int n);
+struct StageTimer {
+    StageTimer(int stage, cudaStream_t s);
+    ~StageTimer();
+    int stage;
+    cudaStream_t stream;
+    void* slot;
+};
+
 }  // namespace fgs

@@ -333,6 +333,7 @@ void launch_preprocess(const PreParams& p, const GeomState& g, int* radii, cudaS
 {
     if (p.P <= 0) return;
     preprocess_kernel<<<(p.P + kThreads - 1) / kThreads, kThreads, 0, s>>>(p, g, radii);
+    note_launches(1);
 }
 
 void launch_compute_radius(int variant, int P, const float* means, const float* scales, const float* rots,
@@ -342,12 +343,14 @@ void launch_compute_radius(int variant, int P, const float* means, const float* 
     if (P <= 0) return;
     compute_radius_kernel<<<(P + 255) / 256, 256, 0, s>>>(variant, P, means, scales, rots, view, proj, fx, fy,
                                                            tanx, tany, radius);
+    note_launches(1);
 }
 
 void launch_mark_visible(int P, const float* means, const float* view, uint8_t* present, cudaStream_t s)
 {
     if (P <= 0) return;
     mark_visible_kernel<<<(P + 255) / 256, 256, 0, s>>>(P, means, view, present);
+    note_launches(1);
 }
 
 void launch_visibility_radius(int P, const float* means, const float* lscales, const float* rots,
@@ -361,6 +364,7 @@ void launch_visibility_radius(int P, const float* means, const float* lscales, c
                                                        padding, mask, radius2d, depth);
     visibility_phase2<<<(P + 255) / 256, 256, 0, s>>>(P, node_index, ancestors, L, radius_max, radius_filter,
                                                        mask, radius2d);
+    note_launches(2);
 }
 
 }  // namespace fgs

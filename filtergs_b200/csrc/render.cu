@@ -442,6 +442,7 @@ void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, co
     render_fwd_kernel<PPT><<<gx * gy, 256 / PPT, 0, s>>>(im.ranges, b.rec, W, H, bg, out_color, im.final_T,
                                                           im.n_contrib, point_id, pw_pixel, point_weight,
                                                           stats ? b.kv_sum : nullptr, stats ? b.kv_cnt : nullptr, err);
+    note_launches(1);
 }
 
 void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, const float* bg,
@@ -452,6 +453,7 @@ void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, co
     constexpr int PPT = 2;
     render_bwd_kernel<PPT><<<gx * gy, 256 / PPT, 0, s>>>(im.ranges, b.rec, W, H, bg, im.final_T, im.n_contrib,
                                                           dL_dpix, dmean2D, dconic, dopac, dcolor, consistent, err);
+    note_launches(1);
 }
 
 }  // namespace fgs

@@ -75,6 +75,7 @@ void launch_kpc_stats(const BinState& b, const ImageState& im, int num_tiles, fl
     if (num_tiles <= 0) return;
     kpc_kernel<<<num_tiles, 128, 0, s>>>(im.ranges, b.kv_sum, b.kv_cnt, used_thresh, dev_out, dev_out + 3 + kBins,
                                          dev_out + 3 + kBins + num_tiles, num_tiles);
+    note_launches(1);
 }
 
 }  // namespace fgs

@@ -147,6 +147,27 @@ int fgs_preprocess_outputs(const void *geom, int P, float *means2D, float *depth
 int fgs_image_outputs(const void *image, int width, int height, float *final_T, uint32_t *n_contrib,
                       uint32_t *ranges, void *stream);
 
+/* ------------------------------------------------------------------ profiling hooks
+ * No reference counterpart (the reference times stages with torch CUDA events
+ * around whole calls, FilterGS/filtergs.py:26-39).  When enabled, forward and
+ * backward record a CUDA event pair around each stage below; fgs_profile_read
+ * synchronises on those events and returns the summed milliseconds and call
+ * counts per stage.  fgs_launch_count is the number of kernels this library
+ * has launched in the process (memsets and copies excluded).               */
+#define FGS_STAGE_PREPROCESS 0
+#define FGS_STAGE_DEPTH_SORT 1
+#define FGS_STAGE_DUPLICATE 2
+#define FGS_STAGE_TILE_SORT 3
+#define FGS_STAGE_RANGES 4
+#define FGS_STAGE_RENDER_FWD 5
+#define FGS_STAGE_STATS 6
+#define FGS_STAGE_RENDER_BWD 7
+#define FGS_STAGE_PREPROCESS_BWD 8
+#define FGS_NUM_STAGES 9
+int fgs_profile_enable(int on);
+int fgs_profile_read(double *ms, long long *calls, int reset);
+long long fgs_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif
