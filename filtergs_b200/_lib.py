@@ -63,6 +63,8 @@ SIGNATURES = {
     "fgs_profile_enable": (i32, [i32]),
     "fgs_profile_read": (i32, [vp, vp, i32]),
     "fgs_launch_count": (i64, []),
+    "fgs_noalloc_capacity_bytes": (sz, []),
+    "fgs_forward_noalloc": (i32, [C.POINTER(RasterArgs), vp, vp, vp, vp, vp, C.POINTER(i64), vp]),
 }
 
 STAGES = ["preprocess", "depth_sort", "duplicate", "tile_sort", "ranges", "render_fwd", "stats", "render_bwd",

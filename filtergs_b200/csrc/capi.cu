@@ -124,7 +124,9 @@ int check_launch()
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
-int make_params(const fgs_raster_args* a, PreParams& p, bool backward = false)
+}  // namespace
+
+int make_params(const fgs_raster_args* a, PreParams& p, bool backward)
 {
     if (!a) return FGS_ERR_ARG;
     if (a->P < 0 || a->width <= 0 || a->height <= 0) return FGS_ERR_ARG;
@@ -168,6 +170,8 @@ int make_params(const fgs_raster_args* a, PreParams& p, bool backward = false)
                 (!p.rots || aligned16(p.rots)) && (!p.shs || aligned16(p.shs));
     return FGS_OK;
 }
+
+namespace {
 
 // rasterizer_impl.cu:44-55
 float kpc_used_thresh()

@@ -105,6 +105,10 @@ void launch_visibility_radius(int P, const float* means, const float* lscales, c
                               float padding, float radius_max, float radius_filter, uint8_t* mask, float* radius2d,
                               float* depth, cudaStream_t s);
 
+// Validate a fgs_raster_args and derive the kernel parameters (opacities may
+// be absent in backward).
+int make_params(const fgs_raster_args* a, PreParams& p, bool backward = false);
+
 // Kernel-launch accounting (fgs_launch_count) and per-stage event timing.
 void note_launches(int n);
 struct StageTimer {

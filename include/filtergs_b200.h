@@ -147,6 +147,27 @@ int fgs_preprocess_outputs(const void *geom, int P, float *means2D, float *depth
 int fgs_image_outputs(const void *image, int width, int height, float *final_T, uint32_t *n_contrib,
                       uint32_t *ranges, void *stream);
 
+/* ------------------------------------------------------------------ forward without allocation
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory while they render (a render thread that must not pay cudaMalloc's
+ * device-wide synchronisation, a plugin inside an application that owns all
+ * device memory, a process under a fixed memory budget): the whole forward
+ * (preprocess, binning, sort, compositing; no statistics) with its scratch
+ * workspaces in one library-owned device array of fgs_noalloc_capacity_bytes()
+ * (32 MiB) that every GPU loading this library keeps until exit.  The caller
+ * passes the inputs in `a` and the outputs: radii [P] int, out_color [3,H,W],
+ * out_point_id [H,W], out_point_weight_pixel [H,W], out_point_weight [P];
+ * num_rendered (host) receives the pair count.  Workspaces that do not fit
+ * the array are rejected with FGS_ERR_CAPACITY (checked before any work for
+ * the per-Gaussian and per-pixel state, after preprocessing for the pairs).
+ * The first call on a device looks up the array's device address.  The call
+ * synchronises `stream`.  Calls share the array: two calls that overlap on
+ * the GPU race and must be serialised by the caller.                       */
+size_t fgs_noalloc_capacity_bytes(void);
+int fgs_forward_noalloc(const fgs_raster_args *a, int *radii, float *out_color, int *out_point_id,
+                        float *out_point_weight_pixel, float *out_point_weight, long long *num_rendered,
+                        void *stream);
+
 /* ------------------------------------------------------------------ profiling hooks
  * No reference counterpart (the reference times stages with torch CUDA events
  * around whole calls, FilterGS/filtergs.py:26-39).  When enabled, forward and
