@@ -19,7 +19,6 @@ per-step camera and upstream gradient copied in from pinned host memory and the
 rendered image copied back.
 """
 import argparse
-import ctypes
 import json
 import os
 import subprocess
@@ -51,6 +50,9 @@ def parse():
     ap.add_argument("--stats", action="store_true", help="ogfs_enable_stats=True (the API default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default render kernel shape")
+    ap.add_argument("--render-config", default=None,
+                    help="fwd_ppt,fwd_batch,bwd_ppt,bwd_batch (skips the autotuner)")
     return ap.parse_args()
 
 
@@ -260,6 +262,17 @@ def main():
     sc, scene, views = make_workload(args, device, rank)
     bg = torch.zeros(3, device=device)
     nv = len(views)
+    tuned = None
+    if args.impl == "ours" and args.render_config:
+        _lib.set_render_config(*[int(x) for x in args.render_config.split(",")])
+    elif args.impl == "ours" and not args.no_autotune:
+        from filtergs_b200.autotune import tune_render
+        it = iter(range(1 << 30))
+        tuned, table = tune_render(lambda: step_c(mod, scene, views[next(it) % nv], bg, args.stats),
+                                   key=("urban", args.P, args.width, args.height))
+        if rank == 0:
+            print("autotune render (ppt,batch)->(fwd ms, bwd ms): " +
+                  ", ".join(f"{k}:{v[0]:.3f}/{v[1]:.3f}" for k, v in sorted(table.items())), file=sys.stderr)
     for i in range(args.warmup):
         step_c(mod, scene, views[i % nv], bg, args.stats)
     torch.cuda.synchronize()
@@ -338,6 +351,8 @@ def main():
                                   "algorithmic_bytes_per_launch": ab, "peak_source": peak_kind,
                                   "note": "render kernels are exp/FP32-issue bound; see profiles/ for pipe utilisation"}
             result["stages"] = stages
+            result["config"]["render_config"] = list(_lib.get_render_config())
+            result["config"]["autotuned"] = tuned is not None
             result["gpu_launches"] = int(launches)
             if e2e:
                 result["e2e"] = e2e

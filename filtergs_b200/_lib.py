@@ -64,6 +64,8 @@ SIGNATURES = {
     "fgs_profile_read": (i32, [vp, vp, i32]),
     "fgs_launch_count": (i64, []),
     "fgs_noalloc_capacity_bytes": (sz, []),
+    "fgs_set_render_config": (i32, [i32, i32, i32, i32]),
+    "fgs_get_render_config": (i32, [vp]),
     "fgs_forward_noalloc": (i32, [C.POINTER(RasterArgs), vp, vp, vp, vp, vp, C.POINTER(i64), vp]),
 }
 
@@ -117,6 +119,17 @@ def profile_read(reset=True):
     check(lib().fgs_profile_read(ms.ctypes.data_as(vp), calls.ctypes.data_as(vp), int(bool(reset))),
           "fgs_profile_read")
     return {n: (float(ms[i]), int(calls[i])) for i, n in enumerate(STAGES)}
+
+
+def set_render_config(fwd_ppt=2, fwd_batch=256, bwd_ppt=2, bwd_batch=256):
+    check(lib().fgs_set_render_config(int(fwd_ppt), int(fwd_batch), int(bwd_ppt), int(bwd_batch)),
+          "fgs_set_render_config")
+
+
+def get_render_config():
+    cfg = (C.c_int * 4)()
+    check(lib().fgs_get_render_config(C.cast(cfg, vp)), "fgs_get_render_config")
+    return tuple(cfg)
 
 
 def launch_count():

@@ -13,6 +13,8 @@
 // forward as computed: max(., 0.3) dilation only when use_filter, with a zero
 // gradient for a clamped diagonal entry, exact 1/det^2, and the t.z
 // dependence of a clamped t.x / t.y.
+#include <algorithm>
+
 #include "fgs_common.cuh"
 #include "fgs_internal.h"
 
@@ -104,18 +106,21 @@ __device__ __forceinline__ float3 sh_backward(int deg, const float* __restrict__
 }
 
 __global__ void __launch_bounds__(256)
-    preprocess_bwd_kernel(PreParams p, const int* __restrict__ radii, const uint8_t* __restrict__ clamped,
+    preprocess_bwd_kernel(PreParams p, const uint32_t* __restrict__ visible_ids,
+                          const unsigned long long* __restrict__ visible_count, const uint8_t* __restrict__ clamped,
                           const float* __restrict__ dmean2D, const float* __restrict__ dconic,
                           const float* __restrict__ dcolor, float* __restrict__ dopac, float* __restrict__ dmean3D,
                           float* __restrict__ dcov3D, float* __restrict__ dsh, float* __restrict__ dscale,
                           float* __restrict__ drot, int consistent)
 {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= p.P) return;
-    const bool live = radii[idx] > 0;
+    // The forward's depth ordering put the V visible Gaussians first; culled
+    // rows were zero-filled by the launcher.
+    const uint32_t V = (uint32_t)*visible_count;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < V; j += gridDim.x * blockDim.x) {
+    const int idx = (int)visible_ids[j];
     float3 dm = {0.f, 0.f, 0.f};
     float dc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (live) {
+    {
         const float3 mean = {p.means[3 * idx], p.means[3 * idx + 1], p.means[3 * idx + 2]};
         float cov3D[6];
         if (p.cov3D) {
@@ -276,20 +281,13 @@ __global__ void __launch_bounds__(256)
             dr[0] = dq.x; dr[1] = dq.y; dr[2] = dq.z; dr[3] = dq.w;
         }
         if (consistent && p.opac && p.opac[idx] < 1e-6f) dopac[idx] = 0.f;
-    } else {
-        if (p.shs && dsh)
-            for (int f = 0; f < p.M * 3; f++) dsh[(size_t)idx * p.M * 3 + f] = 0.f;
-        if (p.scales && dscale) {
-            dscale[3 * (size_t)idx] = dscale[3 * (size_t)idx + 1] = dscale[3 * (size_t)idx + 2] = 0.f;
-            float* dr = drot + 4 * (size_t)idx;
-            dr[0] = dr[1] = dr[2] = dr[3] = 0.f;
-        }
     }
     dmean3D[3 * idx] = dm.x;
     dmean3D[3 * idx + 1] = dm.y;
     dmean3D[3 * idx + 2] = dm.z;
 #pragma unroll
     for (int k = 0; k < 6; k++) dcov3D[6 * (size_t)idx + k] = dc[k];
+    }
 }
 
 }  // namespace
@@ -298,9 +296,21 @@ void launch_preprocess_bwd(const PreParams& p, const int* radii, const GeomState
                            const float* dconic, const float* dcolor, float* dopac, float* dmean3D, float* dcov3D,
                            float* dsh, float* dscale, float* drot, int consistent, cudaStream_t s)
 {
+    (void)radii;
     if (p.P <= 0) return;
-    preprocess_bwd_kernel<<<(p.P + 255) / 256, 256, 0, s>>>(p, radii, g.clamped, dmean2D, dconic, dcolor, dopac,
-                                                             dmean3D, dcov3D, dsh, dscale, drot, consistent);
+    // Dense outputs: culled rows are zero, written here at copy-engine speed.
+    const size_t P = (size_t)p.P;
+    cudaMemsetAsync(dmean3D, 0, sizeof(float) * 3 * P, s);
+    cudaMemsetAsync(dcov3D, 0, sizeof(float) * 6 * P, s);
+    if (dsh) cudaMemsetAsync(dsh, 0, sizeof(float) * 3 * (size_t)p.M * P, s);
+    if (dscale) cudaMemsetAsync(dscale, 0, sizeof(float) * 3 * P, s);
+    if (drot) cudaMemsetAsync(drot, 0, sizeof(float) * 4 * P, s);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = (int)std::min<size_t>((P + 255) / 256, (size_t)sms * 8);
+    preprocess_bwd_kernel<<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dmean2D, dconic, dcolor,
+                                                 dopac, dmean3D, dcov3D, dsh, dscale, drot, consistent);
     note_launches(1);
 }
 

@@ -657,4 +657,20 @@ int fgs_profile_read(double* ms, long long* calls, int reset)
 
 long long fgs_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
+int fgs_set_render_config(int fwd_ppt, int fwd_batch, int bwd_ppt, int bwd_batch)
+{
+    const RenderConfig c{fwd_ppt, fwd_batch, bwd_ppt, bwd_batch};
+    if (!valid_render_config(c)) return FGS_ERR_ARG;
+    set_render_config(c);
+    return FGS_OK;
+}
+
+int fgs_get_render_config(int* cfg)
+{
+    if (!cfg) return FGS_ERR_ARG;
+    const RenderConfig c = get_render_config();
+    cfg[0] = c.fwd_ppt; cfg[1] = c.fwd_batch; cfg[2] = c.bwd_ppt; cfg[3] = c.bwd_batch;
+    return FGS_OK;
+}
+
 }  // extern "C"

@@ -109,6 +109,14 @@ void launch_visibility_radius(int P, const float* means, const float* lscales, c
 // be absent in backward).
 int make_params(const fgs_raster_args* a, PreParams& p, bool backward = false);
 
+// Render kernel shape: pixels per thread {1,2,4} and records per shared-memory batch {64,128,256}.
+struct RenderConfig {
+    int fwd_ppt, fwd_batch, bwd_ppt, bwd_batch;
+};
+bool valid_render_config(const RenderConfig& c);
+void set_render_config(const RenderConfig& c);
+RenderConfig get_render_config();
+
 // Kernel-launch accounting (fgs_launch_count) and per-stage event timing.
 void note_launches(int n);
 struct StageTimer {

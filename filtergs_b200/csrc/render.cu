@@ -20,7 +20,6 @@ namespace fgs {
 
 namespace {
 
-constexpr int kBatch = 256;
 constexpr int kBufs = 3;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
@@ -81,6 +80,38 @@ __device__ __forceinline__ void issue_batch(PairRecord* sbuf, uint64_t* bar, con
     bulk_g2s(sbuf, recs + first, bytes, bar);
 }
 
+// Reduce 9 per-lane values over the warp with 16 shuffles instead of 45:
+// a butterfly in which each level halves the values a lane keeps (the rest
+// go to the partner lane).  Lanes 2s and 2s+1 end with the warp total of
+// value s (s < 9; padded to 16 slots).
+__device__ __forceinline__ float warp_transpose_sum9(const float (&g)[9])
+{
+    const unsigned lane = threadIdx.x & 31;
+    float v[8];
+    {
+        const bool hi = lane & 16;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const float lo_v = g[i];
+            const float hi_v = (i + 8 < 9) ? g[i + 8] : 0.f;
+            const float send = hi ? lo_v : hi_v;
+            const float keep = hi ? hi_v : lo_v;
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+    }
+#pragma unroll
+    for (int w = 4, o = 8; w >= 1; w >>= 1, o >>= 1) {
+        const bool hi = lane & o;
+#pragma unroll
+        for (int i = 0; i < w; i++) {
+            const float send = hi ? v[i] : v[i + w];
+            const float keep = hi ? v[i + w] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
 __device__ __forceinline__ float warp_sum(float v)
 {
 #pragma unroll
@@ -89,7 +120,7 @@ __device__ __forceinline__ float warp_sum(float v)
 }
 
 // ---------------------------------------------------------------- forward
-template <int PPT>
+template <int PPT, int kBatch>
 __global__ void __launch_bounds__(256 / PPT)
     render_fwd_kernel(const uint2* __restrict__ ranges, const PairRecord* __restrict__ recs, int W, int H,
                       const float* __restrict__ bg, float* __restrict__ out_color, float* __restrict__ final_T,
@@ -270,7 +301,7 @@ __global__ void __launch_bounds__(256 / PPT)
 }
 
 // ---------------------------------------------------------------- backward
-template <int PPT>
+template <int PPT, int kBatch>
 __global__ void __launch_bounds__(256 / PPT)
     render_bwd_kernel(const uint2* __restrict__ ranges, const PairRecord* __restrict__ recs, int W, int H,
                       const float* __restrict__ bg, const float* __restrict__ final_Ts,
@@ -395,12 +426,9 @@ __global__ void __launch_bounds__(256 / PPT)
                 any = true;
             }
             if (__any_sync(0xffffffffu, any)) {
-#pragma unroll
-                for (int q = 0; q < NG; q++) g[q] = warp_sum(g[q]);
-                if ((tid & 31) == 0) {
-#pragma unroll
-                    for (int q = 0; q < NG; q++) atomicAdd(&s_acc[q][j], g[q]);
-                }
+                const float tot = warp_transpose_sum9(g);
+                const unsigned lane = tid & 31;
+                if (!(lane & 1) && (lane >> 1) < NG) atomicAdd(&s_acc[lane >> 1][j], tot);
             }
         }
         __syncthreads();
@@ -433,15 +461,59 @@ __global__ void __launch_bounds__(256 / PPT)
 
 }  // namespace
 
+namespace {
+RenderConfig g_cfg{2, 256, 2, 256};
+
+template <int PPT, int B>
+void fwd_launch(int grid, const ImageState& im, const BinState& b, int W, int H, const float* bg, float* out_color,
+                int* point_id, float* pw_pixel, float* point_weight, bool stats, unsigned* err, cudaStream_t s)
+{
+    render_fwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(im.ranges, b.rec, W, H, bg, out_color, im.final_T,
+                                                          im.n_contrib, point_id, pw_pixel, point_weight,
+                                                          stats ? b.kv_sum : nullptr, stats ? b.kv_cnt : nullptr, err);
+}
+
+template <int PPT, int B>
+void bwd_launch(int grid, const ImageState& im, const BinState& b, int W, int H, const float* bg, const float* dL,
+                float* dmean2D, float* dconic, float* dopac, float* dcolor, int consistent, unsigned* err,
+                cudaStream_t s)
+{
+    render_bwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(im.ranges, b.rec, W, H, bg, im.final_T, im.n_contrib, dL,
+                                                          dmean2D, dconic, dopac, dcolor, consistent, err);
+}
+
+#define FGS_RENDER_DISPATCH(FN, PPT_, B_, ...)                                            \
+    do {                                                                                  \
+        const int ppt_ = (PPT_), b_ = (B_);                                               \
+        if (ppt_ == 1 && b_ == 64) FN<1, 64>(__VA_ARGS__);                                \
+        else if (ppt_ == 1 && b_ == 128) FN<1, 128>(__VA_ARGS__);                         \
+        else if (ppt_ == 1) FN<1, 256>(__VA_ARGS__);                                      \
+        else if (ppt_ == 2 && b_ == 64) FN<2, 64>(__VA_ARGS__);                           \
+        else if (ppt_ == 2 && b_ == 128) FN<2, 128>(__VA_ARGS__);                         \
+        else if (ppt_ == 2) FN<2, 256>(__VA_ARGS__);                                      \
+        else if (ppt_ == 4 && b_ == 64) FN<4, 64>(__VA_ARGS__);                           \
+        else if (ppt_ == 4 && b_ == 128) FN<4, 128>(__VA_ARGS__);                         \
+        else FN<4, 256>(__VA_ARGS__);                                                     \
+    } while (0)
+}  // namespace
+
+bool valid_render_config(const RenderConfig& c)
+{
+    auto ok_p = [](int v) { return v == 1 || v == 2 || v == 4; };
+    auto ok_b = [](int v) { return v == 64 || v == 128 || v == 256; };
+    return ok_p(c.fwd_ppt) && ok_p(c.bwd_ppt) && ok_b(c.fwd_batch) && ok_b(c.bwd_batch);
+}
+void set_render_config(const RenderConfig& c) { g_cfg = c; }
+RenderConfig get_render_config() { return g_cfg; }
+
 void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, const float* bg, float* out_color,
                        int* point_id, float* pw_pixel, float* point_weight, bool stats, unsigned* err,
                        cudaStream_t s)
 {
     const int gx = (W + kTileX - 1) / kTileX, gy = (H + kTileY - 1) / kTileY;
-    constexpr int PPT = 2;
-    render_fwd_kernel<PPT><<<gx * gy, 256 / PPT, 0, s>>>(im.ranges, b.rec, W, H, bg, out_color, im.final_T,
-                                                          im.n_contrib, point_id, pw_pixel, point_weight,
-                                                          stats ? b.kv_sum : nullptr, stats ? b.kv_cnt : nullptr, err);
+    const RenderConfig c = g_cfg;
+    FGS_RENDER_DISPATCH(fwd_launch, c.fwd_ppt, c.fwd_batch, gx * gy, im, b, W, H, bg, out_color, point_id, pw_pixel,
+                        point_weight, stats, err, s);
     note_launches(1);
 }
 
@@ -450,9 +522,9 @@ void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, co
                        int consistent, unsigned* err, cudaStream_t s)
 {
     const int gx = (W + kTileX - 1) / kTileX, gy = (H + kTileY - 1) / kTileY;
-    constexpr int PPT = 2;
-    render_bwd_kernel<PPT><<<gx * gy, 256 / PPT, 0, s>>>(im.ranges, b.rec, W, H, bg, im.final_T, im.n_contrib,
-                                                          dL_dpix, dmean2D, dconic, dopac, dcolor, consistent, err);
+    const RenderConfig c = g_cfg;
+    FGS_RENDER_DISPATCH(bwd_launch, c.bwd_ppt, c.bwd_batch, gx * gy, im, b, W, H, bg, dL_dpix, dmean2D, dconic, dopac,
+                        dcolor, consistent, err, s);
     note_launches(1);
 }
 

@@ -186,6 +186,13 @@ int fgs_forward_noalloc(const fgs_raster_args *a, int *radii, float *out_color, 
 #define FGS_STAGE_PREPROCESS_BWD 8
 #define FGS_NUM_STAGES 9
 int fgs_profile_enable(int on);
+/* Render kernel shape used by forward/backward in this process (no reference
+ * counterpart; the reference hard-codes one pixel per thread and 256-record
+ * batches): pixels per thread 1|2|4 and shared-memory batch 64|128|256 for
+ * each of the forward and backward compositing kernels.  Chosen by the
+ * autotuner (filtergs_b200/autotune.py).  cfg: int[4] out.             */
+int fgs_set_render_config(int fwd_ppt, int fwd_batch, int bwd_ppt, int bwd_batch);
+int fgs_get_render_config(int *cfg);
 int fgs_profile_read(double *ms, long long *calls, int reset);
 long long fgs_launch_count(void);
 
