@@ -119,6 +119,42 @@ __device__ __forceinline__ float warp_sum(float v)
     return v;
 }
 
+// Conservative test used to skip (warp, record) pairs: can a Gaussian with mean
+// (mx, my), conic (a, b, c) and opacity o reach alpha >= 1/255 at any pixel
+// centre of [x0,x1] x [y0,y1]?  alpha <= o (power <= 0), so o < 1/255 never
+// contributes; otherwise alpha >= 1/255 needs Q = a dx^2 + 2b dx dy + c dy^2
+// <= 2 ln(255 o), and Q's minimum over the rectangle is 0 when the mean is
+// inside, else on the boundary (one clamped 1-D minimum per edge).  The margin
+// covers float rounding of the per-pixel evaluation by a wide factor; a
+// non-positive-definite conic is never skipped.  Skipping only removes work
+// that the per-pixel tests would reject, so every output is unchanged.
+__device__ __forceinline__ bool may_touch(float mx, float my, float a, float b, float c, float o, float x0, float x1,
+                                          float y0, float y1)
+{
+    if (!(o >= 1.0f / 255.0f)) return false;
+    if (!(a > 0.f && c > 0.f && a * c - b * b > 0.f)) return true;
+    const float X0 = x0 - mx, X1 = x1 - mx, Y0 = y0 - my, Y1 = y1 - my;
+    if (X0 <= 0.f && X1 >= 0.f && Y0 <= 0.f && Y1 >= 0.f) return true;
+    const float thr = 2.f * __logf(255.f * o);
+    float q = 3.4e38f;
+    // edges x = X0, X1
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const float X = i ? X1 : X0;
+        const float dy = fminf(fmaxf(-b * X / c, Y0), Y1);
+        q = fminf(q, a * X * X + 2.f * b * X * dy + c * dy * dy);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        const float Y = i ? Y1 : Y0;
+        const float dx = fminf(fmaxf(-b * Y / a, X0), X1);
+        q = fminf(q, a * dx * dx + 2.f * b * dx * Y + c * Y * Y);
+    }
+    const float mX = fmaxf(fabsf(X0), fabsf(X1)), mY = fmaxf(fabsf(Y0), fabsf(Y1));
+    const float mag = a * mX * mX + c * mY * mY + 2.f * fabsf(b) * mX * mY;
+    return q <= thr + 0.05f + 1e-5f * mag;
+}
+
 // ---------------------------------------------------------------- forward
 template <int PPT, int kBatch>
 __global__ void __launch_bounds__(256 / PPT)
@@ -178,6 +214,9 @@ __global__ void __launch_bounds__(256 / PPT)
         pyf[k] = (float)py;
     }
     const float pxf = (float)px;
+    // this warp's pixel rectangle: 16 columns x 2*PPT rows
+    const float rx0 = (float)(bx * kTileX), rx1 = rx0 + (kTileX - 1);
+    const float ry0 = (float)(by * kTileY + (tid >> 5) * 2 * PPT), ry1 = ry0 + (2 * PPT - 1);
     bool all_done = true;
 #pragma unroll
     for (int k = 0; k < PPT; k++) all_done = all_done && done[k];
@@ -191,60 +230,76 @@ __global__ void __launch_bounds__(256 / PPT)
         const PairRecord* R = s_rec[buf];
         const bool warp_live = !__all_sync(0xffffffffu, all_done);
         if (warp_live) {
-            for (uint32_t j = 0; j < cnt; j++) {
-                if (__all_sync(0xffffffffu, all_done)) break;
-                const uint32_t position = contributor + j + 1;
-                const float4 ra = R[j].a;
-                const float4 rb = R[j].b;
-                float wj = 0.f, ksum = 0.f;
-                uint32_t kc = 0;
-#pragma unroll
-                for (int k = 0; k < PPT; k++) {
-                    if (done[k]) continue;
-                    const float2 d = {ra.x - pxf, ra.y - pyf[k]};
-                    const float power = -0.5f * (ra.z * d.x * d.x + rb.x * d.y * d.y) - ra.w * d.x * d.y;
-                    if (power > 0.0f) continue;
-                    const float alpha = min(0.99f, rb.y * exp(power));
-                    if (alpha < 1.0f / 255.0f) continue;
-                    const float test_T = T[k] * (1 - alpha);
-                    if (test_T < 0.0001f) {
-                        done[k] = true;
-                        continue;
-                    }
-                    const float4 rc = R[j].c;
-                    C[k][0] += rb.z * alpha * T[k];
-                    C[k][1] += rb.w * alpha * T[k];
-                    C[k][2] += rc.x * alpha * T[k];
-                    const float w = T[k] * alpha;
-                    if (w > wmax[k]) {
-                        wmax[k] = w;
-                        maxid[k] = __float_as_int(rc.y);
-                    }
-                    wj = fmaxf(wj, w);
-                    ksum += w;
-                    kc += 1;
-                    T[k] = test_T;
-                    last[k] = position;
+            bool stop = false;
+            for (uint32_t k0 = 0; k0 < cnt && !stop; k0 += 32) {
+                // which of these 32 records can reach alpha >= 1/255 inside this warp's pixels
+                const uint32_t e = k0 + (tid & 31);
+                bool t = false;
+                if (e < cnt) {
+                    const float4 ea = R[e].a, eb = R[e].b;
+                    t = may_touch(ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, rx0, rx1, ry0, ry1);
                 }
-                bool ad = true;
+                uint32_t live = __ballot_sync(0xffffffffu, t);
+                while (live) {
+                    const uint32_t j = k0 + (uint32_t)(__ffs(live) - 1);
+                    live &= live - 1;
+                    const uint32_t position = contributor + j + 1;
+                    const float4 ra = R[j].a;
+                    const float4 rb = R[j].b;
+                    float wj = 0.f, ksum = 0.f;
+                    uint32_t kc = 0;
 #pragma unroll
-                for (int k = 0; k < PPT; k++) ad = ad && done[k];
-                all_done = ad;
-                // per-Gaussian max weight (and statistics): warp, then CTA
-                if (__any_sync(0xffffffffu, wj > 0.f)) {
-                    const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(wj));
-                    float ks = 0.f;
-                    uint32_t kcs = 0;
-                    if (stats) {
-                        ks = warp_sum(ksum);
-                        kcs = __reduce_add_sync(0xffffffffu, kc);
-                    }
-                    if ((tid & 31) == 0) {
-                        atomicMax(&s_wmax[acc][j], wm);
-                        if (stats) {
-                            atomicAdd(&s_ksum[acc][j], ks);
-                            atomicAdd(&s_kcnt[acc][j], kcs);
+                    for (int k = 0; k < PPT; k++) {
+                        if (done[k]) continue;
+                        const float2 d = {ra.x - pxf, ra.y - pyf[k]};
+                        const float power = -0.5f * (ra.z * d.x * d.x + rb.x * d.y * d.y) - ra.w * d.x * d.y;
+                        if (power > 0.0f) continue;
+                        const float alpha = min(0.99f, rb.y * exp(power));
+                        if (alpha < 1.0f / 255.0f) continue;
+                        const float test_T = T[k] * (1 - alpha);
+                        if (test_T < 0.0001f) {
+                            done[k] = true;
+                            continue;
                         }
+                        const float4 rc = R[j].c;
+                        C[k][0] += rb.z * alpha * T[k];
+                        C[k][1] += rb.w * alpha * T[k];
+                        C[k][2] += rc.x * alpha * T[k];
+                        const float w = T[k] * alpha;
+                        if (w > wmax[k]) {
+                            wmax[k] = w;
+                            maxid[k] = __float_as_int(rc.y);
+                        }
+                        wj = fmaxf(wj, w);
+                        ksum += w;
+                        kc += 1;
+                        T[k] = test_T;
+                        last[k] = position;
+                    }
+                    bool ad = true;
+#pragma unroll
+                    for (int k = 0; k < PPT; k++) ad = ad && done[k];
+                    all_done = ad;
+                    // per-Gaussian max weight (and statistics): warp, then CTA
+                    if (__any_sync(0xffffffffu, wj > 0.f)) {
+                        const uint32_t wm = __reduce_max_sync(0xffffffffu, __float_as_uint(wj));
+                        float ks = 0.f;
+                        uint32_t kcs = 0;
+                        if (stats) {
+                            ks = warp_sum(ksum);
+                            kcs = __reduce_add_sync(0xffffffffu, kc);
+                        }
+                        if ((tid & 31) == 0) {
+                            atomicMax(&s_wmax[acc][j], wm);
+                            if (stats) {
+                                atomicAdd(&s_ksum[acc][j], ks);
+                                atomicAdd(&s_kcnt[acc][j], kcs);
+                            }
+                        }
+                    }
+                    if (__all_sync(0xffffffffu, all_done)) {
+                        stop = true;
+                        break;
                     }
                 }
             }
@@ -349,6 +404,8 @@ __global__ void __launch_bounds__(256 / PPT)
         pyf[k] = (float)py;
     }
     const float pxf = (float)px;
+    const float rx0 = (float)(bx * kTileX), rx1 = rx0 + (kTileX - 1);
+    const float ry0 = (float)(by * kTileY + (tid >> 5) * 2 * PPT), ry1 = ry0 + (2 * PPT - 1);
     const float ddelx_dx = 0.5 * W;
     const float ddely_dy = 0.5 * H;
 
@@ -359,8 +416,8 @@ __global__ void __launch_bounds__(256 / PPT)
     }
     for (int e = tid; e < NG * kBatch; e += NT) (&s_acc[0][0])[e] = 0.f;
     __syncthreads();
-    const uint32_t wm = __reduce_max_sync(0xffffffffu, my_max);
-    if ((tid & 31) == 0) atomicMax(&s_max_last, wm);
+    const uint32_t warp_last = __reduce_max_sync(0xffffffffu, my_max);
+    if ((tid & 31) == 0) atomicMax(&s_max_last, warp_last);
     __syncthreads();
     // Entries at or beyond the largest n_contrib of the tile touch no pixel.
     const uint32_t n = min(range.y - range.x, s_max_last);
@@ -379,56 +436,70 @@ __global__ void __launch_bounds__(256 / PPT)
         const uint32_t cnt = hi - lo;
         mbar_wait(&s_bar[buf], (uint32_t)((b / kBufs) & 1), err);
         const PairRecord* R = s_rec[buf];
-        for (int j = (int)cnt - 1; j >= 0; j--) {
-            const uint32_t contributor = lo + (uint32_t)j;  // 0-based position in the tile list
-            const float4 ra = R[j].a;
-            const float4 rb = R[j].b;
-            float g[NG];
-#pragma unroll
-            for (int q = 0; q < NG; q++) g[q] = 0.f;
-            bool any = false;
-#pragma unroll
-            for (int k = 0; k < PPT; k++) {
-                if (contributor >= last[k]) continue;
-                const float2 d = {ra.x - pxf, ra.y - pyf[k]};
-                const float power = -0.5f * (ra.z * d.x * d.x + rb.x * d.y * d.y) - ra.w * d.x * d.y;
-                if (power > 0.0f) continue;
-                const float G = exp(power);
-                const float alpha = min(0.99f, rb.y * G);
-                if (alpha < 1.0f / 255.0f) continue;
-                T[k] = T[k] / (1.f - alpha);
-                const float dchannel_dcolor = alpha * T[k];
-                const float col[3] = {rb.z, rb.w, R[j].c.x};
-                float dL_dalpha = 0.0f;
-#pragma unroll
-                for (int ch = 0; ch < 3; ch++) {
-                    const float c = col[ch];
-                    accum[k][ch] = last_alpha[k] * last_color[k][ch] + (1.f - last_alpha[k]) * accum[k][ch];
-                    last_color[k][ch] = c;
-                    dL_dalpha += (c - accum[k][ch]) * dpix[k][ch];
-                    g[ch] += dchannel_dcolor * dpix[k][ch];
-                }
-                dL_dalpha *= T[k];
-                last_alpha[k] = alpha;
-                dL_dalpha += (-T_final[k] / (1.f - alpha)) * bg_dot[k];
-                if (consistent && rb.y * G > 0.99f) dL_dalpha = 0.f;
-                const float dL_dG = rb.y * dL_dalpha;
-                const float gdx = G * d.x;
-                const float gdy = G * d.y;
-                const float dG_ddelx = -gdx * ra.z - gdy * ra.w;
-                const float dG_ddely = -gdy * rb.x - gdx * ra.w;
-                g[3] += dL_dG * dG_ddelx * ddelx_dx;
-                g[4] += dL_dG * dG_ddely * ddely_dy;
-                g[5] += -0.5f * gdx * d.x * dL_dG;
-                g[6] += -0.5f * gdx * d.y * dL_dG;
-                g[7] += -0.5f * gdy * d.y * dL_dG;
-                g[8] += G * dL_dalpha;
-                any = true;
+        for (int k0 = (int)((cnt - 1) & ~31u); k0 >= 0; k0 -= 32) {
+            // records of this chunk that sit before some pixel's last contributor and can
+            // reach alpha >= 1/255 inside this warp's pixels, walked back to front
+            const uint32_t e = (uint32_t)k0 + (tid & 31);
+            bool t = false;
+            if (e < cnt && lo + e < warp_last) {
+                const float4 ea = R[e].a, eb = R[e].b;
+                t = may_touch(ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, rx0, rx1, ry0, ry1);
             }
-            if (__any_sync(0xffffffffu, any)) {
-                const float tot = warp_transpose_sum9(g);
-                const unsigned lane = tid & 31;
-                if (!(lane & 1) && (lane >> 1) < NG) atomicAdd(&s_acc[lane >> 1][j], tot);
+            uint32_t live = __ballot_sync(0xffffffffu, t);
+            while (live) {
+                const int bit = 31 - __clz(live);
+                live &= ~(1u << bit);
+                const int j = k0 + bit;
+                const uint32_t contributor = lo + (uint32_t)j;  // 0-based position in the tile list
+                const float4 ra = R[j].a;
+                const float4 rb = R[j].b;
+                float g[NG];
+#pragma unroll
+                for (int q = 0; q < NG; q++) g[q] = 0.f;
+                bool any = false;
+#pragma unroll
+                for (int k = 0; k < PPT; k++) {
+                    if (contributor >= last[k]) continue;
+                    const float2 d = {ra.x - pxf, ra.y - pyf[k]};
+                    const float power = -0.5f * (ra.z * d.x * d.x + rb.x * d.y * d.y) - ra.w * d.x * d.y;
+                    if (power > 0.0f) continue;
+                    const float G = exp(power);
+                    const float alpha = min(0.99f, rb.y * G);
+                    if (alpha < 1.0f / 255.0f) continue;
+                    T[k] = T[k] / (1.f - alpha);
+                    const float dchannel_dcolor = alpha * T[k];
+                    const float col[3] = {rb.z, rb.w, R[j].c.x};
+                    float dL_dalpha = 0.0f;
+#pragma unroll
+                    for (int ch = 0; ch < 3; ch++) {
+                        const float c = col[ch];
+                        accum[k][ch] = last_alpha[k] * last_color[k][ch] + (1.f - last_alpha[k]) * accum[k][ch];
+                        last_color[k][ch] = c;
+                        dL_dalpha += (c - accum[k][ch]) * dpix[k][ch];
+                        g[ch] += dchannel_dcolor * dpix[k][ch];
+                    }
+                    dL_dalpha *= T[k];
+                    last_alpha[k] = alpha;
+                    dL_dalpha += (-T_final[k] / (1.f - alpha)) * bg_dot[k];
+                    if (consistent && rb.y * G > 0.99f) dL_dalpha = 0.f;
+                    const float dL_dG = rb.y * dL_dalpha;
+                    const float gdx = G * d.x;
+                    const float gdy = G * d.y;
+                    const float dG_ddelx = -gdx * ra.z - gdy * ra.w;
+                    const float dG_ddely = -gdy * rb.x - gdx * ra.w;
+                    g[3] += dL_dG * dG_ddelx * ddelx_dx;
+                    g[4] += dL_dG * dG_ddely * ddely_dy;
+                    g[5] += -0.5f * gdx * d.x * dL_dG;
+                    g[6] += -0.5f * gdx * d.y * dL_dG;
+                    g[7] += -0.5f * gdy * d.y * dL_dG;
+                    g[8] += G * dL_dalpha;
+                    any = true;
+                }
+                if (__any_sync(0xffffffffu, any)) {
+                    const float tot = warp_transpose_sum9(g);
+                    const unsigned lane = tid & 31;
+                    if (!(lane & 1) && (lane >> 1) < NG) atomicAdd(&s_acc[lane >> 1][j], tot);
+                }
             }
         }
         __syncthreads();
