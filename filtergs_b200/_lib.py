@@ -65,6 +65,14 @@ SIGNATURES = {
     "fgs_launch_count": (i64, []),
     "fgs_noalloc_capacity_bytes": (sz, []),
     "fgs_set_render_config": (i32, [i32, i32, i32, i32]),
+    "fgs_gather_attributes": (i32, [i64, vp, vp, vp, vp, vp, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, vp]),
+    "fgs_compact_scratch_bytes": (sz, [i32]),
+    "fgs_compact_mask": (i32, [i32, vp, vp, vp, vp, vp]),
+    "fgs_gather_activate": (i32, [i64, vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, vp]),
+    "fgs_radius_raw": (i32, [i32, vp, vp, vp, vp, vp, f32, f32, f32, f32, vp, vp]),
+    "fgs_log_cut_scratch_bytes": (sz, [i32, i32, i32, i32]),
+    "fgs_log_cut": (i32, [i32, vp, i32, vp, vp, i32, vp, f32, i32, vp, vp, vp, vp]),
+    "fgs_cull": (i32, [vp, vp, i32, vp, vp, f32, vp, vp, vp, vp]),
     "fgs_get_render_config": (i32, [vp]),
     "fgs_forward_noalloc": (i32, [C.POINTER(RasterArgs), vp, vp, vp, vp, vp, C.POINTER(i64), vp]),
 }

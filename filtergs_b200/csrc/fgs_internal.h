@@ -117,6 +117,27 @@ bool valid_render_config(const RenderConfig& c);
 void set_render_config(const RenderConfig& c);
 RenderConfig get_render_config();
 
+// LoD selection and gather (lod.cu)
+void launch_compact(const uint8_t* mask, uint32_t n, int64_t* out, unsigned long long* count, uint32_t* scratch,
+                    unsigned* err, cudaStream_t s);
+void launch_gather(const int64_t* index, long long N, const float* xyz, const float* scaling, const float* rotation,
+                   const float* opacity, const float* colors, const float* shs, int sh_floats, float* o_xyz,
+                   float* o_scaling, float* o_rotation, float* o_opacity, float* o_colors, float* o_shs,
+                   cudaStream_t s);
+void launch_gather_activate(const int64_t* index, const unsigned long long* count, long long N_cap, const float* xyz,
+                            const float* log_scale, const float* rot, const float* opac_raw, const float* dc,
+                            const float* rest, int deg, int rest_coeffs, const float* campos, float* o_xyz,
+                            float* o_scale, float* o_rot, float* o_opac, float* o_rgb, cudaStream_t s);
+void launch_radius_raw(int P, const float* means, const float* lscales, const float* rots, const float* view,
+                       const float* proj, float fx, float fy, float tanx, float tany, float* radius, cudaStream_t s);
+size_t log_cut_scratch_words(int P, int nroots, int max_child, int levels);
+void launch_log_cut(int P, const int32_t* roots, int nroots, const int32_t* node_index, const int32_t* tree,
+                    int max_child, const float* radius, float min_res, int levels, int32_t* out, uint32_t* scratch,
+                    unsigned* err, cudaStream_t s);
+void launch_cull(const int32_t* in, const uint32_t* n_in, uint32_t cap, const float* radius, const float* opac_raw,
+                 float min_px, int64_t* out, unsigned long long* n_out, uint32_t* scratch, unsigned* err,
+                 cudaStream_t s);
+
 // Kernel-launch accounting (fgs_launch_count) and per-stage event timing.
 void note_launches(int n);
 struct StageTimer {

@@ -77,6 +77,11 @@ def aerial_camera(rng, W=1920, H=1080, fx=1600.0, altitude=150.0, pitch_deg=45.0
     return Camera(look_rotation(fwd), center, fx, fy, W, H, znear, zfar)
 
 
+def look_at_camera(center, target, W=1920, H=1080, fx=1600.0, znear=0.1, zfar=2000.0):
+    fwd = np.asarray(target, np.float64) - np.asarray(center, np.float64)
+    return Camera(look_rotation(fwd), center, fx, fx, W, H, znear, zfar)
+
+
 def identity_camera(W=256, H=256, fx=300.0, fy=300.0, znear=0.01, zfar=100.0):
     return Camera(np.eye(3), np.zeros(3), fx, fy, W, H, znear, zfar)
 

@@ -134,6 +134,49 @@ int fgs_visibility_radius(int P, const float *means3D, const float *log_scales, 
                           float radius_filter_threshold, uint8_t *mask, float *radius2d, float *depth,
                           void *stream);
 
+/* ------------------------------------------------------------------ LoD selection and gather
+ * gather_attributes_cuda (FilterGS/cuda/gather_attributes_kernel.cu:70-145): rows of xyz/scaling [.,3],
+ * rotation [.,4] (16-byte aligned), opacity [.,1], colors [.,3] and optional shs [., sh_coeffs, sh_channels]
+ * at index[0..N) (int64) into the o_* outputs.                                                       */
+int fgs_gather_attributes(long long N, const int64_t *index, const float *xyz, const float *scaling,
+                          const float *rotation, const float *opacity, const float *colors, const float *shs,
+                          int sh_coeffs, int sh_channels, float *o_xyz, float *o_scaling, float *o_rotation,
+                          float *o_opacity, float *o_colors, float *o_shs, void *stream);
+/* torch.nonzero(mask) of FilterGS/filtergs.py:64 without the host sync: ordered int64 indices of the
+ * nonzero bytes of mask[n]; the count stays on the device (*count, u64).  scratch:
+ * fgs_compact_scratch_bytes(n) bytes, 4-byte aligned.                                                 */
+size_t fgs_compact_scratch_bytes(int n);
+int fgs_compact_mask(int n, const uint8_t *mask, int64_t *out_index, unsigned long long *count, void *scratch,
+                     void *stream);
+/* FilterGS get_all (FilterGS/filtergs.py:98-134) fused: gather index[0..min(N_cap, *count_dev)) and
+ * apply LoG/model/activation.py:36-43 -- exp(scale), sigmoid(opacity), F.normalize(rotation),
+ * SH2RGB(features_dc) + eval_sh_wobase(shs_rest, sh_degree) (LoG/model/sh_utils.py:31-74).
+ * count_dev may be null (then N_cap rows).                                                           */
+int fgs_gather_activate(long long N_cap, const int64_t *index, const unsigned long long *count_dev,
+                        const float *xyz, const float *log_scale, const float *rotation, const float *opacity_raw,
+                        const float *features_dc, const float *shs_rest, int sh_degree, int rest_coeffs,
+                        const float *campos, float *o_xyz, float *o_scaling, float *o_rotation, float *o_opacity,
+                        float *o_colors, void *stream);
+/* The LoG node radius (LoG/model/level_of_gaussian.py:66-88 -> compute_radius_kernel_v2.cu:180-229)
+ * from raw parameters: exp(log_scales) and the normalised quaternion are applied in the kernel.        */
+int fgs_radius_raw(int P, const float *means3D, const float *log_scales, const float *rotations,
+                   const float *viewmatrix, const float *projmatrix, float focal_x, float focal_y, float tan_fovx,
+                   float tan_fovy, float *radius, void *stream);
+/* TensorTree.traverse (LoG/model/tensor_tree.py:133-187) on the device: node ids of the cut in the
+ * reference's order (kept roots, then each level's kept children in frontier order) into out[P]; the
+ * count to *out_count_dev (u32, device).  tree: [num_internal, max_child] child ids (-1 = none);
+ * levels = the deepest level to expand (the reference stops at 30).  No host synchronisation.
+ * scratch: fgs_log_cut_scratch_bytes(...) bytes.                                                     */
+size_t fgs_log_cut_scratch_bytes(int P, int num_roots, int max_child, int levels);
+int fgs_log_cut(int P, const int32_t *roots, int num_roots, const int32_t *node_index, const int32_t *tree,
+                int max_child, const float *radius, float min_resolution_pixel, int levels, int32_t *out,
+                uint32_t *out_count_dev, void *scratch, void *stream);
+/* Redundancy culling of a node list (no reference counterpart): keep ids[i] (i < *count_dev) with
+ * radius >= min_px and sigmoid(opacity_raw) >= 1/255, order preserved, as int64 into out; count to
+ * *out_count_dev.  scratch: fgs_compact_scratch_bytes(cap) bytes.                                   */
+int fgs_cull(const int32_t *ids, const uint32_t *count_dev, int cap, const float *radius, const float *opacity_raw,
+             float min_px, int64_t *out, unsigned long long *out_count_dev, void *scratch, void *stream);
+
 /* ------------------------------------------------------------------ test accessors
  * Sorted (tile|depth) keys and Gaussian ids of a forward, in the reference's
  * 64-bit key format (rasterizer_impl.cu:139-141).  keys/vals: [num_rendered]. */

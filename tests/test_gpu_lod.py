@@ -1,0 +1,157 @@
+"""GPU parity of the LoD selection path: the FilterGS visibility mask and radii
+bit-exact against the reference build (oracle/_ref/ref_compute_radius_v2.so),
+the gather bit-exact against ref_gather_attributes.so, the device LoG cut in
+TensorTree.traverse order against the C oracle, culling and activation against
+the oracle, and the selected-set render against the reference rasterizer."""
+import numpy as np
+import pytest
+import torch
+
+from _helpers import O, S, ref_gather_module, ref_module, ref_v2_module
+from filtergs_b200 import filtergs_cuda as FC
+from filtergs_b200 import lod
+
+pytestmark = pytest.mark.gpu
+
+
+def _tree(P=30000, seed=3101, roots=3, depth=8):
+    tr = S.lod_tree(P=P, seed=seed, roots=roots, max_depth=depth, half_extent=60.0)
+    c = tr["xyz"][tr["roots"]].mean(0)
+    cam = S.look_at_camera(c + np.array([15.0, -150.0, 90.0]), c, W=640, H=360, fx=1600.0 / 3)
+    return tr, cam
+
+
+def _t(a, dt=None):
+    x = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    return x if dt is None else x.to(dt)
+
+
+@pytest.fixture(scope="module")
+def v2():
+    m = ref_v2_module()
+    if m is None:
+        pytest.skip("reference build oracle/_ref/ref_compute_radius_v2.so not present")
+    return m
+
+
+def test_visibility_mask_bitexact_vs_reference(cuda, v2):
+    for seed in (3101, 3102):
+        tr, cam = _tree(seed=seed)
+        fx, fy = cam.W / (2 * cam.tanfovx), cam.H / (2 * cam.tanfovy)
+        args = (_t(tr["xyz"]), _t(tr["log_scales"]), _t(tr["rotations"]), _t(cam.projmatrix), _t(cam.viewmatrix),
+                _t(tr["node_index"]), _t(tr["ancestor_path"]), fx, fy, cam.tanfovx, cam.tanfovy)
+        for pad, rmax, thr in ((0.1, 1.5, 700.0), (0.5, 5.0, 0.0), (0.05, 2.0, 30.0)):
+            a = FC.compute_radius_module.compute_visibility_radius(*args, pad, rmax, thr)
+            b = v2.compute_visibility_radius(*args, pad, rmax, thr)
+            assert torch.equal(a[0], b[0]), "mask"
+            assert torch.equal(a[1], b[1]), "radius2d"
+            assert torch.equal(a[2], b[2]), "depth"
+            assert 0 < int(a[0].sum()) < tr["xyz"].shape[0]
+
+
+def test_compute_radius_v2_bitexact_vs_reference(cuda, v2):
+    tr, cam = _tree()
+    fx, fy = cam.W / (2 * cam.tanfovx), cam.H / (2 * cam.tanfovy)
+    sc = torch.exp(_t(tr["log_scales"]))
+    rot = torch.nn.functional.normalize(_t(tr["rotations"]))
+    args = (_t(tr["xyz"]), sc, rot, _t(cam.projmatrix), _t(cam.viewmatrix), fx, fy, cam.tanfovx, cam.tanfovy)
+    assert torch.equal(FC.compute_radius_module.compute_radius(*args), v2.compute_radius(*args))
+
+
+def test_gather_attributes_vs_reference(cuda):
+    g = ref_gather_module()
+    if g is None:
+        pytest.skip("reference gather build not present")
+    rng = np.random.default_rng(5)
+    N, P = 5000, 20000
+    idx = _t(rng.integers(0, P, N))
+    xyz, sc, rot = _t(rng.standard_normal((P, 3), np.float32)), _t(rng.standard_normal((P, 3), np.float32)), \
+        _t(rng.standard_normal((P, 4), np.float32))
+    op, col, shs = _t(rng.standard_normal((P, 1), np.float32)), _t(rng.standard_normal((P, 3), np.float32)), \
+        _t(rng.standard_normal((P, 15, 3), np.float32))
+    a = FC.gather_attributes_cuda(idx, xyz, sc, rot, op, col, shs)
+    b = g.gather_attributes_cuda(idx, xyz, sc, rot, op, col, shs)
+    assert len(a) == len(b) == 6
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+    d = FC.gather_attributes(idx, xyz, sc, rot, op, col)
+    assert set(d) == {"xyz", "scaling", "rotation", "opacity", "colors"} and torch.equal(d["xyz"], b[0])
+
+
+def test_compact_matches_nonzero(cuda):
+    for n, p in ((1, 1.0), (255, 0.3), (256, 0.5), (100_003, 0.01), (1_000_000, 0.4)):
+        m = torch.rand(n, device="cuda") < p
+        idx, cnt = lod.compact(m)
+        nz = torch.nonzero(m, as_tuple=True)[0]
+        assert int(cnt.item()) == nz.numel()
+        assert torch.equal(idx[:nz.numel()], nz)
+
+
+def test_log_cut_order_matches_oracle(cuda):
+    tr, cam = _tree(P=60000, seed=3103, roots=4, depth=9)
+    scene = lod.TreeScene.from_arrays(tr)
+    view, proj = _t(cam.viewmatrix), _t(cam.projmatrix)
+    r = lod.node_radius(scene, view, proj, cam)
+    ids, cnt = lod.log_cut(scene, r, 1.5, levels=30)
+    n = int(cnt.item())
+    o = O.log_cut(tr["roots"], tr["node_index"], tr["tree"], r.cpu().numpy(), 1.5)
+    assert n == len(o) and n > 1000
+    assert np.array_equal(ids[:n].cpu().numpy().astype(np.int64), o)
+    # radius kernel on raw parameters vs the v2 kernel on torch-activated ones
+    fx, fy = cam.W / (2 * cam.tanfovx), cam.H / (2 * cam.tanfovy)
+    r2 = FC.compute_radius_module.compute_radius(scene.xyz, torch.exp(scene.log_scales),
+                                                 torch.nn.functional.normalize(scene.rotations), proj, view, fx, fy,
+                                                 cam.tanfovx, cam.tanfovy)
+    # isotropic nodes make mid^2 - det a cancellation: an ulp in the quaternion norm moves the radius ~1e-5
+    assert torch.allclose(r, r2, rtol=1e-4, atol=1e-4)
+    # culling: order kept, radius < 1 px and opacity < 1/255 dropped
+    out, oc = lod.cull(ids, cnt, r, scene.opacity_raw, 1.0)
+    m = int(oc.item())
+    sel = o[(r.cpu().numpy()[o] >= 1.0) & (1 / (1 + np.exp(-tr["opacity_raw"].reshape(-1)[o])) >= 1 / 255)]
+    assert np.array_equal(out[:m].cpu().numpy(), sel)
+
+
+def test_gather_activate_vs_oracle(cuda):
+    tr, cam = _tree(P=20000, seed=3104)
+    scene = lod.TreeScene.from_arrays(tr)
+    idx = torch.randperm(scene.P, device="cuda")[:7000].sort().values
+    cnt = torch.tensor([6000], dtype=torch.int64, device="cuda")
+    rows = lod.gather_activate(scene, idx, cnt, _t(cam.campos), cap=7000)
+    o = O.gather_activate(idx.cpu().numpy()[:6000], tr["xyz"], tr["log_scales"], tr["rotations"], tr["opacity_raw"],
+                          tr["features_dc"], tr["shs_rest"], 1, cam.campos)
+    for k, ok in (("xyz", "xyz"), ("scaling", "scaling"), ("rotation", "rotation"), ("opacity", "opacity"),
+                  ("colors", "colors")):
+        np.testing.assert_allclose(rows[k][:6000].cpu().numpy(), o[ok], rtol=2e-6, atol=2e-6)
+
+
+def test_filtergs_selected_render_vs_reference_pipeline(cuda, v2, ref):
+    """The device path (mask -> compaction -> fused gather/activation -> rasterizer) against the
+    reference's own pieces (its visibility kernel, torch.nonzero, torch activations, its rasterizer)."""
+    tr, cam = _tree(P=40000, seed=3105)
+    scene = lod.TreeScene.from_arrays(tr)
+    view, proj, cpos = _t(cam.viewmatrix), _t(cam.projmatrix), _t(cam.campos)
+    bg = torch.zeros(3, device="cuda")
+    idx, cnt, mask, r2, dep = lod.select_filtergs(scene, view, proj, cam, 1.5, 0.1, 700.0)
+    mine = lod.render_selected(scene, idx, cnt, view, proj, cpos, cam, bg)
+    fx, fy = cam.W / (2 * cam.tanfovx), cam.H / (2 * cam.tanfovy)
+    rm, _, _ = v2.compute_visibility_radius(scene.xyz, scene.log_scales, scene.rotations, proj, view,
+                                            scene.node_index, scene.ancestor_path, fx, fy, cam.tanfovx, cam.tanfovy,
+                                            0.1, 1.5, 700.0)
+    ri = torch.nonzero(rm, as_tuple=True)[0]
+    assert torch.equal(ri, idx[:int(cnt.item())])
+    xyz = scene.xyz[ri]
+    d = xyz - cpos[None]
+    d = d / torch.norm(d, dim=-1, keepdim=True)
+    rest = scene.shs_rest[ri]
+    C0, C1 = 0.28209479177387814, 0.4886025119029199
+    col = scene.features_dc[ri] * C0 + 0.5 + (-C1 * d[:, 1:2] * rest[:, 0] + C1 * d[:, 2:3] * rest[:, 1] -
+                                              C1 * d[:, 0:1] * rest[:, 2])
+    e = torch.Tensor([])
+    theirs = ref.rasterize_gaussians(bg, xyz, col, torch.sigmoid(scene.opacity_raw[ri])[:, None],
+                                     torch.exp(scene.log_scales[ri]),
+                                     torch.nn.functional.normalize(scene.rotations[ri]), 1.0, e, view, proj,
+                                     cam.tanfovx, cam.tanfovy, cam.H, cam.W, e, 0, cpos, False, True, False, 0.2, 0.2,
+                                     0.05, 0.7, False)
+    assert abs(mine[0] - theirs[0]) <= max(2, 1e-3 * theirs[0])
+    assert (mine[5] != theirs[5]).float().mean().item() <= 1e-3
+    assert (mine[1] - theirs[1]).abs().max().item() <= 2e-4
