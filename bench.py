@@ -81,6 +81,15 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_first(self, timeout=10.0):
+        """Block until nvidia-smi produced a sample, so its start-up never overlaps the timed region."""
+        t0 = time.time()
+        while self.proc is not None and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.05)
+        n = len(self.lines)
+        # keep only samples taken from now on
+        self.skip = n
+
     def stop(self):
         if self.proc is None:
             return None
@@ -91,7 +100,7 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[getattr(self, "skip", 0):]:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -273,16 +282,17 @@ def main():
         if rank == 0:
             print("autotune render (ppt,batch)->(fwd ms, bwd ms): " +
                   ", ".join(f"{k}:{v[0]:.3f}/{v[1]:.3f}" for k, v in sorted(table.items())), file=sys.stderr)
+    clocks = ClockSampler(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+        clocks.wait_first()
     for i in range(args.warmup):
         step_c(mod, scene, views[i % nv], bg, args.stats)
     torch.cuda.synchronize()
     if dist and args.impl == "ours":
         torch.distributed.barrier()
-
-    clocks = ClockSampler(local) if rank == 0 else None
     if clocks:
-        clocks.start()
-        time.sleep(0.3)
+        clocks.skip = len(clocks.lines)
     if args.impl == "ours":
         _lib.profile_read(reset=True)
         _lib.profile_enable(True)
@@ -368,14 +378,18 @@ def main():
 
 def run_e2e(args, mod, scene, views, bg, device, dist):
     """Same metric through the public API: per step, H2D of the camera and the upstream gradient from
-    pinned host memory, forward + backward, D2H of the rendered image."""
+    pinned host memory, forward + backward, D2H of the rendered image.  The copies run on a side stream:
+    step i+1's inputs are uploaded while step i computes, and step i's image is downloaded while its
+    backward runs, as a pipelined caller would do; every step still moves its own bytes."""
     nv = len(views)
     c0 = views[0]["cam"]
     host_cam = [torch.from_numpy(np.concatenate([v["cam"].viewmatrix.reshape(-1), v["cam"].projmatrix.reshape(-1),
                                                  v["cam"].campos])).pin_memory() for v in views]
-    out_host = torch.empty(3, c0.H, c0.W).pin_memory()
-    dev_cam = torch.empty(35, device=device)
-    dev_dL = torch.empty(3, c0.H, c0.W, device=device)
+    out_host = [torch.empty(3, c0.H, c0.W).pin_memory() for _ in range(2)]
+    dev_cam = [torch.empty(35, device=device) for _ in range(2)]
+    dev_dL = [torch.empty(3, c0.H, c0.W, device=device) for _ in range(2)]
+    copy = torch.cuda.Stream(device=device)
+    main = torch.cuda.current_stream(device)
     if args.impl == "ours":
         from filtergs_b200.rasterization import GaussianRasterizationSettings, GaussianRasterizer
         means = scene["means3D"].clone().requires_grad_(True)
@@ -384,37 +398,72 @@ def run_e2e(args, mod, scene, views, bg, device, dist):
         scl = scene["scales"].clone().requires_grad_(True)
         rot = scene["rotations"].clone().requires_grad_(True)
         m2 = torch.zeros_like(means, requires_grad=True)
+    ready = [torch.cuda.Event() for _ in range(2)]
+    freed = [torch.cuda.Event() for _ in range(2)]
+
+    def upload(i):
+        b = i & 1
+        with torch.cuda.stream(copy):
+            copy.wait_event(freed[b])
+            dev_cam[b].copy_(host_cam[i % nv], non_blocking=True)
+            dev_dL[b].copy_(views[i % nv]["dL_host"], non_blocking=True)
+            ready[b].record(copy)
 
     def one(i):
+        b = i & 1
         v = views[i % nv]
         c = v["cam"]
-        dev_cam.copy_(host_cam[i % nv], non_blocking=True)
-        dev_dL.copy_(v["dL_host"], non_blocking=True)
-        view, proj, cpos = dev_cam[:16].view(4, 4), dev_cam[16:32].view(4, 4), dev_cam[32:35]
+        main.wait_event(ready[b])
+        if i + 1 < total[0]:
+            upload(i + 1)
+        view, proj, cpos = dev_cam[b][:16].view(4, 4), dev_cam[b][16:32].view(4, 4), dev_cam[b][32:35]
         if args.impl == "ours":
             rs = GaussianRasterizationSettings(c.H, c.W, c.tanfovx, c.tanfovy, bg, 1.0, view, proj, 3, cpos, False,
                                                False, ogfs_enable_stats=bool(args.stats))
             for t in (means, shs, op, scl, rot, m2):
                 t.grad = None
             color = GaussianRasterizer(rs)(means, m2, op, shs=shs, scales=scl, rotations=rot)[0]
-            color.backward(dev_dL)
+            img_done = torch.cuda.Event()
+            img_done.record(main)
+            with torch.cuda.stream(copy):
+                copy.wait_event(img_done)
+                out_host[b].copy_(color.detach(), non_blocking=True)
+            color.backward(dev_dL[b])
         else:
-            vv = dict(v, view=view, proj=proj, campos=cpos, dL=dev_dL)
-            color = step_c(mod, scene, vv, bg, args.stats)[2]
-        out_host.copy_(color.detach(), non_blocking=True)
+            e = torch.empty(0, device=device)
+            out = mod.rasterize_gaussians(bg, scene["means3D"], e, scene["opacities"], scene["scales"],
+                                          scene["rotations"], 1.0, e, view, proj, c.tanfovx, c.tanfovy, c.H, c.W,
+                                          scene["shs"], 3, cpos, False, True, False, 0.2, 0.2, 0.05, 0.7, args.stats)
+            K, color, pid, pwp, pw, radii, geom, binning, img, st = out
+            img_done = torch.cuda.Event()
+            img_done.record(main)
+            with torch.cuda.stream(copy):
+                copy.wait_event(img_done)
+                out_host[b].copy_(color, non_blocking=True)
+            mod.rasterize_gaussians_backward(bg, scene["means3D"], radii, e, scene["scales"], scene["rotations"], 1.0,
+                                             e, view, proj, c.tanfovx, c.tanfovy, dev_dL[b], scene["shs"], 3, cpos,
+                                             geom, K, binning, img, False)
+        freed[b].record(main)
 
+    total = [args.warmup]
+    upload(0)
     for i in range(args.warmup):
         one(i)
     torch.cuda.synchronize()
     if dist and args.impl == "ours":
         torch.distributed.barrier()
+    total[0] = args.steps
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record()
+    copy.wait_event(start)
+    upload(0)
     for i in range(args.steps):
         one(i)
+    main.wait_stream(copy)      # the last image download is inside the timed region
     end.record()
-    torch.cuda.synchronize()
+    end.synchronize()
     ms = start.elapsed_time(end)
+    torch.cuda.synchronize()
     if dist and args.impl == "ours":
         t = torch.tensor([ms], device=device)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)

@@ -466,7 +466,9 @@ __global__ void __launch_bounds__(256 / PPT)
                     const float G = exp(power);
                     const float alpha = min(0.99f, rb.y * G);
                     if (alpha < 1.0f / 255.0f) continue;
-                    T[k] = T[k] / (1.f - alpha);
+                    // transmittance before this Gaussian (fast reciprocal: 1 - alpha >= 0.01)
+                    const float inv_1ma = __fdividef(1.f, 1.f - alpha);
+                    T[k] = T[k] * inv_1ma;
                     const float dchannel_dcolor = alpha * T[k];
                     const float col[3] = {rb.z, rb.w, R[j].c.x};
                     float dL_dalpha = 0.0f;
@@ -480,7 +482,8 @@ __global__ void __launch_bounds__(256 / PPT)
                     }
                     dL_dalpha *= T[k];
                     last_alpha[k] = alpha;
-                    dL_dalpha += (-T_final[k] / (1.f - alpha)) * bg_dot[k];
+                    // background term; exactly zero (and skipped) for a black background
+                    if (bg_dot[k] != 0.f) dL_dalpha += (-T_final[k] * inv_1ma) * bg_dot[k];
                     if (consistent && rb.y * G > 0.99f) dL_dalpha = 0.f;
                     const float dL_dG = rb.y * dL_dalpha;
                     const float gdx = G * d.x;
