@@ -73,6 +73,13 @@ SIGNATURES = {
     "fgs_log_cut_scratch_bytes": (sz, [i32, i32, i32, i32]),
     "fgs_log_cut": (i32, [i32, vp, i32, vp, vp, i32, vp, f32, i32, vp, vp, vp, vp]),
     "fgs_cull": (i32, [vp, vp, i32, vp, vp, f32, vp, vp, vp, vp]),
+    "fgs_batch_workspace_bytes": (sz, [i32, i32, vp]),
+    "fgs_batch_create": (vp, [C.POINTER(RasterArgs), i32, vp, vp, sz, i32, vp, vp, vp, vp, vp, C.POINTER(i32), vp]),
+    "fgs_batch_forward": (i32, [vp, vp]),
+    "fgs_batch_backward": (i32, [vp, vp]),
+    "fgs_batch_pair_counts": (i32, [vp, vp, vp]),
+    "fgs_batch_check": (i32, [vp, vp]),
+    "fgs_batch_destroy": (None, [vp]),
     "fgs_get_render_config": (i32, [vp]),
     "fgs_forward_noalloc": (i32, [C.POINTER(RasterArgs), vp, vp, vp, vp, vp, C.POINTER(i64), vp]),
 }

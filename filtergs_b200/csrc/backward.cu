@@ -33,7 +33,9 @@ __device__ __forceinline__ float3 dnormvdv(float3 v, float3 dv)
     return r;
 }
 
-// backward.cu:20-139 for one Gaussian; sh / dsh are its [M][3] rows.
+// backward.cu:20-139 for one Gaussian; sh / dsh are its [M][3] rows (added to
+// dsh instead of stored when kAccum).
+template <bool kAccum>
 __device__ __forceinline__ float3 sh_backward(int deg, const float* __restrict__ sh, float3 pos, float3 campos,
                                               uint8_t clamp_bits, float3 dcol, float* __restrict__ dsh, int M)
 {
@@ -98,20 +100,29 @@ __device__ __forceinline__ float3 sh_backward(int deg, const float* __restrict__
     const int ncoef = (deg + 1) * (deg + 1);
 #pragma unroll
     for (int f = 0; f < 48; f++)
-        if (f < M * 3) dsh[f] = f < ncoef * 3 ? g[f] : 0.f;
-    for (int f = 48; f < M * 3; f++) dsh[f] = 0.f;
+        if (f < M * 3) {
+            const float v = f < ncoef * 3 ? g[f] : 0.f;
+            if (kAccum) dsh[f] += v;
+            else dsh[f] = v;
+        }
+    if (!kAccum)
+        for (int f = 48; f < M * 3; f++) dsh[f] = 0.f;
     const float3 ddir = {dx[0] * d[0] + dx[1] * d[1] + dx[2] * d[2], dy[0] * d[0] + dy[1] * d[1] + dy[2] * d[2],
                          dz[0] * d[0] + dz[1] * d[1] + dz[2] * d[2]};
     return dnormvdv(dir_orig, ddir);
 }
 
+// kAccum: add this view's gradients into dense buffers shared by several views
+// (views run one after another on a stream, so each row has one writer at a
+// time) and fold the view's opacity gradient into shared_dopac.
+template <bool kAccum>
 __global__ void __launch_bounds__(256)
     preprocess_bwd_kernel(PreParams p, const uint32_t* __restrict__ visible_ids,
                           const unsigned long long* __restrict__ visible_count, const uint8_t* __restrict__ clamped,
                           const float* __restrict__ dmean2D, const float* __restrict__ dconic,
                           const float* __restrict__ dcolor, float* __restrict__ dopac, float* __restrict__ dmean3D,
                           float* __restrict__ dcov3D, float* __restrict__ dsh, float* __restrict__ dscale,
-                          float* __restrict__ drot, int consistent)
+                          float* __restrict__ drot, int consistent, float* __restrict__ shared_dopac)
 {
     // The forward's depth ordering put the V visible Gaussians first; culled
     // rows were zero-filled by the launcher.
@@ -236,7 +247,8 @@ __global__ void __launch_bounds__(256)
                 if (f < nf) sh[f] = row[f];
             const float3 cam = {p.campos[0], p.campos[1], p.campos[2]};
             const float3 dcol = {dcolor[3 * idx], dcolor[3 * idx + 1], dcolor[3 * idx + 2]};
-            const float3 dmd = sh_backward(p.D, sh, mean, cam, clamped[idx], dcol, dsh + (size_t)idx * p.M * 3, p.M);
+            const float3 dmd =
+                sh_backward<kAccum>(p.D, sh, mean, cam, clamped[idx], dcol, dsh + (size_t)idx * p.M * 3, p.M);
             dm.x += dmd.x; dm.y += dmd.y; dm.z += dmd.z;
         }
         if (p.scales && dscale) {
@@ -263,7 +275,11 @@ __global__ void __launch_bounds__(256)
             float* ds = dscale + 3 * (size_t)idx;
 #pragma unroll
             for (int cc = 0; cc < 3; cc++)
-                ds[cc] = Rt.m[cc][0] * dMt.m[cc][0] + Rt.m[cc][1] * dMt.m[cc][1] + Rt.m[cc][2] * dMt.m[cc][2];
+            {
+                const float v = Rt.m[cc][0] * dMt.m[cc][0] + Rt.m[cc][1] * dMt.m[cc][1] + Rt.m[cc][2] * dMt.m[cc][2];
+                if (kAccum) ds[cc] += v;
+                else ds[cc] = v;
+            }
 #pragma unroll
             for (int cc = 0; cc < 3; cc++)
 #pragma unroll
@@ -278,15 +294,32 @@ __global__ void __launch_bounds__(256)
             dq.w = 2 * r * (dMt.m[0][1] - dMt.m[1][0]) + 2 * x * (dMt.m[2][0] + dMt.m[0][2]) +
                    2 * y * (dMt.m[1][2] + dMt.m[2][1]) - 4 * z * (dMt.m[1][1] + dMt.m[0][0]);
             float* dr = drot + 4 * (size_t)idx;
-            dr[0] = dq.x; dr[1] = dq.y; dr[2] = dq.z; dr[3] = dq.w;
+            if (kAccum) {
+                dr[0] += dq.x; dr[1] += dq.y; dr[2] += dq.z; dr[3] += dq.w;
+            } else {
+                dr[0] = dq.x; dr[1] = dq.y; dr[2] = dq.z; dr[3] = dq.w;
+            }
         }
-        if (consistent && p.opac && p.opac[idx] < 1e-6f) dopac[idx] = 0.f;
+        const bool floor_mask = consistent && p.opac && p.opac[idx] < 1e-6f;
+        if (kAccum) {
+            if (!floor_mask) shared_dopac[idx] += dopac[idx];
+        } else if (floor_mask) {
+            dopac[idx] = 0.f;
+        }
     }
-    dmean3D[3 * idx] = dm.x;
-    dmean3D[3 * idx + 1] = dm.y;
-    dmean3D[3 * idx + 2] = dm.z;
+    if (kAccum) {
+        dmean3D[3 * idx] += dm.x;
+        dmean3D[3 * idx + 1] += dm.y;
+        dmean3D[3 * idx + 2] += dm.z;
 #pragma unroll
-    for (int k = 0; k < 6; k++) dcov3D[6 * (size_t)idx + k] = dc[k];
+        for (int k = 0; k < 6; k++) dcov3D[6 * (size_t)idx + k] += dc[k];
+    } else {
+        dmean3D[3 * idx] = dm.x;
+        dmean3D[3 * idx + 1] = dm.y;
+        dmean3D[3 * idx + 2] = dm.z;
+#pragma unroll
+        for (int k = 0; k < 6; k++) dcov3D[6 * (size_t)idx + k] = dc[k];
+    }
     }
 }
 
@@ -294,23 +327,32 @@ __global__ void __launch_bounds__(256)
 
 void launch_preprocess_bwd(const PreParams& p, const int* radii, const GeomState& g, const float* dmean2D,
                            const float* dconic, const float* dcolor, float* dopac, float* dmean3D, float* dcov3D,
-                           float* dsh, float* dscale, float* drot, int consistent, cudaStream_t s)
+                           float* dsh, float* dscale, float* drot, int consistent, cudaStream_t s, bool accumulate,
+                           float* shared_dopac)
 {
     (void)radii;
     if (p.P <= 0) return;
-    // Dense outputs: culled rows are zero, written here at copy-engine speed.
     const size_t P = (size_t)p.P;
-    cudaMemsetAsync(dmean3D, 0, sizeof(float) * 3 * P, s);
-    cudaMemsetAsync(dcov3D, 0, sizeof(float) * 6 * P, s);
-    if (dsh) cudaMemsetAsync(dsh, 0, sizeof(float) * 3 * (size_t)p.M * P, s);
-    if (dscale) cudaMemsetAsync(dscale, 0, sizeof(float) * 3 * P, s);
-    if (drot) cudaMemsetAsync(drot, 0, sizeof(float) * 4 * P, s);
+    if (!accumulate) {
+        // Dense outputs: culled rows are zero, written here at copy-engine speed.
+        cudaMemsetAsync(dmean3D, 0, sizeof(float) * 3 * P, s);
+        cudaMemsetAsync(dcov3D, 0, sizeof(float) * 6 * P, s);
+        if (dsh) cudaMemsetAsync(dsh, 0, sizeof(float) * 3 * (size_t)p.M * P, s);
+        if (dscale) cudaMemsetAsync(dscale, 0, sizeof(float) * 3 * P, s);
+        if (drot) cudaMemsetAsync(drot, 0, sizeof(float) * 4 * P, s);
+    }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int blocks = (int)std::min<size_t>((P + 255) / 256, (size_t)sms * 8);
-    preprocess_bwd_kernel<<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dmean2D, dconic, dcolor,
-                                                 dopac, dmean3D, dcov3D, dsh, dscale, drot, consistent);
+    if (accumulate)
+        preprocess_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dmean2D, dconic,
+                                                           dcolor, dopac, dmean3D, dcov3D, dsh, dscale, drot,
+                                                           consistent, shared_dopac);
+    else
+        preprocess_bwd_kernel<false><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dmean2D, dconic,
+                                                            dcolor, dopac, dmean3D, dcov3D, dsh, dscale, drot,
+                                                            consistent, nullptr);
     note_launches(1);
 }
 

@@ -1,0 +1,307 @@
+// Many views of one Gaussian set in one stream-ordered, host-sync-free
+// sequence (the batched path; the reference renders one view per call).
+//
+// fgs_batch_create carves a caller-owned workspace into per-view state with
+// fixed pair capacities and uploads the per-view tile descriptors once; after
+// that fgs_batch_forward / fgs_batch_backward only enqueue kernels and
+// memsets on the caller's stream -- no host synchronisation, no allocation --
+// so the pair can be captured into a CUDA graph and replayed.  Per view the
+// front end (preprocess, depth sort, pair emission, tile sort, ranges) runs
+// with the pair count kept on the device; compositing, forward and backward,
+// is ONE persistent launch per direction over the tiles of all views, fed by a
+// global work queue.  Backward sums every view's gradients into shared dense
+// buffers (views in stream order, so each row has a single writer at a time).
+// A view whose pairs exceed its capacity is truncated and FGS_ERR_OVERFLOW is
+// recorded; fgs_batch_check reports it (the caller re-plans with a larger
+// capacity, outside any captured graph).
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "fgs_common.cuh"
+#include "fgs_internal.h"
+
+namespace fgs {
+namespace {
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+struct ViewState {
+    PreParams pre;
+    int num_tiles, tile_bits;
+    long long cap;
+    GeomState g;
+    ImageState im;
+    BinState b;
+    char* geom_base;
+    size_t geom_bytes_v;
+    float *dmean2D, *dconic, *dopac, *dcolor;  // screen-space gradients of this view
+    int* radii_out;
+};
+
+struct Batch {
+    int P, V, consistent;
+    std::vector<ViewState> views;
+    TileArgs* d_args_fwd;
+    TileArgs* d_args_bwd;
+    uint32_t* d_begin;
+    uint32_t* d_queue;
+    unsigned* d_err;
+    uint32_t total_tiles;
+    const float* background;
+    float *g_means3D, *g_opacity, *g_sh, *g_scales, *g_rot, *g_cov3D;
+    int M;
+    bool has_sr;
+};
+
+struct Layout {
+    size_t total;
+    std::vector<size_t> geom_off, img_off, bin_off, grad_off;
+    size_t args_off, begin_off, misc_off, cov_off;
+};
+
+Layout plan(int P, int V, const fgs_view_args* views)
+{
+    Layout L;
+    size_t off = 0;
+    for (int v = 0; v < V; v++) {
+        L.geom_off.push_back(off);
+        off = align_up(off + geom_bytes(P));
+        L.img_off.push_back(off);
+        off = align_up(off + image_bytes(views[v].width, views[v].height));
+        L.bin_off.push_back(off);
+        off = align_up(off + bin_bytes(views[v].pair_capacity, P));
+        L.grad_off.push_back(off);
+        off = align_up(off + sizeof(float) * 11 * (size_t)P);
+    }
+    L.args_off = off;
+    off = align_up(off + 2 * sizeof(TileArgs) * (size_t)V);
+    L.begin_off = off;
+    off = align_up(off + sizeof(uint32_t) * (size_t)(V + 1));
+    L.misc_off = off;
+    off = align_up(off + 64);
+    L.cov_off = off;
+    off = align_up(off + sizeof(float) * 6 * (size_t)P);
+    L.total = off;
+    return L;
+}
+
+__global__ void zero_visible_rows(const uint32_t* __restrict__ ids, const unsigned long long* __restrict__ count,
+                                  float* __restrict__ dmean2D, float* __restrict__ dconic, float* __restrict__ dopac,
+                                  float* __restrict__ dcolor)
+{
+    const uint32_t V = (uint32_t)*count;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < V; j += gridDim.x * blockDim.x) {
+        const uint32_t i = ids[j];
+        dmean2D[3 * i] = dmean2D[3 * i + 1] = dmean2D[3 * i + 2] = 0.f;
+        dconic[4 * i] = dconic[4 * i + 1] = dconic[4 * i + 2] = dconic[4 * i + 3] = 0.f;
+        dopac[i] = 0.f;
+        dcolor[3 * i] = dcolor[3 * i + 1] = dcolor[3 * i + 2] = 0.f;
+    }
+}
+
+int tile_bits_of(int num_tiles)
+{
+    int bits = 1;
+    while (bits < 31 && (1u << bits) < (unsigned)num_tiles) bits++;
+    return bits;
+}
+
+}  // namespace
+}  // namespace fgs
+
+using namespace fgs;
+
+extern "C" {
+
+size_t fgs_batch_workspace_bytes(int P, int nviews, const fgs_view_args* views)
+{
+    if (P < 0 || nviews <= 0 || !views) return 0;
+    for (int v = 0; v < nviews; v++)
+        if (views[v].width <= 0 || views[v].height <= 0 || views[v].pair_capacity < 0) return 0;
+    return plan(P, nviews, views).total;
+}
+
+void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view_args* views, void* workspace,
+                       size_t workspace_bytes, int backward_mode, float* dL_dmeans3D, float* dL_dopacity,
+                       float* dL_dsh, float* dL_dscales, float* dL_drotations, int* status, void* stream)
+{
+    auto fail = [&](int st) -> void* {
+        if (status) *status = st;
+        return nullptr;
+    };
+    if (!shared || nviews <= 0 || !views || !workspace) return fail(FGS_ERR_ARG);
+    if (backward_mode != FGS_BACKWARD_REF_COMPAT && backward_mode != FGS_BACKWARD_CONSISTENT) return fail(FGS_ERR_ARG);
+    const int P = shared->P;
+    if (P <= 0) return fail(FGS_ERR_ARG);
+    const Layout L = plan(P, nviews, views);
+    if (workspace_bytes < L.total) return fail(FGS_ERR_ARG);
+    if ((reinterpret_cast<uintptr_t>(workspace) & (kAlign - 1)) != 0) return fail(FGS_ERR_ARG);
+    Batch* B = new (std::nothrow) Batch();
+    if (!B) return fail(FGS_ERR_CUDA);
+    B->P = P;
+    B->V = nviews;
+    B->consistent = backward_mode == FGS_BACKWARD_CONSISTENT;
+    B->background = shared->background;
+    B->g_means3D = dL_dmeans3D;
+    B->g_opacity = dL_dopacity;
+    B->g_sh = dL_dsh;
+    B->g_scales = dL_dscales;
+    B->g_rot = dL_drotations;
+    char* base = static_cast<char*>(workspace);
+    B->g_cov3D = reinterpret_cast<float*>(base + L.cov_off);
+    std::vector<TileArgs> fa(nviews), ba(nviews);
+    std::vector<uint32_t> begin(nviews + 1, 0);
+    for (int v = 0; v < nviews; v++) {
+        const fgs_view_args& va = views[v];
+        fgs_raster_args a = *shared;
+        a.width = va.width;
+        a.height = va.height;
+        a.viewmatrix = va.viewmatrix;
+        a.projmatrix = va.projmatrix;
+        a.campos = va.campos;
+        a.tan_fovx = va.tan_fovx;
+        a.tan_fovy = va.tan_fovy;
+        a.ogfs_enable_stats = 0;
+        ViewState s{};
+        int st = make_params(&a, s.pre);
+        if (st || !va.out_color || va.pair_capacity >= (1ll << 30)) {
+            delete B;
+            return fail(st ? st : FGS_ERR_ARG);
+        }
+        const int gx = (va.width + kTileX - 1) / kTileX, gy = (va.height + kTileY - 1) / kTileY;
+        s.num_tiles = gx * gy;
+        s.tile_bits = tile_bits_of(s.num_tiles);
+        s.cap = va.pair_capacity;
+        s.geom_base = base + L.geom_off[v];
+        s.geom_bytes_v = geom_bytes(P);
+        s.g = geom_views(s.geom_base, P);
+        s.im = image_views(base + L.img_off[v], va.width, va.height);
+        s.b = bin_views(base + L.bin_off[v], s.cap, P);
+        float* gr = reinterpret_cast<float*>(base + L.grad_off[v]);
+        s.dmean2D = gr;
+        s.dconic = gr + 3 * (size_t)P;
+        s.dopac = gr + 7 * (size_t)P;
+        s.dcolor = gr + 8 * (size_t)P;
+        s.radii_out = va.out_radii;
+        B->M = s.pre.M;
+        B->has_sr = s.pre.scales != nullptr;
+        TileArgs f{};
+        f.ranges = s.im.ranges; f.recs = s.b.rec; f.W = va.width; f.H = va.height; f.bg = shared->background;
+        f.out_color = va.out_color; f.final_T = s.im.final_T; f.n_contrib = s.im.n_contrib;
+        TileArgs bk = f;
+        bk.out_color = nullptr;
+        bk.dL_dpix = va.dL_dout_color; bk.dmean2D = s.dmean2D; bk.dconic = s.dconic; bk.dopac = s.dopac;
+        bk.dcolor = s.dcolor;
+        fa[v] = f;
+        ba[v] = bk;
+        begin[v + 1] = begin[v] + (uint32_t)s.num_tiles;
+        B->views.push_back(s);
+    }
+    B->total_tiles = begin[nviews];
+    B->d_args_fwd = reinterpret_cast<TileArgs*>(base + L.args_off);
+    B->d_args_bwd = B->d_args_fwd + nviews;
+    B->d_begin = reinterpret_cast<uint32_t*>(base + L.begin_off);
+    B->d_queue = reinterpret_cast<uint32_t*>(base + L.misc_off);
+    B->d_err = reinterpret_cast<unsigned*>(base + L.misc_off + 16);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(B->d_args_fwd, fa.data(), sizeof(TileArgs) * nviews, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(B->d_args_bwd, ba.data(), sizeof(TileArgs) * nviews, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(B->d_begin, begin.data(), sizeof(uint32_t) * (nviews + 1), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaMemsetAsync(B->d_queue, 0, 64, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+        delete B;
+        return fail(FGS_ERR_CUDA);
+    }
+    if (status) *status = FGS_OK;
+    return B;
+}
+
+void fgs_batch_destroy(void* handle) { delete static_cast<Batch*>(handle); }
+
+int fgs_batch_forward(void* handle, void* stream)
+{
+    Batch* B = static_cast<Batch*>(handle);
+    if (!B) return FGS_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    for (ViewState& v : B->views) {
+        char* zero_begin = reinterpret_cast<char*>(v.g.hist);
+        cudaMemsetAsync(zero_begin, 0, (size_t)(v.geom_base + v.geom_bytes_v - zero_begin), s);
+        launch_preprocess(v.pre, v.g, v.radii_out, s);
+        launch_depth_sort(v.g, B->P, s);
+    }
+    for (ViewState& v : B->views) {
+        if (v.cap > 0) {
+            cudaMemsetAsync(v.b.status, 0, sizeof(uint32_t) * (v.b.status_words + v.b.scan_words), s);
+            launch_duplicate(v.g, v.b, (uint32_t)B->P, (uint32_t)v.cap, v.pre.W, v.pre.H, v.tile_bits, s);
+            launch_tile_sort(v.g, v.b, v.cap, v.tile_bits, s, v.g.total);
+        }
+        launch_ranges(v.b, v.im, v.cap, v.num_tiles, s, v.g.total);
+    }
+    launch_render_fwd_multi(B->d_args_fwd, B->d_begin, B->V, B->total_tiles, B->d_queue, B->d_err, s);
+    return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
+}
+
+int fgs_batch_backward(void* handle, void* stream)
+{
+    Batch* B = static_cast<Batch*>(handle);
+    if (!B) return FGS_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t P = (size_t)B->P;
+    if (!B->g_means3D || !B->g_opacity) return FGS_ERR_ARG;
+    cudaMemsetAsync(B->g_means3D, 0, sizeof(float) * 3 * P, s);
+    cudaMemsetAsync(B->g_opacity, 0, sizeof(float) * P, s);
+    cudaMemsetAsync(B->g_cov3D, 0, sizeof(float) * 6 * P, s);
+    if (B->g_sh && B->M > 0) cudaMemsetAsync(B->g_sh, 0, sizeof(float) * 3 * (size_t)B->M * P, s);
+    if (B->g_scales) cudaMemsetAsync(B->g_scales, 0, sizeof(float) * 3 * P, s);
+    if (B->g_rot) cudaMemsetAsync(B->g_rot, 0, sizeof(float) * 4 * P, s);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    for (ViewState& v : B->views) {
+        zero_visible_rows<<<sms * 2, 256, 0, s>>>(v.g.sort_ids_b, v.g.total + 1, v.dmean2D, v.dconic, v.dopac,
+                                                  v.dcolor);
+        note_launches(1);
+    }
+    launch_render_bwd_multi(B->d_args_bwd, B->d_begin, B->V, B->total_tiles, B->d_queue + 1, B->consistent, B->d_err,
+                            s);
+    for (ViewState& v : B->views) {
+        launch_preprocess_bwd(v.pre, nullptr, v.g, v.dmean2D, v.dconic, v.dcolor, v.dopac, B->g_means3D, B->g_cov3D,
+                              (v.pre.shs && B->g_sh) ? B->g_sh : nullptr, B->has_sr ? B->g_scales : nullptr,
+                              B->has_sr ? B->g_rot : nullptr, B->consistent, s, true, B->g_opacity);
+    }
+    return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
+}
+
+int fgs_batch_pair_counts(void* handle, long long* counts, void* stream)
+{
+    Batch* B = static_cast<Batch*>(handle);
+    if (!B || !counts) return FGS_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::vector<unsigned long long> tot(2 * B->V);
+    for (int v = 0; v < B->V; v++)
+        cudaMemcpyAsync(&tot[2 * v], B->views[v].g.total, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return FGS_ERR_CUDA;
+    for (int v = 0; v < B->V; v++) counts[v] = (long long)tot[2 * v];
+    return FGS_OK;
+}
+
+int fgs_batch_check(void* handle, void* stream)
+{
+    Batch* B = static_cast<Batch*>(handle);
+    if (!B) return FGS_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::vector<unsigned> errs(B->V + 1, 0);
+    for (int v = 0; v < B->V; v++)
+        cudaMemcpyAsync(&errs[v], B->views[v].g.err, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&errs[B->V], B->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return FGS_ERR_CUDA;
+    unsigned all = 0;
+    for (unsigned e : errs) all |= e;
+    for (int c = 1; c < 32; c++)
+        if (all & (1u << c)) return c;
+    return FGS_OK;
+}
+
+}  // extern "C"

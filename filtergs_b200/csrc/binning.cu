@@ -106,7 +106,8 @@ __global__ void __launch_bounds__(kSortThreads)
     onesweep_kernel(const uint32_t* __restrict__ keys_in, uint32_t* __restrict__ keys_out,
                     const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ vals_out, uint32_t n, int shift,
                     int nbits, const uint32_t* __restrict__ pass_hist, uint32_t* status, uint32_t* chunk_counter,
-                    unsigned* err, const PairRecord* __restrict__ grec, PairRecord* __restrict__ rec_out)
+                    unsigned* err, const PairRecord* __restrict__ grec, PairRecord* __restrict__ rec_out,
+                    const unsigned long long* __restrict__ n_dev)
 {
     __shared__ uint32_t s_hist[kSortWarps][kRadix];
     __shared__ uint32_t s_keys[kSortTile];
@@ -123,6 +124,10 @@ __global__ void __launch_bounds__(kSortThreads)
     __syncthreads();
     const uint32_t chunk = s_chunk;
     const uint32_t base = chunk * kSortTile;
+    // With a device-side count the grid is sized for a capacity; chunks past the
+    // live count have nothing to do (and no later chunk waits on them).
+    if (n_dev) n = (uint32_t)min((unsigned long long)n, *n_dev);
+    if (base >= n) return;
     const uint32_t count = min((uint32_t)kSortTile, n - base);
     const uint32_t dmask = (1u << nbits) - 1u;
 
@@ -288,9 +293,11 @@ __global__ void __launch_bounds__(256)
 }
 
 // identifyTileRanges (rasterizer_impl.cu:172-194) over the sorted tile ids.
-__global__ void ranges_kernel(const uint32_t* __restrict__ tile, uint32_t K, uint2* __restrict__ ranges)
+__global__ void ranges_kernel(const uint32_t* __restrict__ tile, uint32_t K, uint2* __restrict__ ranges,
+                              const unsigned long long* __restrict__ n_dev)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n_dev) K = (uint32_t)min((unsigned long long)K, *n_dev);
     if (i >= K) return;
     const uint32_t t = tile[i];
     if (i == 0 || tile[i - 1] != t) ranges[t].x = i;
@@ -320,7 +327,7 @@ void launch_depth_sort(const GeomState& g, int P, cudaStream_t s)
     for (int pass = 0; pass < 4; pass++) {
         onesweep_kernel<<<nch, kSortThreads, 0, s>>>(kin[pass], kout[pass], vin[pass], vout[pass], n, 8 * pass, 8,
                                                      g.hist + pass * kRadix, g.status + (size_t)pass * nch * kRadix,
-                                                     g.counters + pass, g.err, nullptr, nullptr);
+                                                     g.counters + pass, g.err, nullptr, nullptr, nullptr);
     }
 }
 
@@ -340,7 +347,8 @@ void launch_duplicate(const GeomState& g, const BinState& b, uint32_t V, uint32_
     note_launches(1);
 }
 
-void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int tile_bits, cudaStream_t s)
+void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int tile_bits, cudaStream_t s,
+                      const unsigned long long* n_dev)
 {
     if (K <= 0) return;
     const uint32_t n = (uint32_t)K;
@@ -355,18 +363,19 @@ void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int ti
         uint32_t* vo = (vi == b.val_a) ? b.val_b : b.val_a;
         onesweep_kernel<<<nch, kSortThreads, 0, s>>>(ki, ko, vi, vo, n, 8 * pass, nbits, g.hist + (4 + pass) * kRadix,
                                                      b.status + (size_t)pass * nch * kRadix, g.counters + 4 + pass,
-                                                     g.err, last ? g.grec : nullptr, last ? b.rec : nullptr);
+                                                     g.err, last ? g.grec : nullptr, last ? b.rec : nullptr, n_dev);
         ki = ko;
         vi = vo;
     }
     note_launches(passes);
 }
 
-void launch_ranges(const BinState& b, const ImageState& im, long long K, int num_tiles, cudaStream_t s)
+void launch_ranges(const BinState& b, const ImageState& im, long long K, int num_tiles, cudaStream_t s,
+                   const unsigned long long* n_dev)
 {
     cudaMemsetAsync(im.ranges, 0, sizeof(uint2) * (size_t)num_tiles, s);
     if (K <= 0) return;
-    ranges_kernel<<<chunks_of(K, 256), 256, 0, s>>>(b.tile_b, (uint32_t)K, im.ranges);
+    ranges_kernel<<<chunks_of(K, 256), 256, 0, s>>>(b.tile_b, (uint32_t)K, im.ranges, n_dev);
     note_launches(1);
 }
 

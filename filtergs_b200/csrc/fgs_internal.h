@@ -79,8 +79,11 @@ void launch_depth_sort(const GeomState& g, int P, cudaStream_t s);
 void launch_duplicate(const GeomState& g, const BinState& b, uint32_t V, uint32_t K, int W, int H, int tile_bits,
                       cudaStream_t s);
 int sort_chunk_size();
-void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int tile_bits, cudaStream_t s);
-void launch_ranges(const BinState& b, const ImageState& im, long long K, int num_tiles, cudaStream_t s);
+// K is the pair count, or the capacity when n_dev (device-side count) is given.
+void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int tile_bits, cudaStream_t s,
+                      const unsigned long long* n_dev = nullptr);
+void launch_ranges(const BinState& b, const ImageState& im, long long K, int num_tiles, cudaStream_t s,
+                   const unsigned long long* n_dev = nullptr);
 void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, const float* bg, float* out_color,
                        int* point_id, float* pw_pixel, float* point_weight, bool stats, unsigned* err,
                        cudaStream_t s);
@@ -90,7 +93,7 @@ void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, co
 void launch_preprocess_bwd(const PreParams& p, const int* radii, const GeomState& g, const float* dmean2D,
                            const float* dconic, const float* dcolor, float* dopac, float* dmean3D,
                            float* dcov3D, float* dsh, float* dscale, float* drot, int consistent,
-                           cudaStream_t s);
+                           cudaStream_t s, bool accumulate = false, float* shared_dopac = nullptr);
 void launch_kpc_stats(const BinState& b, const ImageState& im, int num_tiles, float used_thresh, double* dev_out,
                       cudaStream_t s);
 
@@ -108,6 +111,39 @@ void launch_visibility_radius(int P, const float* means, const float* lscales, c
 // Validate a fgs_raster_args and derive the kernel parameters (opacities may
 // be absent in backward).
 int make_params(const fgs_raster_args* a, PreParams& p, bool backward = false);
+
+// ---------------------------------------------------------------- render views
+// Everything one tile needs, for the plain launch (one view, one tile per CTA)
+// and the persistent multi-view launch (CTAs pop (view, tile) work items).
+struct TileArgs {
+    const uint2* ranges;
+    const PairRecord* recs;
+    int W, H;
+    const float* bg;
+    // forward outputs
+    float* out_color;
+    float* final_T;
+    uint32_t* n_contrib;
+    int* out_point_id;
+    float* out_pw_pixel;
+    float* out_point_weight;
+    float* kv_sum;
+    uint32_t* kv_cnt;
+    // backward inputs / outputs
+    const float* dL_dpix;
+    float* dmean2D;
+    float* dconic;
+    float* dopac;
+    float* dcolor;
+};
+
+// Persistent multi-view compositing over the tiles of `nviews` views; begin[v]
+// is the first work item of view v (begin[nviews] == total_tiles); queue is a
+// device counter (zeroed here).
+void launch_render_fwd_multi(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total_tiles,
+                             uint32_t* queue, unsigned* err, cudaStream_t s);
+void launch_render_bwd_multi(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total_tiles,
+                             uint32_t* queue, int consistent, unsigned* err, cudaStream_t s);
 
 // Render kernel shape: pixels per thread {1,2,4} and records per shared-memory batch {64,128,256}.
 struct RenderConfig {

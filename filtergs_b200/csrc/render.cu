@@ -155,46 +155,55 @@ __device__ __forceinline__ bool may_touch(float mx, float my, float a, float b, 
     return q <= thr + 0.05f + 1e-5f * mag;
 }
 
+// ---------------------------------------------------------------- per-view render descriptors
+// Everything one tile needs, for the plain launch (one view, one tile per CTA)
+// and the persistent multi-view launch (CTAs pop (view, tile) work items).
+
+template <int kBatch>
+struct FwdSmem {
+    PairRecord rec[kBufs][kBatch];
+    uint64_t bar[kBufs];
+    uint32_t wmax[2][kBatch];
+    float ksum[2][kBatch];
+    uint32_t kcnt[2][kBatch];
+};
+
+template <int kBatch>
+struct BwdSmem {
+    PairRecord rec[kBufs][kBatch];
+    uint64_t bar[kBufs];
+    float acc[9][kBatch];
+    uint32_t max_last;
+};
+
 // ---------------------------------------------------------------- forward
+// One tile.  Callers guarantee every thread of the CTA is synchronised on
+// entry and that no bulk copy is in flight.  `gb` counts the record batches
+// this CTA has ever waited for: batch g lives in buffer g % 3 and completes
+// phase (g / 3) & 1 of that buffer's mbarrier, so the barriers are initialised
+// once per CTA and keep their phase across tiles.
 template <int PPT, int kBatch>
-__global__ void __launch_bounds__(256 / PPT)
-    render_fwd_kernel(const uint2* __restrict__ ranges, const PairRecord* __restrict__ recs, int W, int H,
-                      const float* __restrict__ bg, float* __restrict__ out_color, float* __restrict__ final_T,
-                      uint32_t* __restrict__ n_contrib, int* __restrict__ out_point_id,
-                      float* __restrict__ out_pw_pixel, float* __restrict__ out_point_weight,
-                      float* __restrict__ kv_sum, uint32_t* __restrict__ kv_cnt, unsigned* err)
+__device__ __forceinline__ void render_fwd_tile(FwdSmem<kBatch>& sm, const TileArgs& a, int tile, uint32_t& gb,
+                                                unsigned* err)
 {
     constexpr int NT = 256 / PPT;
-    __shared__ __align__(128) PairRecord s_rec[kBufs][kBatch];
-    __shared__ __align__(8) uint64_t s_bar[kBufs];
-    __shared__ uint32_t s_wmax[2][kBatch];
-    __shared__ float s_ksum[2][kBatch];
-    __shared__ uint32_t s_kcnt[2][kBatch];
-
     const int tid = threadIdx.x;
+    const int W = a.W, H = a.H;
     const int gx = (W + kTileX - 1) / kTileX;
-    const int tile = blockIdx.x;
     const int bx = tile % gx, by = tile / gx;
     const int lx = tid & 15, ly0 = (tid >> 4) * PPT;
     const int px = bx * kTileX + lx;
-    const uint2 range = ranges[tile];
+    const uint2 range = a.ranges[tile];
     const uint32_t n = range.y - range.x;
     const int nb = (int)((n + kBatch - 1) / kBatch);
-    const bool stats = kv_sum != nullptr;
+    const bool stats = a.kv_sum != nullptr;
+    const PairRecord* recs = a.recs;
 
-    for (int e = tid; e < 2 * kBatch; e += NT) {
-        (&s_wmax[0][0])[e] = 0;
-        (&s_ksum[0][0])[e] = 0.f;
-        (&s_kcnt[0][0])[e] = 0;
-    }
     if (tid == 0) {
-        for (int i = 0; i < kBufs; i++) mbar_init(&s_bar[i], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (tid == 0) {
-        for (int b = 0; b < 2 && b < nb; b++)
-            issue_batch(s_rec[b], &s_bar[b], recs, range.x + b * kBatch, min((uint32_t)kBatch, n - b * kBatch));
+        for (int b = 0; b < 2 && b < nb; b++) {
+            const int buf = (int)((gb + b) % kBufs);
+            issue_batch(sm.rec[buf], &sm.bar[buf], recs, range.x + b * kBatch, min((uint32_t)kBatch, n - b * kBatch));
+        }
     }
 
     float T[PPT], C[PPT][3], wmax[PPT];
@@ -221,13 +230,15 @@ __global__ void __launch_bounds__(256 / PPT)
 #pragma unroll
     for (int k = 0; k < PPT; k++) all_done = all_done && done[k];
 
+    int issued = nb < 2 ? nb : 2;
     uint32_t contributor = 0;
     for (int b = 0; b < nb; b++) {
-        const int buf = b % kBufs;
+        const uint32_t g = gb + b;
+        const int buf = (int)(g % kBufs);
         const int acc = b & 1;
         const uint32_t cnt = min((uint32_t)kBatch, n - b * kBatch);
-        if (!mbar_wait(&s_bar[buf], (uint32_t)((b / kBufs) & 1), err)) all_done = true;
-        const PairRecord* R = s_rec[buf];
+        if (!mbar_wait(&sm.bar[buf], (g / kBufs) & 1, err)) all_done = true;
+        const PairRecord* R = sm.rec[buf];
         const bool warp_live = !__all_sync(0xffffffffu, all_done);
         if (warp_live) {
             bool stop = false;
@@ -290,10 +301,10 @@ __global__ void __launch_bounds__(256 / PPT)
                             kcs = __reduce_add_sync(0xffffffffu, kc);
                         }
                         if ((tid & 31) == 0) {
-                            atomicMax(&s_wmax[acc][j], wm);
+                            atomicMax(&sm.wmax[acc][j], wm);
                             if (stats) {
-                                atomicAdd(&s_ksum[acc][j], ks);
-                                atomicAdd(&s_kcnt[acc][j], kcs);
+                                atomicAdd(&sm.ksum[acc][j], ks);
+                                atomicAdd(&sm.kcnt[acc][j], kcs);
                             }
                         }
                     }
@@ -307,95 +318,140 @@ __global__ void __launch_bounds__(256 / PPT)
         contributor += cnt;
         const int ndone = __syncthreads_count(all_done);
         for (uint32_t e = tid; e < cnt; e += NT) {
-            const uint32_t wm = s_wmax[acc][e];
+            const uint32_t wm = sm.wmax[acc][e];
             if (wm) {
                 const int id = __float_as_int(R[e].c.y);
-                atomicMax(reinterpret_cast<unsigned*>(out_point_weight) + id, wm);
-                s_wmax[acc][e] = 0;
+                if (a.out_point_weight) atomicMax(reinterpret_cast<unsigned*>(a.out_point_weight) + id, wm);
+                sm.wmax[acc][e] = 0;
             }
             if (stats) {
-                kv_sum[range.x + b * kBatch + e] = s_ksum[acc][e];
-                kv_cnt[range.x + b * kBatch + e] = s_kcnt[acc][e];
-                s_ksum[acc][e] = 0.f;
-                s_kcnt[acc][e] = 0;
+                a.kv_sum[range.x + b * kBatch + e] = sm.ksum[acc][e];
+                a.kv_cnt[range.x + b * kBatch + e] = sm.kcnt[acc][e];
+                sm.ksum[acc][e] = 0.f;
+                sm.kcnt[acc][e] = 0;
             }
         }
         if (ndone == NT) {
-            // drain the copy still in flight before the CTA's shared memory goes away
-            if (tid == 0 && b + 1 < nb) mbar_wait(&s_bar[(b + 1) % kBufs], (uint32_t)(((b + 1) / kBufs) & 1), err);
+            // drain the copy still in flight before the buffers are reused or the CTA exits
+            if (tid == 0 && b + 1 < nb)
+                mbar_wait(&sm.bar[(g + 1) % kBufs], ((g + 1) / kBufs) & 1, err);
             if (stats) {
                 // pairs never reached contribute nothing
                 for (uint32_t e = (b + 1) * kBatch + tid; e < n; e += NT) {
-                    kv_sum[range.x + e] = 0.f;
-                    kv_cnt[range.x + e] = 0;
+                    a.kv_sum[range.x + e] = 0.f;
+                    a.kv_cnt[range.x + e] = 0;
                 }
             }
             break;
         }
-        if (tid == 0 && b + 2 < nb) {
-            const int nbuf = (b + 2) % kBufs;
-            issue_batch(s_rec[nbuf], &s_bar[nbuf], recs, range.x + (b + 2) * kBatch,
-                        min((uint32_t)kBatch, n - (b + 2) * kBatch));
+        if (b + 2 < nb) {
+            if (tid == 0) {
+                const int nbuf = (int)((g + 2) % kBufs);
+                issue_batch(sm.rec[nbuf], &sm.bar[nbuf], recs, range.x + (b + 2) * kBatch,
+                            min((uint32_t)kBatch, n - (b + 2) * kBatch));
+            }
+            issued = b + 3;
         }
     }
+    gb += (uint32_t)issued;
 
 #pragma unroll
     for (int k = 0; k < PPT; k++) {
         const int py = by * kTileY + ly0 + k;
         if (px < W && py < H) {
             const int pix = W * py + px;
-            final_T[pix] = T[k];
-            n_contrib[pix] = last[k];
-            out_color[pix] = C[k][0] + T[k] * bg[0];
-            out_color[H * W + pix] = C[k][1] + T[k] * bg[1];
-            out_color[2 * H * W + pix] = C[k][2] + T[k] * bg[2];
-            out_point_id[pix] = maxid[k];
-            out_pw_pixel[pix] = wmax[k];
+            a.final_T[pix] = T[k];
+            a.n_contrib[pix] = last[k];
+            a.out_color[pix] = C[k][0] + T[k] * a.bg[0];
+            a.out_color[H * W + pix] = C[k][1] + T[k] * a.bg[1];
+            a.out_color[2 * H * W + pix] = C[k][2] + T[k] * a.bg[2];
+            if (a.out_point_id) a.out_point_id[pix] = maxid[k];
+            if (a.out_pw_pixel) a.out_pw_pixel[pix] = wmax[k];
         }
+    }
+}
+
+template <int kBatch>
+__device__ __forceinline__ void fwd_smem_init(FwdSmem<kBatch>& sm, int NT)
+{
+    for (int e = threadIdx.x; e < 2 * kBatch; e += NT) {
+        (&sm.wmax[0][0])[e] = 0;
+        (&sm.ksum[0][0])[e] = 0.f;
+        (&sm.kcnt[0][0])[e] = 0;
+    }
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kBufs; i++) mbar_init(&sm.bar[i], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+}
+
+template <int PPT, int kBatch>
+__global__ void __launch_bounds__(256 / PPT) render_fwd_kernel(TileArgs a, unsigned* err)
+{
+    __shared__ __align__(128) FwdSmem<kBatch> sm;
+    fwd_smem_init(sm, 256 / PPT);
+    uint32_t gb = 0;
+    render_fwd_tile<PPT, kBatch>(sm, a, blockIdx.x, gb, err);
+}
+
+// Persistent multi-view forward: CTAs pop work items from one queue; item i is
+// tile (i - begin[v]) of view v.  Views are laid out in the caller's order.
+template <int PPT, int kBatch>
+__global__ void __launch_bounds__(256 / PPT)
+    render_fwd_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin, int nviews,
+                            uint32_t total, uint32_t* queue, unsigned* err)
+{
+    __shared__ __align__(128) FwdSmem<kBatch> sm;
+    __shared__ uint32_t s_item;
+    fwd_smem_init(sm, 256 / PPT);
+    uint32_t gb = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(queue, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= total) break;
+        int v = 0;
+        while (v + 1 < nviews && begin[v + 1] <= item) v++;
+        const TileArgs a = views[v];
+        render_fwd_tile<PPT, kBatch>(sm, a, (int)(item - begin[v]), gb, err);
+        __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------- backward
 template <int PPT, int kBatch>
-__global__ void __launch_bounds__(256 / PPT)
-    render_bwd_kernel(const uint2* __restrict__ ranges, const PairRecord* __restrict__ recs, int W, int H,
-                      const float* __restrict__ bg, const float* __restrict__ final_Ts,
-                      const uint32_t* __restrict__ n_contrib, const float* __restrict__ dL_dpixels,
-                      float* __restrict__ dL_dmean2D, float* __restrict__ dL_dconic, float* __restrict__ dL_dopacity,
-                      float* __restrict__ dL_dcolors, int consistent, unsigned* err)
+__device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch>& sm, const TileArgs& a, int tile, uint32_t& gb,
+                                                int consistent, unsigned* err)
 {
     constexpr int NT = 256 / PPT;
     constexpr int NG = 9;  // dcolor r,g,b ; dmean2D x,y ; dconic x,y,w ; dopacity
-    __shared__ __align__(128) PairRecord s_rec[kBufs][kBatch];
-    __shared__ __align__(8) uint64_t s_bar[kBufs];
-    __shared__ float s_acc[NG][kBatch];
-    __shared__ uint32_t s_max_last;
-
     const int tid = threadIdx.x;
+    const int W = a.W, H = a.H;
     const int gx = (W + kTileX - 1) / kTileX;
-    const int tile = blockIdx.x;
     const int bx = tile % gx, by = tile / gx;
     const int lx = tid & 15, ly0 = (tid >> 4) * PPT;
     const int px = bx * kTileX + lx;
-    const uint2 range = ranges[tile];
+    const uint2 range = a.ranges[tile];
+    const PairRecord* recs = a.recs;
 
     float T[PPT], T_final[PPT], dpix[PPT][3], accum[PPT][3], last_color[PPT][3], last_alpha[PPT], pyf[PPT];
     uint32_t last[PPT];
     float bg_dot[PPT];
-    const float bg0 = bg[0], bg1 = bg[1], bg2 = bg[2];
+    const float bg0 = a.bg[0], bg1 = a.bg[1], bg2 = a.bg[2];
     uint32_t my_max = 0;
 #pragma unroll
     for (int k = 0; k < PPT; k++) {
         const int py = by * kTileY + ly0 + k;
         const bool inside = px < W && py < H;
         const int pix = W * py + px;
-        T_final[k] = inside ? final_Ts[pix] : 0.f;
+        T_final[k] = inside ? a.final_T[pix] : 0.f;
         T[k] = T_final[k];
-        last[k] = inside ? n_contrib[pix] : 0;
+        last[k] = inside ? a.n_contrib[pix] : 0;
         my_max = max(my_max, last[k]);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            dpix[k][c] = inside ? dL_dpixels[c * H * W + pix] : 0.f;
+            dpix[k][c] = inside ? a.dL_dpix[c * H * W + pix] : 0.f;
             accum[k][c] = 0.f;
             last_color[k][c] = 0.f;
         }
@@ -409,33 +465,30 @@ __global__ void __launch_bounds__(256 / PPT)
     const float ddelx_dx = 0.5 * W;
     const float ddely_dy = 0.5 * H;
 
-    if (tid == 0) {
-        s_max_last = 0;
-        for (int i = 0; i < kBufs; i++) mbar_init(&s_bar[i], 1);
-        mbar_fence_init();
-    }
-    for (int e = tid; e < NG * kBatch; e += NT) (&s_acc[0][0])[e] = 0.f;
+    if (tid == 0) sm.max_last = 0;
     __syncthreads();
     const uint32_t warp_last = __reduce_max_sync(0xffffffffu, my_max);
-    if ((tid & 31) == 0) atomicMax(&s_max_last, warp_last);
+    if ((tid & 31) == 0) atomicMax(&sm.max_last, warp_last);
     __syncthreads();
     // Entries at or beyond the largest n_contrib of the tile touch no pixel.
-    const uint32_t n = min(range.y - range.x, s_max_last);
+    const uint32_t n = min(range.y - range.x, sm.max_last);
     const int nb = (int)((n + kBatch - 1) / kBatch);
     // batch b holds entries [lo_b, hi_b) with hi_b = n - b*kBatch (back to front)
     if (tid == 0) {
         for (int b = 0; b < 2 && b < nb; b++) {
             const uint32_t hi = n - b * kBatch, lo = hi > (uint32_t)kBatch ? hi - kBatch : 0;
-            issue_batch(s_rec[b], &s_bar[b], recs, range.x + lo, hi - lo);
+            const int buf = (int)((gb + b) % kBufs);
+            issue_batch(sm.rec[buf], &sm.bar[buf], recs, range.x + lo, hi - lo);
         }
     }
 
     for (int b = 0; b < nb; b++) {
-        const int buf = b % kBufs;
+        const uint32_t g = gb + b;
+        const int buf = (int)(g % kBufs);
         const uint32_t hi = n - b * kBatch, lo = hi > (uint32_t)kBatch ? hi - kBatch : 0;
         const uint32_t cnt = hi - lo;
-        mbar_wait(&s_bar[buf], (uint32_t)((b / kBufs) & 1), err);
-        const PairRecord* R = s_rec[buf];
+        mbar_wait(&sm.bar[buf], (g / kBufs) & 1, err);
+        const PairRecord* R = sm.rec[buf];
         for (int k0 = (int)((cnt - 1) & ~31u); k0 >= 0; k0 -= 32) {
             // records of this chunk that sit before some pixel's last contributor and can
             // reach alpha >= 1/255 inside this warp's pixels, walked back to front
@@ -453,9 +506,9 @@ __global__ void __launch_bounds__(256 / PPT)
                 const uint32_t contributor = lo + (uint32_t)j;  // 0-based position in the tile list
                 const float4 ra = R[j].a;
                 const float4 rb = R[j].b;
-                float g[NG];
+                float gr[NG];
 #pragma unroll
-                for (int q = 0; q < NG; q++) g[q] = 0.f;
+                for (int q = 0; q < NG; q++) gr[q] = 0.f;
                 bool any = false;
 #pragma unroll
                 for (int k = 0; k < PPT; k++) {
@@ -478,7 +531,7 @@ __global__ void __launch_bounds__(256 / PPT)
                         accum[k][ch] = last_alpha[k] * last_color[k][ch] + (1.f - last_alpha[k]) * accum[k][ch];
                         last_color[k][ch] = c;
                         dL_dalpha += (c - accum[k][ch]) * dpix[k][ch];
-                        g[ch] += dchannel_dcolor * dpix[k][ch];
+                        gr[ch] += dchannel_dcolor * dpix[k][ch];
                     }
                     dL_dalpha *= T[k];
                     last_alpha[k] = alpha;
@@ -490,18 +543,18 @@ __global__ void __launch_bounds__(256 / PPT)
                     const float gdy = G * d.y;
                     const float dG_ddelx = -gdx * ra.z - gdy * ra.w;
                     const float dG_ddely = -gdy * rb.x - gdx * ra.w;
-                    g[3] += dL_dG * dG_ddelx * ddelx_dx;
-                    g[4] += dL_dG * dG_ddely * ddely_dy;
-                    g[5] += -0.5f * gdx * d.x * dL_dG;
-                    g[6] += -0.5f * gdx * d.y * dL_dG;
-                    g[7] += -0.5f * gdy * d.y * dL_dG;
-                    g[8] += G * dL_dalpha;
+                    gr[3] += dL_dG * dG_ddelx * ddelx_dx;
+                    gr[4] += dL_dG * dG_ddely * ddely_dy;
+                    gr[5] += -0.5f * gdx * d.x * dL_dG;
+                    gr[6] += -0.5f * gdx * d.y * dL_dG;
+                    gr[7] += -0.5f * gdy * d.y * dL_dG;
+                    gr[8] += G * dL_dalpha;
                     any = true;
                 }
                 if (__any_sync(0xffffffffu, any)) {
-                    const float tot = warp_transpose_sum9(g);
+                    const float tot = warp_transpose_sum9(gr);
                     const unsigned lane = tid & 31;
-                    if (!(lane & 1) && (lane >> 1) < NG) atomicAdd(&s_acc[lane >> 1][j], tot);
+                    if (!(lane & 1) && (lane >> 1) < NG) atomicAdd(&sm.acc[lane >> 1][j], tot);
                 }
             }
         }
@@ -511,24 +564,67 @@ __global__ void __launch_bounds__(256 / PPT)
             float v[NG];
 #pragma unroll
             for (int q = 0; q < NG; q++) {
-                v[q] = s_acc[q][e];
-                s_acc[q][e] = 0.f;
+                v[q] = sm.acc[q][e];
+                sm.acc[q][e] = 0.f;
             }
-            if (v[0] != 0.f) atomicAdd(dL_dcolors + 3 * id, v[0]);
-            if (v[1] != 0.f) atomicAdd(dL_dcolors + 3 * id + 1, v[1]);
-            if (v[2] != 0.f) atomicAdd(dL_dcolors + 3 * id + 2, v[2]);
-            if (v[3] != 0.f) atomicAdd(dL_dmean2D + 3 * id, v[3]);
-            if (v[4] != 0.f) atomicAdd(dL_dmean2D + 3 * id + 1, v[4]);
-            if (v[5] != 0.f) atomicAdd(dL_dconic + 4 * id, v[5]);
-            if (v[6] != 0.f) atomicAdd(dL_dconic + 4 * id + 1, v[6]);
-            if (v[7] != 0.f) atomicAdd(dL_dconic + 4 * id + 3, v[7]);
-            if (v[8] != 0.f) atomicAdd(dL_dopacity + id, v[8]);
+            if (v[0] != 0.f) atomicAdd(a.dcolor + 3 * id, v[0]);
+            if (v[1] != 0.f) atomicAdd(a.dcolor + 3 * id + 1, v[1]);
+            if (v[2] != 0.f) atomicAdd(a.dcolor + 3 * id + 2, v[2]);
+            if (v[3] != 0.f) atomicAdd(a.dmean2D + 3 * id, v[3]);
+            if (v[4] != 0.f) atomicAdd(a.dmean2D + 3 * id + 1, v[4]);
+            if (v[5] != 0.f) atomicAdd(a.dconic + 4 * id, v[5]);
+            if (v[6] != 0.f) atomicAdd(a.dconic + 4 * id + 1, v[6]);
+            if (v[7] != 0.f) atomicAdd(a.dconic + 4 * id + 3, v[7]);
+            if (v[8] != 0.f) atomicAdd(a.dopac + id, v[8]);
         }
         if (tid == 0 && b + 2 < nb) {
-            const int nbuf = (b + 2) % kBufs;
+            const int nbuf = (int)((g + 2) % kBufs);
             const uint32_t hi2 = n - (b + 2) * kBatch, lo2 = hi2 > (uint32_t)kBatch ? hi2 - kBatch : 0;
-            issue_batch(s_rec[nbuf], &s_bar[nbuf], recs, range.x + lo2, hi2 - lo2);
+            issue_batch(sm.rec[nbuf], &sm.bar[nbuf], recs, range.x + lo2, hi2 - lo2);
         }
+        __syncthreads();
+    }
+    gb += (uint32_t)nb;
+}
+
+template <int kBatch>
+__device__ __forceinline__ void bwd_smem_init(BwdSmem<kBatch>& sm, int NT)
+{
+    for (int e = threadIdx.x; e < 9 * kBatch; e += NT) (&sm.acc[0][0])[e] = 0.f;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kBufs; i++) mbar_init(&sm.bar[i], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+}
+
+template <int PPT, int kBatch>
+__global__ void __launch_bounds__(256 / PPT) render_bwd_kernel(TileArgs a, int consistent, unsigned* err)
+{
+    __shared__ __align__(128) BwdSmem<kBatch> sm;
+    bwd_smem_init(sm, 256 / PPT);
+    uint32_t gb = 0;
+    render_bwd_tile<PPT, kBatch>(sm, a, blockIdx.x, gb, consistent, err);
+}
+
+template <int PPT, int kBatch>
+__global__ void __launch_bounds__(256 / PPT)
+    render_bwd_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin, int nviews,
+                            uint32_t total, uint32_t* queue, int consistent, unsigned* err)
+{
+    __shared__ __align__(128) BwdSmem<kBatch> sm;
+    __shared__ uint32_t s_item;
+    bwd_smem_init(sm, 256 / PPT);
+    uint32_t gb = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(queue, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= total) break;
+        int v = 0;
+        while (v + 1 < nviews && begin[v + 1] <= item) v++;
+        const TileArgs a = views[v];
+        render_bwd_tile<PPT, kBatch>(sm, a, (int)(item - begin[v]), gb, consistent, err);
         __syncthreads();
     }
 }
@@ -542,9 +638,12 @@ template <int PPT, int B>
 void fwd_launch(int grid, const ImageState& im, const BinState& b, int W, int H, const float* bg, float* out_color,
                 int* point_id, float* pw_pixel, float* point_weight, bool stats, unsigned* err, cudaStream_t s)
 {
-    render_fwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(im.ranges, b.rec, W, H, bg, out_color, im.final_T,
-                                                          im.n_contrib, point_id, pw_pixel, point_weight,
-                                                          stats ? b.kv_sum : nullptr, stats ? b.kv_cnt : nullptr, err);
+    TileArgs a{};
+    a.ranges = im.ranges; a.recs = b.rec; a.W = W; a.H = H; a.bg = bg;
+    a.out_color = out_color; a.final_T = im.final_T; a.n_contrib = im.n_contrib; a.out_point_id = point_id;
+    a.out_pw_pixel = pw_pixel; a.out_point_weight = point_weight;
+    a.kv_sum = stats ? b.kv_sum : nullptr; a.kv_cnt = stats ? b.kv_cnt : nullptr;
+    render_fwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(a, err);
 }
 
 template <int PPT, int B>
@@ -552,8 +651,11 @@ void bwd_launch(int grid, const ImageState& im, const BinState& b, int W, int H,
                 float* dmean2D, float* dconic, float* dopac, float* dcolor, int consistent, unsigned* err,
                 cudaStream_t s)
 {
-    render_bwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(im.ranges, b.rec, W, H, bg, im.final_T, im.n_contrib, dL,
-                                                          dmean2D, dconic, dopac, dcolor, consistent, err);
+    TileArgs a{};
+    a.ranges = im.ranges; a.recs = b.rec; a.W = W; a.H = H; a.bg = bg;
+    a.final_T = im.final_T; a.n_contrib = im.n_contrib;
+    a.dL_dpix = dL; a.dmean2D = dmean2D; a.dconic = dconic; a.dopac = dopac; a.dcolor = dcolor;
+    render_bwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(a, consistent, err);
 }
 
 #define FGS_RENDER_DISPATCH(FN, PPT_, B_, ...)                                            \
@@ -588,6 +690,51 @@ void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, co
     const RenderConfig c = g_cfg;
     FGS_RENDER_DISPATCH(fwd_launch, c.fwd_ppt, c.fwd_batch, gx * gy, im, b, W, H, bg, out_color, point_id, pw_pixel,
                         point_weight, stats, err, s);
+    note_launches(1);
+}
+
+namespace {
+template <int PPT, int B>
+void fwd_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total, uint32_t* queue,
+                      unsigned* err, cudaStream_t s)
+{
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_fwd_multi_kernel<PPT, B>, 256 / PPT, 0);
+    const int grid = sms * (per_sm > 0 ? per_sm : 1);
+    render_fwd_multi_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(views, begin, nviews, total, queue, err);
+}
+
+template <int PPT, int B>
+void bwd_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total, uint32_t* queue,
+                      int consistent, unsigned* err, cudaStream_t s)
+{
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_bwd_multi_kernel<PPT, B>, 256 / PPT, 0);
+    const int grid = sms * (per_sm > 0 ? per_sm : 1);
+    render_bwd_multi_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(views, begin, nviews, total, queue, consistent, err);
+}
+}  // namespace
+
+void launch_render_fwd_multi(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total_tiles,
+                             uint32_t* queue, unsigned* err, cudaStream_t s)
+{
+    cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
+    const RenderConfig c = g_cfg;
+    FGS_RENDER_DISPATCH(fwd_multi_launch, c.fwd_ppt, c.fwd_batch, views, begin, nviews, total_tiles, queue, err, s);
+    note_launches(1);
+}
+
+void launch_render_bwd_multi(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total_tiles,
+                             uint32_t* queue, int consistent, unsigned* err, cudaStream_t s)
+{
+    cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
+    const RenderConfig c = g_cfg;
+    FGS_RENDER_DISPATCH(bwd_multi_launch, c.bwd_ppt, c.bwd_batch, views, begin, nviews, total_tiles, queue,
+                        consistent, err, s);
     note_launches(1);
 }
 

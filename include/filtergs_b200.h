@@ -134,6 +134,44 @@ int fgs_visibility_radius(int P, const float *means3D, const float *log_scales, 
                           float radius_filter_threshold, uint8_t *mask, float *radius2d, float *depth,
                           void *stream);
 
+/* ------------------------------------------------------------------ batched views
+ * No counterpart in the reference (it renders one view per call, with a host
+ * synchronisation in each).  Many views of one Gaussian set: per view the
+ * front end runs with its pair count kept on the device, and compositing --
+ * forward and backward -- is one persistent launch over the tiles of all
+ * views.  After fgs_batch_create, forward/backward enqueue work only (no host
+ * synchronisation, no allocation), so they can be captured in a CUDA graph.
+ * Gradients of all views are summed into the shared dense outputs given at
+ * creation.  A view whose pairs exceed pair_capacity is truncated and
+ * FGS_ERR_OVERFLOW is reported by fgs_batch_check.                          */
+typedef struct fgs_view_args {
+    int width, height;
+    float tan_fovx, tan_fovy;
+    const float *viewmatrix;      /* [16] device */
+    const float *projmatrix;      /* [16] device */
+    const float *campos;          /* [3] device */
+    long long pair_capacity;      /* tile/Gaussian pairs reserved for this view */
+    float *out_color;             /* [3,H,W] forward output */
+    int *out_radii;               /* [P] or null */
+    const float *dL_dout_color;   /* [3,H,W] backward input (read by fgs_batch_backward) */
+} fgs_view_args;
+/* Workspace bytes for P Gaussians and these views (their sizes and capacities). */
+size_t fgs_batch_workspace_bytes(int P, int nviews, const fgs_view_args *views);
+/* `shared` carries the Gaussians and global settings (its camera fields are ignored).
+ * Shared gradient outputs (dense, summed over views): dL_dmeans3D [P,3], dL_dopacity [P],
+ * dL_dsh [P,M,3] (null if no SH), dL_dscales [P,3], dL_drotations [P,4] (null with cov3D_precomp).
+ * Returns a handle (null on error, *status set); synchronises `stream` once.            */
+void *fgs_batch_create(const fgs_raster_args *shared, int nviews, const fgs_view_args *views, void *workspace,
+                       size_t workspace_bytes, int backward_mode, float *dL_dmeans3D, float *dL_dopacity,
+                       float *dL_dsh, float *dL_dscales, float *dL_drotations, int *status, void *stream);
+int fgs_batch_forward(void *handle, void *stream);
+int fgs_batch_backward(void *handle, void *stream);
+/* Pair counts of the last forward per view (host [nviews]); synchronises. */
+int fgs_batch_pair_counts(void *handle, long long *counts, void *stream);
+/* Synchronise and return the first device-side error of the batch (FGS_OK when none). */
+int fgs_batch_check(void *handle, void *stream);
+void fgs_batch_destroy(void *handle);
+
 /* ------------------------------------------------------------------ LoD selection and gather
  * gather_attributes_cuda (FilterGS/cuda/gather_attributes_kernel.cu:70-145): rows of xyz/scaling [.,3],
  * rotation [.,4] (16-byte aligned), opacity [.,1], colors [.,3] and optional shs [., sh_coeffs, sh_channels]

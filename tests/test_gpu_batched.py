@@ -1,0 +1,97 @@
+"""GPU: the batched multi-view path (fgs_batch_*, CUDA-graph replay) against the
+plain one-view-per-call path.  Images and radii are bit-identical (same kernels,
+same arithmetic); the shared gradients equal the sum of the per-view gradients
+within float summation-order noise."""
+import numpy as np
+import pytest
+import torch
+
+from _helpers import S, norm_rel, ours
+from filtergs_b200 import _lib
+from filtergs_b200.batched import BatchedRasterizer, Camera
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(P=300_000, seed=5001):
+    sc = S.urban_scene(P=P, seed=seed, half_extent=150.0, buildings=60)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    return {k: (t(v) if isinstance(v, np.ndarray) else v) for k, v in sc.items()}
+
+
+def _cams(n, seed=5002):
+    rng = np.random.default_rng(seed)
+    res = [(320, 180), (640, 360), (480, 272), (250, 170)]
+    out = []
+    for i in range(n):
+        W, H = res[i % len(res)]
+        c = S.aerial_camera(rng, W=W, H=H, fx=1600.0 * W / 1920, altitude=rng.uniform(60, 120),
+                            pitch_deg=rng.uniform(30, 75), xy_range=60.0)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+        out.append(Camera(c.W, c.H, c.tanfovx, c.tanfovy, t(c.viewmatrix), t(c.projmatrix), t(c.campos)))
+    return out
+
+
+def _plain(sc, cam, dL, bg):
+    e = torch.empty(0, device="cuda")
+    f = ours.rasterize_gaussians(bg, sc["means3D"], e, sc["opacities"], sc["scales"], sc["rotations"], 1.0, e,
+                                 cam.viewmatrix, cam.projmatrix, cam.tanfovx, cam.tanfovy, cam.H, cam.W, sc["shs"], 3,
+                                 cam.campos, False, True, False, 0.2, 0.2, 0.05, 0.7, False)
+    g = ours.rasterize_gaussians_backward(bg, sc["means3D"], f[5], e, sc["scales"], sc["rotations"], 1.0, e,
+                                          cam.viewmatrix, cam.projmatrix, cam.tanfovx, cam.tanfovy, dL, sc["shs"], 3,
+                                          cam.campos, f[6], f[0], f[7], f[8], False)
+    return f, g
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batched_matches_plain(cuda, graph):
+    sc = _scene()
+    cams = _cams(6)
+    bg = torch.zeros(3, device="cuda")
+    br = BatchedRasterizer(sc["means3D"], sc["opacities"], sc["scales"], sc["rotations"], cams, shs=sc["shs"],
+                           sh_degree=3, bg=bg, graph=graph)
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    for v in range(len(cams)):
+        br.dL[v].copy_(torch.randn(br.dL[v].shape, device="cuda", generator=gen))
+    for _ in range(2):                       # replay twice: state left by the first must not leak
+        br.step()
+    br.check()
+    torch.cuda.synchronize()
+
+    def plain_sums():
+        sums = {k: torch.zeros_like(v) for k, v in br.grad.items()}
+        for v, cam in enumerate(cams):
+            f, g = _plain(sc, cam, br.dL[v], bg)
+            assert torch.equal(br.radii[v], f[5]), v
+            assert torch.equal(br.images[v], f[1]), v
+            sums["means3D"] += g[3]
+            sums["opacity"] += g[2]
+            sums["sh"] += g[5]
+            sums["scales"] += g[6]
+            sums["rotations"] += g[7]
+        return sums
+
+    a, b = plain_sums(), plain_sums()
+    for k in a:
+        # float atomics make every run differ in the last bits (the plain path against itself
+        # sets the floor; conic sums with cancellation amplify it for scales / rotations)
+        floor = norm_rel(b[k], a[k])
+        err = norm_rel(br.grad[k], a[k])
+        assert err <= max(1e-4, 5 * floor), (k, err, floor)
+    K = br.pair_counts()
+    assert all(0 < k <= c for k, c in zip(K, br.capacity))
+
+
+def test_batched_capacity_overflow_is_reported(cuda):
+    sc = _scene(P=100_000, seed=5003)
+    cams = _cams(2, seed=5004)
+    br = BatchedRasterizer(sc["means3D"], sc["opacities"], sc["scales"], sc["rotations"], cams, shs=sc["shs"],
+                           sh_degree=3, graph=False)
+    br.capacity = [max(1, c // 4) for c in br.capacity]   # far too small
+    br._build()
+    br.forward()
+    with pytest.raises(_lib.FgsError, match="too many"):
+        br.check()
+    br.replan()                                            # exact counts again
+    br.forward()
+    br.check()
