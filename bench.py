@@ -1,22 +1,31 @@
 #!/usr/bin/env python
-"""Benchmark: forward+backward views/s of the FilterGS tile rasterizer.
+"""Benchmark: forward+backward views/s of the FilterGS tile rasterizer, batched vs plain.
 
-Workload (one step = one view, forward + backward, plain one-view-per-call path):
-  urban aerial scene, 2,000,000 Gaussians (70% ground plane, 30% faces of 400 boxes),
-  SH degree 3, 1920x1080 camera at 150 m altitude, 45 deg pitch, random yaw, upstream
-  gradient ~ N(0,1).  Synthetic, seeded; 8 distinct cameras cycled over the steps.
+Workload: urban aerial scene, 2,000,000 Gaussians (70% ground plane, 30% faces of 400
+boxes), SH degree 3; 16 cameras at 1920x1080, fx=fy=1600, 150 m altitude, 45 deg pitch,
+random position and yaw; upstream gradient ~ N(0,1) per view.  Synthetic and seeded.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+One step = forward + backward of all 16 views:
+  batched (headline): one CUDA-graph replay of the batched path (per-view front ends,
+      one persistent compositing launch per direction over all views' tiles, gradients
+      summed into shared buffers; no host synchronisation);
+  plain (beside it):  16 calls of the one-view-per-call `_C` operator path.
+A second workload (the mixed-resolution batch: 16 cameras with resolutions drawn from
+{640x360, 1280x720, 1600x900, 1920x1080}, altitudes 80-300 m, pitch 30-75 deg) is
+measured the same way and reported under `mixed_resolution`.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--path batched|plain]
 
 --impl reference times the reference's own rasterizer (its CUDA sources compiled
-unmodified into oracle/_ref by oracle/build_ref.py) on the same workload, through its
-own `_C` entry points.  The reference has no CPU implementation of this path.
+unmodified into oracle/_ref by oracle/build_ref.py) on the same 16 cameras, one view per
+call through its own `_C` entry points (it has no batched path and no CPU implementation).
 
 Prints ONE JSON line (rank 0).  `value` is device-timed with CUDA events over exactly K
 steps (inputs resident in HBM; the 472 MB of Gaussian parameters exceed the 126 MB L2),
-max over ranks.  `e2e` is the same metric through the public operator API with the
-per-step camera and upstream gradient copied in from pinned host memory and the
-rendered image copied back.
+max over ranks; ranks render disjoint camera sets (weak scaling, no collective on the
+data path).  `e2e` is the same metric through the public API with every view's camera
+and upstream gradient copied in from pinned host memory and every rendered image copied
+back, inside the timed region.
 """
 import argparse
 import json
@@ -34,33 +43,40 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd views/s @2M Gaussians 1080p: batched vs plain, same GPU; HBM GB/s frac"
-WORKLOAD = "urban-aerial 2M Gaussians SH3, 1920x1080, fwd+bwd, plain one-view-per-call path"
+MIXED_RES = ((640, 360), (1280, 720), (1600, 900), (1920, 1080))
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--path", choices=["batched", "plain"], default="batched",
+                    help="the path timed as `value` (the other one is measured beside it unless --no-plain)")
     ap.add_argument("--P", type=int, default=2_000_000)
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
-    ap.add_argument("--views", type=int, default=8)
-    ap.add_argument("--stats", action="store_true", help="ogfs_enable_stats=True (the API default)")
+    ap.add_argument("--views", type=int, default=16, help="cameras per step")
+    ap.add_argument("--stats", action="store_true", help="ogfs_enable_stats=True in the plain path (API default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-resolution workload")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default render kernel shape")
     ap.add_argument("--render-config", default=None,
                     help="fwd_ppt,fwd_batch,bwd_ppt,bwd_batch (skips the autotuner)")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
+    """nvidia-smi sampled every 200 ms in the background; `window(t0, t1)` summarises the samples
+    taken between two host times (the timed region)."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
@@ -79,28 +95,19 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def wait_first(self, timeout=10.0):
-        """Block until nvidia-smi produced a sample, so its start-up never overlaps the timed region."""
+        """Block until nvidia-smi produced a sample, so its start-up never overlaps a timed region."""
         t0 = time.time()
         while self.proc is not None and not self.lines and time.time() - t0 < timeout:
             time.sleep(0.05)
-        n = len(self.lines)
-        # keep only samples taken from now on
-        self.skip = n
 
-    def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+    def window(self, t0, t1):
         sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines[getattr(self, "skip", 0):]:
+        for t, ln in list(self.lines):
+            if t < t0 or t > t1 + 0.25:
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -109,7 +116,7 @@ class ClockSampler:
                 mx.append(float(f[2]))
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
+            for n, v in zip(self.REASONS, f[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
         if not sm:
@@ -117,27 +124,50 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
                 "samples": len(sm)}
 
+    def stop(self):
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+
 
 # ---------------------------------------------------------------- workload
-def make_workload(args, device, rank):
+def make_scene(P, device):
     from filtergs_b200 import synthetic as S
-    sc = S.urban_scene(P=args.P, seed=1001)
-    rng = np.random.default_rng(2001 + 97 * rank)
-    cams = [S.aerial_camera(rng, W=args.width, H=args.height) for _ in range(args.views)]
+    sc = S.urban_scene(P=P, seed=1001)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
-    scene = dict(means3D=t(sc["means3D"]), scales=t(sc["scales"]), rotations=t(sc["rotations"]),
-                 opacities=t(sc["opacities"]), shs=t(sc["shs"]))
-    g = torch.Generator(device="cpu").manual_seed(3001 + rank)
+    return sc, dict(means3D=t(sc["means3D"]), scales=t(sc["scales"]), rotations=t(sc["rotations"]),
+                    opacities=t(sc["opacities"]), shs=t(sc["shs"]))
+
+
+def make_views(n, device, rank, W=1920, H=1080, mixed=False):
+    """n cameras of the 1080p workload, or of the mixed-resolution one (same field of view at every
+    resolution: fx scales with the width).  Rank r draws its own cameras."""
+    from filtergs_b200 import synthetic as S
+    rng = np.random.default_rng((4001 if mixed else 2001) + 97 * rank)
+    cams = []
+    for _ in range(n):
+        if mixed:
+            w, h = MIXED_RES[int(rng.integers(len(MIXED_RES)))]
+            cams.append(S.aerial_camera(rng, W=w, H=h, fx=1600.0 * w / 1920, altitude=float(rng.uniform(80, 300)),
+                                        pitch_deg=float(rng.uniform(30, 75))))
+        else:
+            cams.append(S.aerial_camera(rng, W=W, H=H))
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+    g = torch.Generator(device="cpu").manual_seed(3001 + 7 * rank + (1 if mixed else 0))
     views = []
     for c in cams:
         views.append(dict(cam=c, view=t(c.viewmatrix), proj=t(c.projmatrix), campos=t(c.campos),
                           dL=torch.randn(3, c.H, c.W, generator=g).to(device),
                           dL_host=torch.randn(3, c.H, c.W, generator=g).pin_memory()))
-    return sc, scene, views
+    return views
 
 
 def step_c(mod, scene, v, bg, stats):
-    """One forward + backward through the `_C` entry points (reference signature)."""
+    """One view forward + backward through the `_C` entry points (reference signature)."""
     e = torch.empty(0, device=bg.device)
     c = v["cam"]
     out = mod.rasterize_gaussians(bg, scene["means3D"], e, scene["opacities"], scene["scales"], scene["rotations"],
@@ -148,6 +178,21 @@ def step_c(mod, scene, v, bg, stats):
                                              e, v["view"], v["proj"], c.tanfovx, c.tanfovy, v["dL"], scene["shs"], 3,
                                              v["campos"], geom, K, binning, img, False)
     return K, radii, color, grads
+
+
+def make_batched(scene, views, bg):
+    """BatchedRasterizer over `views`; its cameras live in one packed device buffer br.cam_dev
+    [nv, 35] (view 16, proj 16, campos 3 per row)."""
+    from filtergs_b200.batched import BatchedRasterizer, Camera
+    cam_dev = torch.stack([torch.cat([v["view"].reshape(-1), v["proj"].reshape(-1), v["campos"].reshape(-1)])
+                           for v in views]).contiguous()
+    cams = [Camera(v["cam"].W, v["cam"].H, v["cam"].tanfovx, v["cam"].tanfovy, cam_dev[i, :16], cam_dev[i, 16:32],
+                   cam_dev[i, 32:35]) for i, v in enumerate(views)]
+    br = BatchedRasterizer(scene["means3D"], scene["opacities"], scene["scales"], scene["rotations"], cams,
+                           shs=scene["shs"], sh_degree=3, bg=bg, graph=True)
+    br.cam_dev = cam_dev
+    br.set_io_many(list(range(len(views))), list(br.images), [v["dL"] for v in views])
+    return br
 
 
 # algorithmic bytes per launch (per view) for each stage; K pairs, V visible, P Gaussians, N pixels
@@ -238,6 +283,150 @@ def cpu_baseline(sc, cam, threads):
                       f"scaled x{T / covered:.1f}; measured {(t1 - t0) + (t2 - t1) + t_r + t_b + t_pb:.1f}s CPU wall"}
 
 
+# ---------------------------------------------------------------- timing
+def _barrier(dist):
+    if dist:
+        torch.distributed.barrier()
+
+
+def max_over_ranks(ms, device, dist):
+    if not dist:
+        return ms
+    t = torch.tensor([ms], device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def timed(fn, steps, clocks=None):
+    """Device time (ms) of `steps` calls of fn(i): CUDA events on the launching stream, synchronised
+    on both sides.  Returns (ms, clock summary of the region)."""
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    a.record()
+    for i in range(steps):
+        fn(i)
+    b.record()
+    torch.cuda.synchronize()
+    t1 = time.time()
+    return a.elapsed_time(b), (clocks.window(t0, t1) if clocks else None)
+
+
+def profiled(fn, steps):
+    """Per-stage CUDA-event times of `steps` eager calls of fn(i) (events recorded around each launch
+    group on the stream it runs on) and the number of kernels launched."""
+    from filtergs_b200 import _lib
+    torch.cuda.synchronize()
+    _lib.profile_read(reset=True)
+    _lib.profile_enable(True)
+    l0 = _lib.launch_count()
+    for i in range(steps):
+        fn(i)
+    torch.cuda.synchronize()
+    launches = _lib.launch_count() - l0
+    _lib.profile_enable(False)
+    return _lib.profile_read(reset=True), launches
+
+
+def autotune(args, fn, key, rank):
+    from filtergs_b200 import _lib
+    if args.render_config:
+        _lib.set_render_config(*[int(x) for x in args.render_config.split(",")])
+        return None
+    if args.no_autotune:
+        return None
+    from filtergs_b200.autotune import tune_render
+    it = iter(range(1 << 30))
+    tuned, table = tune_render(lambda: fn(next(it)), key=key)
+    if rank == 0:
+        print(f"autotune {key[0]} (ppt,batch)->(fwd ms, bwd ms): " +
+              ", ".join(f"{k}:{v[0]:.3f}/{v[1]:.3f}" for k, v in sorted(table.items())), file=sys.stderr)
+    return list(tuned)
+
+
+def measure_plain(args, mod, scene, views, bg, dev, dist, rank, ours=True, clocks=None, profile=False):
+    """K steps of the plain path: each step renders (forward + backward) every view, one call each."""
+    nv = len(views)
+    tuned = None
+    if ours:
+        tuned = autotune(args, lambda i: step_c(mod, scene, views[i % nv], bg, args.stats),
+                         ("plain", args.P, tuple((v["cam"].W, v["cam"].H) for v in views)), rank)
+    for _ in range(args.warmup):
+        for v in views:
+            step_c(mod, scene, v, bg, args.stats)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    first = []
+
+    def one(i):
+        for v in views:
+            K, radii, color, grads = step_c(mod, scene, v, bg, args.stats)
+            if i == 0:
+                first.append((K, radii))
+
+    ms, clk = timed(one, args.steps, clocks)
+    ms = max_over_ranks(ms, dev, dist)
+    out = dict(ms=ms, clocks=clk, tuned=tuned, K=[int(k) for k, _ in first],
+               vis=[int((r > 0).sum().item()) for _, r in first])
+    if ours and profile:
+        out["prof"], out["launches"] = profiled(one, args.steps)
+    return out
+
+
+def measure_batched(args, scene, views, bg, dev, dist, rank, clocks=None, profile=True):
+    """K steps of the batched path: each step is one CUDA-graph replay of forward + backward of all views."""
+    br = make_batched(scene, views, bg)
+    tuned = autotune(args, lambda i: (br.forward(), br.backward()),
+                     ("batched", args.P, tuple((v["cam"].W, v["cam"].H) for v in views)), rank)
+    for _ in range(args.warmup):
+        br.step()                       # the first replay captures the graph (after the autotuner)
+    br.check()
+    _barrier(dist)
+    ms, clk = timed(lambda i: br.step(), args.steps, clocks)
+    br.check()
+    ms = max_over_ranks(ms, dev, dist)
+    out = dict(ms=ms, clocks=clk, tuned=tuned, br=br, K=br.pair_counts(),
+               vis=[int((r > 0).sum().item()) for r in br.radii])
+    if profile:
+        # per-launch times cannot be taken inside a graph replay: the same K steps again, eagerly
+        out["prof"], out["launches"] = profiled(lambda i: (br.forward(), br.backward()), args.steps)
+        br.check()
+    return out
+
+
+def roofline(prof, P, views, K, vis, batched):
+    """Roofline of the dominant kernel: algorithmic bytes per launch / its mean CUDA-event duration."""
+    dom = max(prof, key=lambda k: prof[k][0])
+    calls = max(1, prof[dom][1])
+    per_call_ms = prof[dom][0] / calls
+
+    def bytes_of(stage, v, k, n):
+        c = views[v]["cam"]
+        T = ((c.W + 15) // 16) * ((c.H + 15) // 16)
+        return algo_bytes(stage, P, n, k, c.W * c.H, T)
+
+    if batched and dom in ("render_fwd", "render_bwd"):
+        ab = sum(bytes_of(dom, v, K[v], vis[v]) for v in range(len(views)))   # one launch covers all views
+        key = "batched." + dom
+    else:
+        ab = float(np.mean([bytes_of(dom, v, K[v], vis[v]) for v in range(len(views))]))
+        key = ("batched." if batched else "") + dom
+    peak, kind = measured_peak()
+    achieved = ab / (per_call_ms / 1000.0) / 1e9
+    return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": ncu_traffic(key), "algorithmic_bytes_per_launch": ab,
+            "launch_ms": per_call_ms, "peak_source": f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured"
+            else "fallback 6650 GB/s",
+            "timing": "CUDA events around each launch, eager pass of the same K steps" if batched
+            else "CUDA events around each launch over the timed steps",
+            "note": "the compositing kernels are FP32/SFU issue-bound (exp per pixel-splat pair), not DRAM-bound"}
+
+
+def stages_of(prof):
+    return {k: {"ms_total": v[0], "launch_groups": v[1], "ms_per_call": (v[0] / v[1]) if v[1] else 0.0}
+            for k, v in prof.items() if v[1]}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -252,7 +441,8 @@ def main():
         torch.distributed.destroy_process_group()
         return
     torch.cuda.set_device(local)
-    device = torch.device("cuda", local)
+    dev = torch.device("cuda", local)
+    ref_dist = dist and args.impl != "reference"
 
     if args.impl == "reference":
         from oracle import build_ref
@@ -266,211 +456,255 @@ def main():
             return
     else:
         from filtergs_b200 import _C as mod
-        from filtergs_b200 import _lib
 
-    sc, scene, views = make_workload(args, device, rank)
-    bg = torch.zeros(3, device=device)
+    sc, scene = make_scene(args.P, dev)
+    views = make_views(args.views, dev, rank, args.width, args.height)
+    bg = torch.zeros(3, device=dev)
     nv = len(views)
-    tuned = None
-    if args.impl == "ours" and args.render_config:
-        _lib.set_render_config(*[int(x) for x in args.render_config.split(",")])
-    elif args.impl == "ours" and not args.no_autotune:
-        from filtergs_b200.autotune import tune_render
-        it = iter(range(1 << 30))
-        tuned, table = tune_render(lambda: step_c(mod, scene, views[next(it) % nv], bg, args.stats),
-                                   key=("urban", args.P, args.width, args.height))
-        if rank == 0:
-            print("autotune render (ppt,batch)->(fwd ms, bwd ms): " +
-                  ", ".join(f"{k}:{v[0]:.3f}/{v[1]:.3f}" for k, v in sorted(table.items())), file=sys.stderr)
+    n_ranks = world if args.impl == "ours" else 1
     clocks = ClockSampler(local) if rank == 0 else None
     if clocks:
         clocks.start()
         clocks.wait_first()
-    for i in range(args.warmup):
-        step_c(mod, scene, views[i % nv], bg, args.stats)
-    torch.cuda.synchronize()
-    if dist and args.impl == "ours":
-        torch.distributed.barrier()
-    if clocks:
-        clocks.skip = len(clocks.lines)
-    if args.impl == "ours":
-        _lib.profile_read(reset=True)
-        _lib.profile_enable(True)
-        l0 = _lib.launch_count()
-    Ks, Vs = [], []
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    start.record()
-    for i in range(args.steps):
-        K, radii, color, grads = step_c(mod, scene, views[i % nv], bg, args.stats)
-        Ks.append(K)
-        Vs.append(radii)
-    end.record()
-    torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
-    if args.impl == "ours":
-        launches = _lib.launch_count() - l0
-        _lib.profile_enable(False)
-        prof = _lib.profile_read(reset=True)
-    clk = clocks.stop() if clocks else None
-    Vs = [int((r > 0).sum().item()) for r in Vs]
-    if dist and args.impl == "ours":
-        t = torch.tensor([ms], device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    n_ranks = world if args.impl == "ours" else 1
-    value = n_ranks * args.steps / (ms / 1000.0)
 
-    # ---------------------------------------------------------------- e2e through the public API
+    plain = mixed = None
+    if args.impl == "reference":
+        head = measure_plain(args, mod, scene, views, bg, dev, False, rank, ours=False, clocks=clocks)
+        path = "plain"
+    elif args.path == "batched":
+        head = measure_batched(args, scene, views, bg, dev, ref_dist, rank, clocks=clocks)
+        path = "batched"
+    else:
+        head = measure_plain(args, mod, scene, views, bg, dev, ref_dist, rank, clocks=clocks, profile=True)
+        path = "plain"
+    value = n_ranks * nv * args.steps / (head["ms"] / 1000.0)
+
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, mod, scene, views, bg, device, dist)
-
-    result = None
-    if rank == 0:
-        cfg = {"workload": WORKLOAD, "gaussians": args.P, "width": args.width, "height": args.height, "sh_degree": 3,
-               "views_cycled": nv, "path": "plain", "ogfs_enable_stats": bool(args.stats),
-               "l2": "inputs larger than L2 (472 MB Gaussian parameters per step)",
-               "mean_pairs_K": float(np.mean(Ks)), "mean_visible_V": float(np.mean(Vs))}
-        result = {"metric": METRIC, "value": value, "unit": "views/s", "n_gpus": n_ranks, "steps": args.steps,
-                  "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-                  "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded urban-aerial scene)",
-                  "config": cfg}
-        if args.impl == "reference":
-            result["impl"] = "reference"
-            result["cpu_baseline"] = {"value": value, "unit": "views/s", "cores": 1, "kind": "reference",
-                                      "sample": "the reference's own rasterizer (CUDA sources compiled unmodified, "
-                                                "oracle/_ref) on this GPU; it has no CPU implementation"}
-            if e2e:
-                result["e2e"] = e2e
-            else:
-                result["e2e"] = {"value": value, "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+        if path == "batched":
+            e2e = e2e_batched(args, head["br"], views, dev, ref_dist, n_ranks)
         else:
-            P, N = args.P, args.width * args.height
-            T = ((args.width + 15) // 16) * ((args.height + 15) // 16)
-            Km, Vm = float(np.mean(Ks)), float(np.mean(Vs))
-            stages = {k: {"ms_total": v[0], "launch_groups": v[1], "ms_per_call": (v[0] / v[1]) if v[1] else 0.0}
-                      for k, v in prof.items()}
-            dom = max(prof, key=lambda k: prof[k][0])
-            peak, peak_kind = measured_peak()
-            per_call_ms = prof[dom][0] / max(1, prof[dom][1])
-            ab = algo_bytes(dom, P, Vm, Km, N, T)
-            achieved = ab / (per_call_ms / 1000.0) / 1e9
-            result["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                                  "unit": "GB/s", "frac": achieved / peak, "traffic": ncu_traffic(dom),
-                                  "algorithmic_bytes_per_launch": ab, "peak_source": peak_kind,
-                                  "note": "render kernels are exp/FP32-issue bound; see profiles/ for pipe utilisation"}
-            result["stages"] = stages
-            result["config"]["render_config"] = list(_lib.get_render_config())
-            result["config"]["autotuned"] = tuned is not None
-            result["gpu_launches"] = int(launches)
+            e2e = e2e_plain(args, mod, scene, views, bg, dev, ref_dist if args.impl == "ours" else False, n_ranks)
+    if "br" in head:
+        del head["br"]
+        torch.cuda.empty_cache()
+    if args.impl == "ours" and path == "batched" and not args.no_plain:
+        plain = measure_plain(args, mod, scene, views, bg, dev, ref_dist, rank)
+    if args.impl == "ours" and path == "batched" and not args.no_mixed:
+        mv = make_views(args.views, dev, rank, mixed=True)
+        mb = measure_batched(args, scene, mv, bg, dev, ref_dist, rank, profile=False)
+        del mb["br"]
+        torch.cuda.empty_cache()
+        mp = measure_plain(args, mod, scene, mv, bg, dev, ref_dist, rank)
+        mixed = {"resolutions": [f"{v['cam'].W}x{v['cam'].H}" for v in mv],
+                 "batched_value": n_ranks * nv * args.steps / (mb["ms"] / 1000.0),
+                 "plain_value": n_ranks * nv * args.steps / (mp["ms"] / 1000.0),
+                 "unit": "views/s", "batched_render_config": mb["tuned"], "plain_render_config": mp["tuned"],
+                 "pairs_K": mb["K"], "visible_V": mb["vis"], "altitude_m": "80-300", "pitch_deg": "30-75"}
+    if clocks:
+        clocks.stop()
+
+    if rank == 0:
+        cfg = {"workload": f"urban-aerial {args.P / 1e6:g}M Gaussians SH3, {nv} cameras {args.width}x{args.height} "
+                           f"per step, fwd+bwd, {path} path",
+               "gaussians": args.P, "width": args.width, "height": args.height, "sh_degree": 3,
+               "views_per_step": nv, "path": path,
+               "l2": "inputs larger than L2 (472 MB Gaussian parameters read per view)",
+               "pairs_K": head["K"], "visible_V": head["vis"], "mean_pairs_K": float(np.mean(head["K"])),
+               "mean_visible_V": float(np.mean(head["vis"]))}
+        if path == "plain":
+            cfg["ogfs_enable_stats"] = bool(args.stats)
+        res = {"metric": METRIC, "value": value, "unit": "views/s", "n_gpus": n_ranks, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded urban-aerial scene and cameras)", "config": cfg}
+        if args.impl == "reference":
+            res["impl"] = "reference"
+            res["cpu_baseline"] = {"value": value, "unit": "views/s", "cores": 1, "kind": "reference",
+                                   "sample": "the reference's own rasterizer (CUDA sources compiled unmodified, "
+                                             "oracle/_ref) on this GPU, one view per call; it has no CPU "
+                                             "implementation of the path"}
+            res["e2e"] = e2e or {"value": value, "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+        else:
+            cfg["render_config"] = head["tuned"]
+            res["roofline"] = roofline(head["prof"], args.P, views, head["K"], head["vis"], path == "batched")
+            res["stages"] = stages_of(head["prof"])
+            res["gpu_launches"] = int(head["launches"])
+            if plain:
+                res["plain"] = {"value": n_ranks * nv * args.steps / (plain["ms"] / 1000.0), "unit": "views/s",
+                                "ms_per_step": plain["ms"] / args.steps, "render_config": plain["tuned"],
+                                "clocks": plain["clocks"]}
+            if mixed:
+                res["mixed_resolution"] = mixed
             if e2e:
-                result["e2e"] = e2e
+                res["e2e"] = e2e
             if not args.no_cpu_baseline:
-                result["cpu_baseline"] = cpu_baseline(sc, views[0]["cam"], os.cpu_count() or 1)
-        if clk:
-            result["clocks"] = clk
-        print(json.dumps(result), flush=True)
+                res["cpu_baseline"] = cpu_baseline(sc, views[0]["cam"], os.cpu_count() or 1)
+        if head["clocks"]:
+            res["clocks"] = head["clocks"]
+        print(json.dumps(res), flush=True)
     if dist:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
 
 
-def run_e2e(args, mod, scene, views, bg, device, dist):
-    """Same metric through the public API: per step, H2D of the camera and the upstream gradient from
-    pinned host memory, forward + backward, D2H of the rendered image.  The copies run on a side stream:
-    step i+1's inputs are uploaded while step i computes, and step i's image is downloaded while its
-    backward runs, as a pipelined caller would do; every step still moves its own bytes."""
+# ---------------------------------------------------------------- end to end through the public API
+def e2e_plain(args, mod, scene, views, bg, dev, dist, n_ranks):
+    """Plain path through the public API: per view, H2D of its camera and upstream gradient from
+    pinned host memory, forward + backward, D2H of the rendered image.  The copies run on a side
+    stream (view j+1's inputs upload while view j computes, view j's image downloads while its
+    backward runs), as a pipelined caller would do; every view still moves its own bytes."""
     nv = len(views)
-    c0 = views[0]["cam"]
     host_cam = [torch.from_numpy(np.concatenate([v["cam"].viewmatrix.reshape(-1), v["cam"].projmatrix.reshape(-1),
-                                                 v["cam"].campos])).pin_memory() for v in views]
-    out_host = [torch.empty(3, c0.H, c0.W).pin_memory() for _ in range(2)]
-    dev_cam = [torch.empty(35, device=device) for _ in range(2)]
-    dev_dL = [torch.empty(3, c0.H, c0.W, device=device) for _ in range(2)]
-    copy = torch.cuda.Stream(device=device)
-    main = torch.cuda.current_stream(device)
-    if args.impl == "ours":
+                                                 v["cam"].campos]).astype(np.float32)).pin_memory() for v in views]
+    out_host = [[torch.empty(3, v["cam"].H, v["cam"].W).pin_memory() for v in views] for _ in range(2)]
+    dev_cam = [torch.empty(35, device=dev) for _ in range(2)]
+    dev_dL = [[torch.empty(3, v["cam"].H, v["cam"].W, device=dev) for v in views] for _ in range(2)]
+    copy = torch.cuda.Stream(device=dev)
+    main = torch.cuda.current_stream(dev)
+    ours = args.impl == "ours"
+    if ours:
         from filtergs_b200.rasterization import GaussianRasterizationSettings, GaussianRasterizer
-        means = scene["means3D"].clone().requires_grad_(True)
-        shs = scene["shs"].clone().requires_grad_(True)
-        op = scene["opacities"].clone().requires_grad_(True)
-        scl = scene["scales"].clone().requires_grad_(True)
-        rot = scene["rotations"].clone().requires_grad_(True)
-        m2 = torch.zeros_like(means, requires_grad=True)
+        params = [scene[k].clone().requires_grad_(True) for k in ("means3D", "shs", "opacities", "scales",
+                                                                  "rotations")]
+        m2 = torch.zeros_like(params[0], requires_grad=True)
     ready = [torch.cuda.Event() for _ in range(2)]
     freed = [torch.cuda.Event() for _ in range(2)]
+    total = [0]
 
-    def upload(i):
-        b = i & 1
+    def upload(j):
+        b, v = j & 1, j % nv
         with torch.cuda.stream(copy):
             copy.wait_event(freed[b])
-            dev_cam[b].copy_(host_cam[i % nv], non_blocking=True)
-            dev_dL[b].copy_(views[i % nv]["dL_host"], non_blocking=True)
+            dev_cam[b].copy_(host_cam[v], non_blocking=True)
+            dev_dL[b][v].copy_(views[v]["dL_host"], non_blocking=True)
             ready[b].record(copy)
 
-    def one(i):
-        b = i & 1
-        v = views[i % nv]
-        c = v["cam"]
+    def one(j):
+        b, v = j & 1, j % nv
+        c = views[v]["cam"]
         main.wait_event(ready[b])
-        if i + 1 < total[0]:
-            upload(i + 1)
+        if j + 1 < total[0]:
+            upload(j + 1)
         view, proj, cpos = dev_cam[b][:16].view(4, 4), dev_cam[b][16:32].view(4, 4), dev_cam[b][32:35]
-        if args.impl == "ours":
+        if ours:
             rs = GaussianRasterizationSettings(c.H, c.W, c.tanfovx, c.tanfovy, bg, 1.0, view, proj, 3, cpos, False,
                                                False, ogfs_enable_stats=bool(args.stats))
-            for t in (means, shs, op, scl, rot, m2):
+            for t in params + [m2]:
                 t.grad = None
+            means, shs, op, scl, rot = params
             color = GaussianRasterizer(rs)(means, m2, op, shs=shs, scales=scl, rotations=rot)[0]
-            img_done = torch.cuda.Event()
-            img_done.record(main)
-            with torch.cuda.stream(copy):
-                copy.wait_event(img_done)
-                out_host[b].copy_(color.detach(), non_blocking=True)
-            color.backward(dev_dL[b])
         else:
-            e = torch.empty(0, device=device)
+            e = torch.empty(0, device=dev)
             out = mod.rasterize_gaussians(bg, scene["means3D"], e, scene["opacities"], scene["scales"],
                                           scene["rotations"], 1.0, e, view, proj, c.tanfovx, c.tanfovy, c.H, c.W,
                                           scene["shs"], 3, cpos, False, True, False, 0.2, 0.2, 0.05, 0.7, args.stats)
             K, color, pid, pwp, pw, radii, geom, binning, img, st = out
-            img_done = torch.cuda.Event()
-            img_done.record(main)
-            with torch.cuda.stream(copy):
-                copy.wait_event(img_done)
-                out_host[b].copy_(color, non_blocking=True)
+        img_done = torch.cuda.Event()
+        img_done.record(main)
+        with torch.cuda.stream(copy):
+            copy.wait_event(img_done)
+            out_host[b][v].copy_(color.detach(), non_blocking=True)
+        if ours:
+            color.backward(dev_dL[b][v])
+        else:
             mod.rasterize_gaussians_backward(bg, scene["means3D"], radii, e, scene["scales"], scene["rotations"], 1.0,
-                                             e, view, proj, c.tanfovx, c.tanfovy, dev_dL[b], scene["shs"], 3, cpos,
+                                             e, view, proj, c.tanfovx, c.tanfovy, dev_dL[b][v], scene["shs"], 3, cpos,
                                              geom, K, binning, img, False)
         freed[b].record(main)
 
-    total = [args.warmup]
-    upload(0)
-    for i in range(args.warmup):
-        one(i)
+    def run(nviews):
+        total[0] = nviews
+        upload(0)
+        for j in range(nviews):
+            one(j)
+
+    run(args.warmup * nv)
     torch.cuda.synchronize()
-    if dist and args.impl == "ours":
-        torch.distributed.barrier()
-    total[0] = args.steps
+    _barrier(dist)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record()
     copy.wait_event(start)
-    upload(0)
-    for i in range(args.steps):
-        one(i)
+    run(args.steps * nv)
     main.wait_stream(copy)      # the last image download is inside the timed region
     end.record()
-    end.synchronize()
-    ms = start.elapsed_time(end)
     torch.cuda.synchronize()
-    if dist and args.impl == "ours":
-        t = torch.tensor([ms], device=device)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    n_ranks = (int(os.environ.get("WORLD_SIZE", "1")) if args.impl == "ours" else 1)
-    return {"value": n_ranks * args.steps / (ms / 1000.0), "unit": "views/s",
-            "h2d_bytes_per_step": int(35 * 4 + 3 * c0.H * c0.W * 4), "d2h_bytes_per_step": int(3 * c0.H * c0.W * 4)}
+    ms = max_over_ranks(start.elapsed_time(end), dev, dist)
+    px = sum(v["cam"].W * v["cam"].H for v in views)
+    return {"value": n_ranks * args.steps * nv / (ms / 1000.0), "unit": "views/s",
+            "h2d_bytes_per_step": int(nv * 35 * 4 + 3 * px * 4), "d2h_bytes_per_step": int(3 * px * 4),
+            "api": "GaussianRasterizer (autograd)" if ours else "reference _C rasterize_gaussians(+_backward)"}
+
+
+def e2e_batched(args, br, views, dev, dist, n_ranks):
+    """Batched path through its public API (BatchedRasterizer): per step, H2D of all cameras and all
+    upstream gradients from pinned host memory, one graph replay, D2H of every rendered image.
+    Images and gradients are double-buffered (set_io_many re-targets the captured graph), so step
+    i+1's uploads and step i's downloads overlap step i+1's compute on two copy streams."""
+    nv = len(views)
+    cam_host = torch.from_numpy(np.stack([np.concatenate([v["cam"].viewmatrix.reshape(-1),
+                                                          v["cam"].projmatrix.reshape(-1), v["cam"].campos])
+                                          for v in views]).astype(np.float32)).pin_memory()
+    cam_stage = [torch.empty(nv, 35, device=dev) for _ in range(2)]
+    imgs = [[torch.empty(3, v["cam"].H, v["cam"].W, device=dev) for v in views] for _ in range(2)]
+    dls = [[torch.empty(3, v["cam"].H, v["cam"].W, device=dev) for v in views] for _ in range(2)]
+    out_host = [[torch.empty(3, v["cam"].H, v["cam"].W).pin_memory() for v in views] for _ in range(2)]
+    h2d, d2h = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+    main = torch.cuda.current_stream(dev)
+    ready = [torch.cuda.Event() for _ in range(2)]
+    freed = [torch.cuda.Event() for _ in range(2)]
+    downloaded = [torch.cuda.Event() for _ in range(2)]
+    ids = list(range(nv))
+    total = [0]
+
+    def upload(i):
+        b = i & 1
+        with torch.cuda.stream(h2d):
+            h2d.wait_event(freed[b])
+            cam_stage[b].copy_(cam_host, non_blocking=True)
+            for v in range(nv):
+                dls[b][v].copy_(views[v]["dL_host"], non_blocking=True)
+            ready[b].record(h2d)
+
+    def one(i):
+        b = i & 1
+        main.wait_event(ready[b])
+        main.wait_event(downloaded[b])
+        br.cam_dev.copy_(cam_stage[b])      # the captured kernels read the cameras from these rows
+        br.set_io_many(ids, imgs[b], dls[b])
+        br.step()
+        freed[b].record(main)
+        if i + 1 < total[0]:
+            upload(i + 1)
+        with torch.cuda.stream(d2h):
+            d2h.wait_event(freed[b])
+            for v in range(nv):
+                out_host[b][v].copy_(imgs[b][v], non_blocking=True)
+            downloaded[b].record(d2h)
+
+    def run(n):
+        total[0] = n
+        upload(0)
+        for i in range(n):
+            one(i)
+
+    run(args.warmup)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    h2d.wait_event(start)
+    d2h.wait_event(start)
+    run(args.steps)
+    main.wait_stream(d2h)       # the last downloads are inside the timed region
+    end.record()
+    torch.cuda.synchronize()
+    br.check()
+    ms = max_over_ranks(start.elapsed_time(end), dev, dist)
+    px = sum(v["cam"].W * v["cam"].H for v in views)
+    return {"value": n_ranks * args.steps * nv / (ms / 1000.0), "unit": "views/s",
+            "h2d_bytes_per_step": int(nv * 35 * 4 + 3 * px * 4), "d2h_bytes_per_step": int(3 * px * 4),
+            "api": "BatchedRasterizer.step (CUDA-graph replay)"}
 
 
 if __name__ == "__main__":

@@ -166,6 +166,30 @@ class BatchedRasterizer:
         _lib.check(_L().fgs_batch_backward(self.handle, _s()), "fgs_batch_backward")
         return self.grad
 
+    def set_io(self, view, image, dL=None):
+        """Point view `view` at another image buffer (and upstream gradient) for the steps that follow
+        on the current stream; a captured graph follows without re-capture (double-buffered I/O)."""
+        self.set_io_many([view], [image], [dL])
+
+    def set_io_many(self, views, images, dLs=None):
+        dLs = dLs if dLs is not None else [None] * len(views)
+        for v, img, d in zip(views, images, dLs):
+            c = self.cams[v]
+            for t in (img, d):
+                if t is not None and (tuple(t.shape) != (3, c.H, c.W) or t.dtype != torch.float32 or
+                                      not t.is_contiguous() or t.device != self.dev):
+                    raise ValueError(f"view {v}: expected a contiguous float32 [3,{c.H},{c.W}] tensor on {self.dev}")
+        n = len(views)
+        ids = (C.c_int * n)(*[int(v) for v in views])
+        outs = (C.c_void_p * n)(*[t.data_ptr() for t in images])
+        dls = (C.c_void_p * n)(*[(t.data_ptr() if t is not None else None) for t in dLs])
+        _lib.check(_L().fgs_batch_set_view_io(self.handle, n, C.cast(ids, C.c_void_p), C.cast(outs, C.c_void_p),
+                                              C.cast(dls, C.c_void_p), _s()), "fgs_batch_set_view_io")
+        for v, img, d in zip(views, images, dLs):
+            self.images[v] = img
+            if d is not None:
+                self.dL[v] = d
+
     def pair_counts(self):
         out = (C.c_longlong * self.V)()
         _lib.check(_L().fgs_batch_pair_counts(self.handle, C.cast(out, C.c_void_p), _s()), "fgs_batch_pair_counts")

@@ -33,80 +33,116 @@ __device__ __forceinline__ float3 dnormvdv(float3 v, float3 dv)
     return r;
 }
 
-// backward.cu:20-139 for one Gaussian; sh / dsh are its [M][3] rows (added to
-// dsh instead of stored when kAccum).
+// backward.cu:20-139 for one Gaussian; shrow / dsh are its [M][3] rows (added to
+// dsh instead of stored when kAccum; vec: both rows 16-byte aligned, M*3 % 4 == 0).
+// dL/dsh depends only on the direction, so it is written before the SH row is
+// read: the two 48-float sets are never live at the same time.
 template <bool kAccum>
-__device__ __forceinline__ float3 sh_backward(int deg, const float* __restrict__ sh, float3 pos, float3 campos,
-                                              uint8_t clamp_bits, float3 dcol, float* __restrict__ dsh, int M)
+__device__ __forceinline__ float3 sh_backward(int deg, const float* __restrict__ shrow, float3 pos, float3 campos,
+                                              uint8_t clamp_bits, float3 dcol, float* __restrict__ dsh, int M,
+                                              bool vec)
 {
     const float3 dir_orig = {pos.x - campos.x, pos.y - campos.y, pos.z - campos.z};
     const float len = sqrtf(dir_orig.x * dir_orig.x + dir_orig.y * dir_orig.y + dir_orig.z * dir_orig.z);
     const float x = dir_orig.x / len, y = dir_orig.y / len, z = dir_orig.z / len;
-    float d[3] = {(clamp_bits & 1) ? 0.f : dcol.x, (clamp_bits & 2) ? 0.f : dcol.y, (clamp_bits & 4) ? 0.f : dcol.z};
-    float dx[3] = {0.f, 0.f, 0.f}, dy[3] = {0.f, 0.f, 0.f}, dz[3] = {0.f, 0.f, 0.f};
-    float g[48];
+    const float d[3] = {(clamp_bits & 1) ? 0.f : dcol.x, (clamp_bits & 2) ? 0.f : dcol.y,
+                        (clamp_bits & 4) ? 0.f : dcol.z};
+    const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+    // basis values (dL/dsh[i][c] = B[i] * d[c])
+    float B[16];
+    B[0] = kSH_C0;
+    B[1] = -kSH_C1 * y;
+    B[2] = kSH_C1 * z;
+    B[3] = -kSH_C1 * x;
+    B[4] = kSH_C2_0 * xy;
+    B[5] = kSH_C2_1 * yz;
+    B[6] = kSH_C2_2 * (2.f * zz - xx - yy);
+    B[7] = kSH_C2_3 * xz;
+    B[8] = kSH_C2_4 * (xx - yy);
+    B[9] = kSH_C3_0 * y * (3.f * xx - yy);
+    B[10] = kSH_C3_1 * xy * z;
+    B[11] = kSH_C3_2 * y * (4.f * zz - xx - yy);
+    B[12] = kSH_C3_3 * z * (2.f * zz - 3.f * xx - 3.f * yy);
+    B[13] = kSH_C3_4 * x * (4.f * zz - xx - yy);
+    B[14] = kSH_C3_5 * z * (xx - yy);
+    B[15] = kSH_C3_6 * x * (xx - 3.f * yy);
+    const int ncoef = (deg + 1) * (deg + 1);
+    const int nfl = M * 3;
+#define FGS_DSH(f) (((f) / 3 < ncoef) ? B[(f) / 3] * d[(f) % 3] : 0.f)
+    if (vec) {
+        float4* d4 = reinterpret_cast<float4*>(dsh);
 #pragma unroll
-    for (int c = 0; c < 3; c++) g[c] = kSH_C0 * d[c];
-    if (deg > 0) {
+        for (int v = 0; v < 12; v++)
+            if (4 * v < nfl) {
+                float4 o = make_float4(FGS_DSH(4 * v), FGS_DSH(4 * v + 1), FGS_DSH(4 * v + 2), FGS_DSH(4 * v + 3));
+                if (kAccum) {
+                    const float4 a = d4[v];
+                    o.x += a.x; o.y += a.y; o.z += a.z; o.w += a.w;
+                }
+                d4[v] = o;
+            }
+    } else {
+#pragma unroll
+        for (int f = 0; f < 48; f++)
+            if (f < nfl) {
+                if (kAccum) dsh[f] += FGS_DSH(f);
+                else dsh[f] = FGS_DSH(f);
+            }
+    }
+#undef FGS_DSH
+    if (!kAccum)
+        for (int f = 48; f < nfl; f++) dsh[f] = 0.f;
+    if (deg == 0) return make_float3(0.f, 0.f, 0.f);
+
+    // dRGB/ddir (backward.cu:59-124 expression order) from the SH row
+    float sh[48];
+    const int nf = min(48, nfl);
+    if (vec) {
+        const float4* r4 = reinterpret_cast<const float4*>(shrow);
+#pragma unroll
+        for (int v = 0; v < 12; v++)
+            if (4 * v < nf) {
+                const float4 q = __ldg(r4 + v);
+                sh[4 * v] = q.x; sh[4 * v + 1] = q.y; sh[4 * v + 2] = q.z; sh[4 * v + 3] = q.w;
+            }
+    } else {
+#pragma unroll
+        for (int f = 0; f < 48; f++)
+            if (f < nf) sh[f] = __ldg(shrow + f);
+    }
+    float dx[3], dy[3], dz[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        dx[c] = -kSH_C1 * sh[9 + c];
+        dy[c] = -kSH_C1 * sh[3 + c];
+        dz[c] = kSH_C1 * sh[6 + c];
+    }
+    if (deg > 1) {
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            g[3 + c] = -kSH_C1 * y * d[c];
-            g[6 + c] = kSH_C1 * z * d[c];
-            g[9 + c] = -kSH_C1 * x * d[c];
-            dx[c] = -kSH_C1 * sh[9 + c];
-            dy[c] = -kSH_C1 * sh[3 + c];
-            dz[c] = kSH_C1 * sh[6 + c];
+            dx[c] += kSH_C2_0 * y * sh[12 + c] + kSH_C2_2 * 2.f * -x * sh[18 + c] + kSH_C2_3 * z * sh[21 + c] +
+                     kSH_C2_4 * 2.f * x * sh[24 + c];
+            dy[c] += kSH_C2_0 * x * sh[12 + c] + kSH_C2_1 * z * sh[15 + c] + kSH_C2_2 * 2.f * -y * sh[18 + c] +
+                     kSH_C2_4 * 2.f * -y * sh[24 + c];
+            dz[c] += kSH_C2_1 * y * sh[15 + c] + kSH_C2_2 * 2.f * 2.f * z * sh[18 + c] + kSH_C2_3 * x * sh[21 + c];
         }
-        if (deg > 1) {
-            const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+        if (deg > 2) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                g[12 + c] = kSH_C2_0 * xy * d[c];
-                g[15 + c] = kSH_C2_1 * yz * d[c];
-                g[18 + c] = kSH_C2_2 * (2.f * zz - xx - yy) * d[c];
-                g[21 + c] = kSH_C2_3 * xz * d[c];
-                g[24 + c] = kSH_C2_4 * (xx - yy) * d[c];
-                dx[c] += kSH_C2_0 * y * sh[12 + c] + kSH_C2_2 * 2.f * -x * sh[18 + c] + kSH_C2_3 * z * sh[21 + c] +
-                         kSH_C2_4 * 2.f * x * sh[24 + c];
-                dy[c] += kSH_C2_0 * x * sh[12 + c] + kSH_C2_1 * z * sh[15 + c] + kSH_C2_2 * 2.f * -y * sh[18 + c] +
-                         kSH_C2_4 * 2.f * -y * sh[24 + c];
-                dz[c] += kSH_C2_1 * y * sh[15 + c] + kSH_C2_2 * 2.f * 2.f * z * sh[18 + c] + kSH_C2_3 * x * sh[21 + c];
-            }
-            if (deg > 2) {
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    g[27 + c] = kSH_C3_0 * y * (3.f * xx - yy) * d[c];
-                    g[30 + c] = kSH_C3_1 * xy * z * d[c];
-                    g[33 + c] = kSH_C3_2 * y * (4.f * zz - xx - yy) * d[c];
-                    g[36 + c] = kSH_C3_3 * z * (2.f * zz - 3.f * xx - 3.f * yy) * d[c];
-                    g[39 + c] = kSH_C3_4 * x * (4.f * zz - xx - yy) * d[c];
-                    g[42 + c] = kSH_C3_5 * z * (xx - yy) * d[c];
-                    g[45 + c] = kSH_C3_6 * x * (xx - 3.f * yy) * d[c];
-                    dx[c] += (kSH_C3_0 * sh[27 + c] * 3.f * 2.f * xy + kSH_C3_1 * sh[30 + c] * yz +
-                              kSH_C3_2 * sh[33 + c] * -2.f * xy + kSH_C3_3 * sh[36 + c] * -3.f * 2.f * xz +
-                              kSH_C3_4 * sh[39 + c] * (-3.f * xx + 4.f * zz - yy) + kSH_C3_5 * sh[42 + c] * 2.f * xz +
-                              kSH_C3_6 * sh[45 + c] * 3.f * (xx - yy));
-                    dy[c] += (kSH_C3_0 * sh[27 + c] * 3.f * (xx - yy) + kSH_C3_1 * sh[30 + c] * xz +
-                              kSH_C3_2 * sh[33 + c] * (-3.f * yy + 4.f * zz - xx) +
-                              kSH_C3_3 * sh[36 + c] * -3.f * 2.f * yz + kSH_C3_4 * sh[39 + c] * -2.f * xy +
-                              kSH_C3_5 * sh[42 + c] * -2.f * yz + kSH_C3_6 * sh[45 + c] * -3.f * 2.f * xy);
-                    dz[c] += (kSH_C3_1 * sh[30 + c] * xy + kSH_C3_2 * sh[33 + c] * 4.f * 2.f * yz +
-                              kSH_C3_3 * sh[36 + c] * 3.f * (2.f * zz - xx - yy) + kSH_C3_4 * sh[39 + c] * 4.f * 2.f * xz +
-                              kSH_C3_5 * sh[42 + c] * (xx - yy));
-                }
+                dx[c] += (kSH_C3_0 * sh[27 + c] * 3.f * 2.f * xy + kSH_C3_1 * sh[30 + c] * yz +
+                          kSH_C3_2 * sh[33 + c] * -2.f * xy + kSH_C3_3 * sh[36 + c] * -3.f * 2.f * xz +
+                          kSH_C3_4 * sh[39 + c] * (-3.f * xx + 4.f * zz - yy) + kSH_C3_5 * sh[42 + c] * 2.f * xz +
+                          kSH_C3_6 * sh[45 + c] * 3.f * (xx - yy));
+                dy[c] += (kSH_C3_0 * sh[27 + c] * 3.f * (xx - yy) + kSH_C3_1 * sh[30 + c] * xz +
+                          kSH_C3_2 * sh[33 + c] * (-3.f * yy + 4.f * zz - xx) +
+                          kSH_C3_3 * sh[36 + c] * -3.f * 2.f * yz + kSH_C3_4 * sh[39 + c] * -2.f * xy +
+                          kSH_C3_5 * sh[42 + c] * -2.f * yz + kSH_C3_6 * sh[45 + c] * -3.f * 2.f * xy);
+                dz[c] += (kSH_C3_1 * sh[30 + c] * xy + kSH_C3_2 * sh[33 + c] * 4.f * 2.f * yz +
+                          kSH_C3_3 * sh[36 + c] * 3.f * (2.f * zz - xx - yy) + kSH_C3_4 * sh[39 + c] * 4.f * 2.f * xz +
+                          kSH_C3_5 * sh[42 + c] * (xx - yy));
             }
         }
     }
-    const int ncoef = (deg + 1) * (deg + 1);
-#pragma unroll
-    for (int f = 0; f < 48; f++)
-        if (f < M * 3) {
-            const float v = f < ncoef * 3 ? g[f] : 0.f;
-            if (kAccum) dsh[f] += v;
-            else dsh[f] = v;
-        }
-    if (!kAccum)
-        for (int f = 48; f < M * 3; f++) dsh[f] = 0.f;
     const float3 ddir = {dx[0] * d[0] + dx[1] * d[1] + dx[2] * d[2], dy[0] * d[0] + dy[1] * d[1] + dy[2] * d[2],
                          dz[0] * d[0] + dz[1] * d[1] + dz[2] * d[2]};
     return dnormvdv(dir_orig, ddir);
@@ -238,19 +274,6 @@ __global__ void __launch_bounds__(256)
         dm.y += (pr[4] * m_w - pr[7] * mul1) * g2x + (pr[5] * m_w - pr[7] * mul2) * g2y;
         dm.z += (pr[8] * m_w - pr[11] * mul1) * g2x + (pr[9] * m_w - pr[11] * mul2) * g2y;
 
-        if (p.shs && dsh) {
-            float sh[48];
-            const int nf = min(48, p.M * 3);
-            const float* row = p.shs + (size_t)idx * p.M * 3;
-#pragma unroll
-            for (int f = 0; f < 48; f++)
-                if (f < nf) sh[f] = row[f];
-            const float3 cam = {p.campos[0], p.campos[1], p.campos[2]};
-            const float3 dcol = {dcolor[3 * idx], dcolor[3 * idx + 1], dcolor[3 * idx + 2]};
-            const float3 dmd =
-                sh_backward<kAccum>(p.D, sh, mean, cam, clamped[idx], dcol, dsh + (size_t)idx * p.M * 3, p.M);
-            dm.x += dmd.x; dm.y += dmd.y; dm.z += dmd.z;
-        }
         if (p.scales && dscale) {
             // backward.cu:278-341 (gradient w.r.t. the quaternion as given)
             const float r = p.rots[4 * idx], x = p.rots[4 * idx + 1], y = p.rots[4 * idx + 2], z = p.rots[4 * idx + 3];
@@ -323,6 +346,31 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// SH part of the per-Gaussian backward as its own pass over the visible ids
+// (after preprocess_bwd_kernel on the same stream): dL/dsh and the SH term of
+// dL/dmean, added to the row preprocess_bwd_kernel wrote.  Kept apart so that
+// neither kernel holds the 48-float SH rows next to the covariance chain.
+template <bool kAccum>
+__global__ void __launch_bounds__(256, 3)
+    sh_bwd_kernel(PreParams p, const uint32_t* __restrict__ visible_ids,
+                  const unsigned long long* __restrict__ visible_count, const uint8_t* __restrict__ clamped,
+                  const float* __restrict__ dcolor, float* __restrict__ dmean3D, float* __restrict__ dsh)
+{
+    const uint32_t V = (uint32_t)*visible_count;
+    const bool vec = p.aligned && ((p.M * 3) & 3) == 0;
+    const float3 cam = {p.campos[0], p.campos[1], p.campos[2]};
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < V; j += gridDim.x * blockDim.x) {
+        const int idx = (int)visible_ids[j];
+        const float3 mean = {p.means[3 * idx], p.means[3 * idx + 1], p.means[3 * idx + 2]};
+        const float3 dcol = {dcolor[3 * idx], dcolor[3 * idx + 1], dcolor[3 * idx + 2]};
+        const float3 dmd = sh_backward<kAccum>(p.D, p.shs + (size_t)idx * p.M * 3, mean, cam, clamped[idx], dcol,
+                                               dsh + (size_t)idx * p.M * 3, p.M, vec);
+        dmean3D[3 * idx] += dmd.x;
+        dmean3D[3 * idx + 1] += dmd.y;
+        dmean3D[3 * idx + 2] += dmd.z;
+    }
+}
+
 }  // namespace
 
 void launch_preprocess_bwd(const PreParams& p, const int* radii, const GeomState& g, const float* dmean2D,
@@ -345,15 +393,21 @@ void launch_preprocess_bwd(const PreParams& p, const int* radii, const GeomState
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int blocks = (int)std::min<size_t>((P + 255) / 256, (size_t)sms * 8);
-    if (accumulate)
+    const bool sh = p.shs && dsh;
+    if (accumulate) {
         preprocess_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dmean2D, dconic,
                                                            dcolor, dopac, dmean3D, dcov3D, dsh, dscale, drot,
                                                            consistent, shared_dopac);
-    else
+        if (sh)
+            sh_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dcolor, dmean3D, dsh);
+    } else {
         preprocess_bwd_kernel<false><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dmean2D, dconic,
                                                             dcolor, dopac, dmean3D, dcov3D, dsh, dscale, drot,
                                                             consistent, nullptr);
-    note_launches(1);
+        if (sh)
+            sh_bwd_kernel<false><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dcolor, dmean3D, dsh);
+    }
+    note_launches(sh ? 2 : 1);
 }
 
 }  // namespace fgs

@@ -45,6 +45,7 @@ struct Batch {
     std::vector<ViewState> views;
     TileArgs* d_args_fwd;
     TileArgs* d_args_bwd;
+    std::vector<TileArgs> h_args;  // host copy of d_args_fwd ++ d_args_bwd (sources of pointer updates)
     uint32_t* d_begin;
     uint32_t* d_queue;
     unsigned* d_err;
@@ -200,6 +201,8 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
         B->views.push_back(s);
     }
     B->total_tiles = begin[nviews];
+    B->h_args = fa;
+    B->h_args.insert(B->h_args.end(), ba.begin(), ba.end());
     B->d_args_fwd = reinterpret_cast<TileArgs*>(base + L.args_off);
     B->d_args_bwd = B->d_args_fwd + nviews;
     B->d_begin = reinterpret_cast<uint32_t*>(base + L.begin_off);
@@ -220,25 +223,55 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
 
 void fgs_batch_destroy(void* handle) { delete static_cast<Batch*>(handle); }
 
+int fgs_batch_set_view_io(void* handle, int count, const int* view_ids, float* const* out_color,
+                          const float* const* dL_dout_color, void* stream)
+{
+    Batch* B = static_cast<Batch*>(handle);
+    if (!B || count < 0 || (count > 0 && (!view_ids || !out_color))) return FGS_ERR_ARG;
+    for (int i = 0; i < count; i++)
+        if (view_ids[i] < 0 || view_ids[i] >= B->V || !out_color[i]) return FGS_ERR_ARG;
+    for (int i = 0; i < count; i++) {
+        B->h_args[view_ids[i]].out_color = out_color[i];
+        if (dL_dout_color && dL_dout_color[i]) B->h_args[B->V + view_ids[i]].dL_dpix = dL_dout_color[i];
+    }
+    // one copy of the whole descriptor table (forward ++ backward are contiguous); the source is
+    // pageable, so it is staged before the call returns and later updates cannot race it
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(B->d_args_fwd, B->h_args.data(), sizeof(TileArgs) * B->h_args.size(), cudaMemcpyHostToDevice,
+                        s) != cudaSuccess)
+        return FGS_ERR_CUDA;
+    return FGS_OK;
+}
+
 int fgs_batch_forward(void* handle, void* stream)
 {
     Batch* B = static_cast<Batch*>(handle);
     if (!B) return FGS_ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     for (ViewState& v : B->views) {
-        char* zero_begin = reinterpret_cast<char*>(v.g.hist);
-        cudaMemsetAsync(zero_begin, 0, (size_t)(v.geom_base + v.geom_bytes_v - zero_begin), s);
-        launch_preprocess(v.pre, v.g, v.radii_out, s);
+        {
+            StageTimer t(FGS_STAGE_PREPROCESS, s);
+            char* zero_begin = reinterpret_cast<char*>(v.g.hist);
+            cudaMemsetAsync(zero_begin, 0, (size_t)(v.geom_base + v.geom_bytes_v - zero_begin), s);
+            launch_preprocess(v.pre, v.g, v.radii_out, s);
+        }
+        StageTimer t(FGS_STAGE_DEPTH_SORT, s);
         launch_depth_sort(v.g, B->P, s);
     }
     for (ViewState& v : B->views) {
         if (v.cap > 0) {
-            cudaMemsetAsync(v.b.status, 0, sizeof(uint32_t) * (v.b.status_words + v.b.scan_words), s);
-            launch_duplicate(v.g, v.b, (uint32_t)B->P, (uint32_t)v.cap, v.pre.W, v.pre.H, v.tile_bits, s);
+            {
+                StageTimer t(FGS_STAGE_DUPLICATE, s);
+                cudaMemsetAsync(v.b.status, 0, sizeof(uint32_t) * (v.b.status_words + v.b.scan_words), s);
+                launch_duplicate(v.g, v.b, (uint32_t)B->P, (uint32_t)v.cap, v.pre.W, v.pre.H, v.tile_bits, s);
+            }
+            StageTimer t(FGS_STAGE_TILE_SORT, s);
             launch_tile_sort(v.g, v.b, v.cap, v.tile_bits, s, v.g.total);
         }
+        StageTimer t(FGS_STAGE_RANGES, s);
         launch_ranges(v.b, v.im, v.cap, v.num_tiles, s, v.g.total);
     }
+    StageTimer t(FGS_STAGE_RENDER_FWD, s);
     launch_render_fwd_multi(B->d_args_fwd, B->d_begin, B->V, B->total_tiles, B->d_queue, B->d_err, s);
     return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
 }
@@ -250,22 +283,30 @@ int fgs_batch_backward(void* handle, void* stream)
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t P = (size_t)B->P;
     if (!B->g_means3D || !B->g_opacity) return FGS_ERR_ARG;
-    cudaMemsetAsync(B->g_means3D, 0, sizeof(float) * 3 * P, s);
-    cudaMemsetAsync(B->g_opacity, 0, sizeof(float) * P, s);
-    cudaMemsetAsync(B->g_cov3D, 0, sizeof(float) * 6 * P, s);
-    if (B->g_sh && B->M > 0) cudaMemsetAsync(B->g_sh, 0, sizeof(float) * 3 * (size_t)B->M * P, s);
-    if (B->g_scales) cudaMemsetAsync(B->g_scales, 0, sizeof(float) * 3 * P, s);
-    if (B->g_rot) cudaMemsetAsync(B->g_rot, 0, sizeof(float) * 4 * P, s);
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    for (ViewState& v : B->views) {
-        zero_visible_rows<<<sms * 2, 256, 0, s>>>(v.g.sort_ids_b, v.g.total + 1, v.dmean2D, v.dconic, v.dopac,
-                                                  v.dcolor);
-        note_launches(1);
+    {
+        // dense zeroing of the shared outputs and of the views' visible screen-space rows
+        StageTimer t(FGS_STAGE_PREPROCESS_BWD, s);
+        cudaMemsetAsync(B->g_means3D, 0, sizeof(float) * 3 * P, s);
+        cudaMemsetAsync(B->g_opacity, 0, sizeof(float) * P, s);
+        cudaMemsetAsync(B->g_cov3D, 0, sizeof(float) * 6 * P, s);
+        if (B->g_sh && B->M > 0) cudaMemsetAsync(B->g_sh, 0, sizeof(float) * 3 * (size_t)B->M * P, s);
+        if (B->g_scales) cudaMemsetAsync(B->g_scales, 0, sizeof(float) * 3 * P, s);
+        if (B->g_rot) cudaMemsetAsync(B->g_rot, 0, sizeof(float) * 4 * P, s);
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        for (ViewState& v : B->views) {
+            zero_visible_rows<<<sms * 2, 256, 0, s>>>(v.g.sort_ids_b, v.g.total + 1, v.dmean2D, v.dconic, v.dopac,
+                                                      v.dcolor);
+            note_launches(1);
+        }
     }
-    launch_render_bwd_multi(B->d_args_bwd, B->d_begin, B->V, B->total_tiles, B->d_queue + 1, B->consistent, B->d_err,
-                            s);
+    {
+        StageTimer t(FGS_STAGE_RENDER_BWD, s);
+        launch_render_bwd_multi(B->d_args_bwd, B->d_begin, B->V, B->total_tiles, B->d_queue + 1, B->consistent,
+                                B->d_err, s);
+    }
+    StageTimer t(FGS_STAGE_PREPROCESS_BWD, s);
     for (ViewState& v : B->views) {
         launch_preprocess_bwd(v.pre, nullptr, v.g, v.dmean2D, v.dconic, v.dcolor, v.dopac, B->g_means3D, B->g_cov3D,
                               (v.pre.shs && B->g_sh) ? B->g_sh : nullptr, B->has_sr ? B->g_scales : nullptr,

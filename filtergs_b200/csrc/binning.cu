@@ -13,10 +13,11 @@
 // Every sort pass is one onesweep kernel (Adinets & Merrill 2022): chunks
 // take ascending indices from an atomic counter, rank their keys with
 // warp-level match/ballot, and learn their global offsets per digit from a
-// decoupled look-back over the preceding chunks.  Each look-back poll is
-// bounded; on timeout the kernel records FGS_ERR_TIMEOUT and moves on.
+// decoupled look-back over the preceding chunks (fgs_scan.cuh: windowed,
+// bounded; on timeout the kernel records FGS_ERR_TIMEOUT and moves on).
 #include "fgs_common.cuh"
 #include "fgs_internal.h"
+#include "fgs_scan.cuh"
 
 namespace fgs {
 
@@ -27,21 +28,6 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kRadix = 256;
-constexpr uint32_t kFlagAgg = 1u << 30;
-constexpr uint32_t kFlagPrefix = 2u << 30;
-constexpr uint32_t kValMask = (1u << 30) - 1;
-
-__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v)
-{
-    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p)
-{
-    uint32_t v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
 // Exclusive scan of one value per thread over a 256-thread block.
 __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp /*[8]*/, uint32_t* total)
 {
@@ -66,43 +52,19 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp
     return wpre + x - v;
 }
 
-// Look-back over `status` words of the preceding chunks (stride `stride`),
-// returning the exclusive prefix.  Publishes aggregate, then inclusive prefix.
-__device__ __forceinline__ uint32_t lookback(uint32_t* status, uint32_t chunk, int stride, uint32_t agg,
-                                             unsigned* err)
-{
-    uint32_t* mine = status + (size_t)chunk * stride;
-    if (chunk == 0) {
-        st_relaxed(mine, kFlagPrefix | agg);
-        return 0;
-    }
-    st_relaxed(mine, kFlagAgg | agg);
-    uint32_t excl = 0;
-    long long j = (long long)chunk - 1;
-    long long spins = 0;
-    while (j >= 0) {
-        const uint32_t s = ld_relaxed(status + (size_t)j * stride);
-        const uint32_t flag = s & ~kValMask;
-        if (flag == 0) {
-            if (++spins > kSpinLimit) {
-                set_error(err, FGS_ERR_TIMEOUT);
-                break;
-            }
-            continue;
-        }
-        excl += s & kValMask;
-        if (flag == kFlagPrefix) break;
-        --j;
-    }
-    st_relaxed(mine, kFlagPrefix | ((excl + agg) & kValMask));
-    return excl;
-}
-
 // One onesweep pass over `n` 32-bit keys with 32-bit values.
 //   vals_in == nullptr: values are the element indices.
 //   rec_out != nullptr (last tile pass): also gathers the per-Gaussian render
 //   record of each value into sorted position.
-__global__ void __launch_bounds__(kSortThreads)
+//   n_dev != nullptr: the live count is min(n, *n_dev) (the grid covers n).
+// Persistent: each CTA takes chunks from the counter until none is left, so a
+// grid sized for a bound costs nothing for the chunks that are not live.  Per
+// chunk: rank the keys (warp match), publish the digit counts at once, sort the
+// chunk locally in shared memory (which needs no global offsets), and only
+// then walk back for the global offsets -- the registers that held the keys
+// are free by then, so the walk keeps 32 status loads in flight per digit
+// (64 registers, 4 CTAs per SM).
+__global__ void __launch_bounds__(kSortThreads, 4)
     onesweep_kernel(const uint32_t* __restrict__ keys_in, uint32_t* __restrict__ keys_out,
                     const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ vals_out, uint32_t n, int shift,
                     int nbits, const uint32_t* __restrict__ pass_hist, uint32_t* status, uint32_t* chunk_counter,
@@ -118,84 +80,92 @@ __global__ void __launch_bounds__(kSortThreads)
     __shared__ uint32_t s_chunk;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_chunk = atomicAdd(chunk_counter, 1u);
-#pragma unroll
-    for (int w = 0; w < kSortWarps; w++) s_hist[w][tid] = 0;
-    __syncthreads();
-    const uint32_t chunk = s_chunk;
-    const uint32_t base = chunk * kSortTile;
-    // With a device-side count the grid is sized for a capacity; chunks past the
-    // live count have nothing to do (and no later chunk waits on them).
     if (n_dev) n = (uint32_t)min((unsigned long long)n, *n_dev);
-    if (base >= n) return;
-    const uint32_t count = min((uint32_t)kSortTile, n - base);
+    const uint32_t live = (n + kSortTile - 1) / kSortTile;
+    if (blockIdx.x >= live) return;
     const uint32_t dmask = (1u << nbits) - 1u;
-
-    uint32_t key[kSortItems], rank[kSortItems];
-    const unsigned lt = (1u << lane) - 1u;
-#pragma unroll
-    for (int i = 0; i < kSortItems; i++) {
-        const uint32_t pos = warp * (kSortItems * 32) + i * 32 + lane;
-        const bool valid = pos < count;
-        key[i] = valid ? __ldg(keys_in + base + pos) : 0xffffffffu;
-        const uint32_t dg = valid ? ((key[i] >> shift) & dmask) : kRadix;
-        const unsigned peers = __match_any_sync(0xffffffffu, dg);
-        const int leader = __ffs(peers) - 1;
-        uint32_t old = 0;
-        if (lane == leader && dg < kRadix) {
-            old = s_hist[warp][dg];
-            s_hist[warp][dg] = old + __popc(peers);
-        }
-        old = __shfl_sync(0xffffffffu, old, leader);
-        rank[i] = old + __popc(peers & lt);
-        __syncwarp();
-    }
-    __syncthreads();
-    // per digit (thread d): exclusive prefix over warps, chunk total
-    uint32_t tot = 0;
-#pragma unroll
-    for (int w = 0; w < kSortWarps; w++) {
-        const uint32_t c = s_hist[w][tid];
-        s_hist[w][tid] = tot;
-        tot += c;
-    }
-    const uint32_t excl = lookback(status + tid, chunk, kRadix, tot, err);
-    const uint32_t local = block_excl_scan(tot, s_warp, nullptr);
+    // global start of every digit in this pass (the same for all chunks)
     const uint32_t gh = (uint32_t)tid <= dmask ? __ldg(pass_hist + tid) : 0u;
     const uint32_t gofs = block_excl_scan(gh, s_warp, nullptr);
-    s_start[tid] = local;
-    s_gbase[tid] = gofs + excl;
-    __syncthreads();
+    const unsigned lt = (1u << lane) - 1u;
+
+    for (;;) {
+        if (tid == 0) s_chunk = atomicAdd(chunk_counter, 1u);
 #pragma unroll
-    for (int i = 0; i < kSortItems; i++) {
-        const uint32_t pos = warp * (kSortItems * 32) + i * 32 + lane;
-        if (pos < count) {
-            const uint32_t dg = (key[i] >> shift) & dmask;
-            const uint32_t lp = s_start[dg] + s_hist[warp][dg] + rank[i];
-            s_keys[lp] = key[i];
-            s_vals[lp] = vals_in ? __ldg(vals_in + base + pos) : base + pos;
+        for (int w = 0; w < kSortWarps; w++) s_hist[w][tid] = 0;
+        __syncthreads();
+        const uint32_t chunk = s_chunk;
+        if (chunk >= live) break;
+        const uint32_t base = chunk * kSortTile;
+        const uint32_t count = min((uint32_t)kSortTile, n - base);
+
+        uint32_t key[kSortItems], rank[kSortItems];
+#pragma unroll
+        for (int i = 0; i < kSortItems; i++) {
+            const uint32_t pos = warp * (kSortItems * 32) + i * 32 + lane;
+            const bool valid = pos < count;
+            key[i] = valid ? __ldg(keys_in + base + pos) : 0xffffffffu;
+            const uint32_t dg = valid ? ((key[i] >> shift) & dmask) : kRadix;
+            const unsigned peers = __match_any_sync(0xffffffffu, dg);
+            const int leader = __ffs(peers) - 1;
+            uint32_t old = 0;
+            if (lane == leader && dg < kRadix) {
+                old = s_hist[warp][dg];
+                s_hist[warp][dg] = old + __popc(peers);
+            }
+            old = __shfl_sync(0xffffffffu, old, leader);
+            rank[i] = old + __popc(peers & lt);
+            __syncwarp();
         }
-    }
-    __syncthreads();
-    for (uint32_t p = tid; p < count; p += kSortThreads) {
-        const uint32_t k = s_keys[p];
-        const uint32_t dg = (k >> shift) & dmask;
-        const uint32_t gp = s_gbase[dg] + (p - s_start[dg]);
-        const uint32_t v = s_vals[p];
-        if (gp >= n) {  // cannot happen with consistent histograms; never write out of bounds
-            set_error(err, FGS_ERR_OVERFLOW);
-            continue;
+        __syncthreads();
+        // per digit (thread d): exclusive prefix over warps, chunk total, published at once
+        uint32_t tot = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; w++) {
+            const uint32_t c = s_hist[w][tid];
+            s_hist[w][tid] = tot;
+            tot += c;
         }
-        if (keys_out) keys_out[gp] = k;
-        vals_out[gp] = v;
-        if (rec_out) rec_out[gp] = grec[v];
+        lookback_publish(status + tid, chunk, kRadix, tot);
+        s_start[tid] = block_excl_scan(tot, s_warp, nullptr);
+        __syncthreads();
+        // local sort of the chunk by digit
+#pragma unroll
+        for (int i = 0; i < kSortItems; i++) {
+            const uint32_t pos = warp * (kSortItems * 32) + i * 32 + lane;
+            if (pos < count) {
+                const uint32_t dg = (key[i] >> shift) & dmask;
+                const uint32_t lp = s_start[dg] + s_hist[warp][dg] + rank[i];
+                s_keys[lp] = key[i];
+                s_vals[lp] = vals_in ? __ldg(vals_in + base + pos) : base + pos;
+            }
+        }
+        // global offset of this chunk's digit run
+        s_gbase[tid] = gofs + thread_lookback_walk<32>(status + tid, chunk, kRadix, tot, err);
+        __syncthreads();
+        for (uint32_t p = tid; p < count; p += kSortThreads) {
+            const uint32_t k = s_keys[p];
+            const uint32_t dg = (k >> shift) & dmask;
+            const uint32_t gp = s_gbase[dg] + (p - s_start[dg]);
+            const uint32_t v = s_vals[p];
+            if (gp >= n) {  // cannot happen with consistent histograms; never write out of bounds
+                set_error(err, FGS_ERR_OVERFLOW);
+                continue;
+            }
+            if (keys_out) keys_out[gp] = k;
+            vals_out[gp] = v;
+            if (rec_out) rec_out[gp] = grec[v];
+        }
+        __syncthreads();  // shared buffers are reused by the next chunk
     }
 }
 
 // Histograms of the 4 depth-key bytes (one read of the keys).
-__global__ void depth_hist_kernel(const uint32_t* __restrict__ keys, uint32_t n, uint32_t* __restrict__ hist)
+__global__ void depth_hist_kernel(const uint32_t* __restrict__ keys, uint32_t n,
+                                  const unsigned long long* __restrict__ n_dev, uint32_t* __restrict__ hist)
 {
     __shared__ uint32_t s[4][kRadix];
+    n = (uint32_t)min((unsigned long long)n, *n_dev);
     for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) (&s[0][0])[i] = 0;
     __syncthreads();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -211,7 +181,8 @@ __global__ void depth_hist_kernel(const uint32_t* __restrict__ keys, uint32_t n,
 }
 
 // duplicateWithKeys over the depth-ordered Gaussians, with the prefix sum of
-// tiles_touched fused in (decoupled look-back over 256-Gaussian chunks) and
+// tiles_touched fused in (decoupled look-back over 256-Gaussian chunks, taken
+// by persistent CTAs; the tile histograms leave each CTA once) and
 // warp-aggregated pair emission: the pairs of a warp's 32 Gaussians are
 // spread evenly over its lanes, so a large splat does not serialise on one
 // thread.  Also builds the per-pass tile digit histograms for the tile sort.
@@ -220,72 +191,81 @@ __global__ void __launch_bounds__(256)
                      const PairRecord* __restrict__ grec, const int* __restrict__ radii, uint32_t V, int gx,
                      int gy, uint32_t* __restrict__ tile_out, uint32_t* __restrict__ val_out, uint32_t K,
                      uint32_t* status, uint32_t* chunk_counter, uint32_t* __restrict__ tile_hist, int tile_passes,
-                     unsigned* err)
+                     const unsigned long long* __restrict__ V_dev, unsigned* err)
 {
     __shared__ uint32_t s_hist[4][kRadix];
     __shared__ uint32_t s_warp[8];
-    __shared__ uint32_t s_chunk;
+    __shared__ uint32_t s_chunk, s_prefix;
     const int tid = threadIdx.x, lane = tid & 31;
-    if (tid == 0) s_chunk = atomicAdd(chunk_counter, 1u);
+    // persistent over chunks of 256 Gaussians (the grid covers a bound on V)
+    V = (uint32_t)min((unsigned long long)V, *V_dev);
+    const uint32_t live = (V + 255) / 256;
+    if (blockIdx.x >= live) return;
     for (int i = tid; i < 4 * kRadix; i += 256) (&s_hist[0][0])[i] = 0;
-    __syncthreads();
-    const uint32_t chunk = s_chunk;
-    const uint32_t j = chunk * 256 + tid;
-    uint32_t id = 0, cnt = 0;
-    int x0 = 0, y0 = 0, w = 1;
-    if (j < V) {
-        id = __ldg(sorted_ids + j);
-        cnt = __ldg(tiles + id);
-        const float4 a = grec[id].a;
-        int x1, y1;
-        tile_rect(a.x, a.y, __ldg(radii + id), gx, gy, kTileX, kTileY, x0, y0, x1, y1);
-        w = max(1, x1 - x0);
-    }
-    uint32_t block_total;
-    const uint32_t local = block_excl_scan(cnt, s_warp, &block_total);
-    __shared__ uint32_t s_prefix;
-    if (tid == 0) s_prefix = lookback(status, chunk, 1, block_total, err);
-    __syncthreads();
-    const uint32_t off = s_prefix + local;
-    // warp-local exclusive prefix of cnt
-    uint32_t wx = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, wx, o);
-        if (lane >= o) wx += y;
-    }
-    const uint32_t wtotal = __shfl_sync(0xffffffffu, wx, 31);
-    wx -= cnt;  // exclusive
-    for (uint32_t pb = 0; pb < wtotal; pb += 32) {
-        const uint32_t p = pb + lane;
-        // owner lane: last lane g with wx[g] <= p (lanes with no pairs never win)
-        int lo = 0;
-#pragma unroll
-        for (int step = 16; step > 0; step >>= 1) {
-            const int probe = lo + step;
-            const uint32_t e = __shfl_sync(0xffffffffu, wx, probe);
-            if (e <= p) lo = probe;
+    for (;;) {
+        if (tid == 0) s_chunk = atomicAdd(chunk_counter, 1u);
+        __syncthreads();
+        const uint32_t chunk = s_chunk;
+        if (chunk >= live) break;
+        const uint32_t j = chunk * 256 + tid;
+        uint32_t id = 0, cnt = 0;
+        int x0 = 0, y0 = 0, w = 1;
+        if (j < V) {
+            id = __ldg(sorted_ids + j);
+            cnt = __ldg(tiles + id);
+            const float4 a = grec[id].a;
+            int x1, y1;
+            tile_rect(a.x, a.y, __ldg(radii + id), gx, gy, kTileX, kTileY, x0, y0, x1, y1);
+            w = max(1, x1 - x0);
         }
-        const uint32_t owx = __shfl_sync(0xffffffffu, wx, lo);
-        const uint32_t ooff = __shfl_sync(0xffffffffu, off, lo);
-        const uint32_t oid = __shfl_sync(0xffffffffu, id, lo);
-        const int ox0 = __shfl_sync(0xffffffffu, x0, lo);
-        const int oy0 = __shfl_sync(0xffffffffu, y0, lo);
-        const int ow = __shfl_sync(0xffffffffu, w, lo);
-        if (p < wtotal) {
-            const uint32_t t = p - owx;
-            if (ooff + t >= K) {  // K and tiles_touched come from the same kernel; guard anyway
-                set_error(err, FGS_ERR_OVERFLOW);
-                continue;
+        uint32_t block_total;
+        const uint32_t local = block_excl_scan(cnt, s_warp, &block_total);
+        if (tid < 32) {
+            const uint32_t e = warp_lookback(status, chunk, 1, block_total, err);
+            if (tid == 0) s_prefix = e;
+        }
+        __syncthreads();
+        const uint32_t off = s_prefix + local;
+        // warp-local exclusive prefix of cnt
+        uint32_t wx = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, wx, o);
+            if (lane >= o) wx += y;
+        }
+        const uint32_t wtotal = __shfl_sync(0xffffffffu, wx, 31);
+        wx -= cnt;  // exclusive
+        for (uint32_t pb = 0; pb < wtotal; pb += 32) {
+            const uint32_t p = pb + lane;
+            // owner lane: last lane g with wx[g] <= p (lanes with no pairs never win)
+            int lo = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int probe = lo + step;
+                const uint32_t e = __shfl_sync(0xffffffffu, wx, probe);
+                if (e <= p) lo = probe;
             }
-            const uint32_t ty = t / (uint32_t)ow, tx = t - ty * (uint32_t)ow;
-            const uint32_t tile = (uint32_t)(oy0 + ty) * (uint32_t)gx + (uint32_t)(ox0 + tx);
-            tile_out[ooff + t] = tile;
-            val_out[ooff + t] = oid;
-            for (int b = 0; b < tile_passes; b++) atomicAdd(&s_hist[b][(tile >> (8 * b)) & 255u], 1u);
+            const uint32_t owx = __shfl_sync(0xffffffffu, wx, lo);
+            const uint32_t ooff = __shfl_sync(0xffffffffu, off, lo);
+            const uint32_t oid = __shfl_sync(0xffffffffu, id, lo);
+            const int ox0 = __shfl_sync(0xffffffffu, x0, lo);
+            const int oy0 = __shfl_sync(0xffffffffu, y0, lo);
+            const int ow = __shfl_sync(0xffffffffu, w, lo);
+            if (p < wtotal) {
+                const uint32_t t = p - owx;
+                if (ooff + t >= K) {  // K and tiles_touched come from the same kernel; guard anyway
+                    set_error(err, FGS_ERR_OVERFLOW);
+                    continue;
+                }
+                const uint32_t ty = t / (uint32_t)ow, tx = t - ty * (uint32_t)ow;
+                const uint32_t tile = (uint32_t)(oy0 + ty) * (uint32_t)gx + (uint32_t)(ox0 + tx);
+                tile_out[ooff + t] = tile;
+                val_out[ooff + t] = oid;
+                for (int b = 0; b < tile_passes; b++) atomicAdd(&s_hist[b][(tile >> (8 * b)) & 255u], 1u);
+            }
         }
+        __syncthreads();  // s_chunk / s_prefix / s_warp are reused by the next chunk
     }
-    __syncthreads();
     for (int i = tid; i < tile_passes * kRadix; i += 256) {
         const uint32_t c = (&s_hist[0][0])[i];
         if (c) atomicAdd(tile_hist + i, c);
@@ -306,28 +286,47 @@ __global__ void ranges_kernel(const uint32_t* __restrict__ tile, uint32_t K, uin
 
 inline uint32_t chunks_of(long long n, int tile) { return (uint32_t)((n + tile - 1) / tile); }
 
+// Resident CTAs of a kernel on this device (persistent grids never exceed it).
+template <typename Kern>
+uint32_t resident_ctas(Kern k, int threads)
+{
+    static uint32_t cache[64] = {};  // per device ordinal; the same value if two threads race
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
+    int sms = 148, per = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, 0);
+    const uint32_t r = (uint32_t)(sms * (per > 0 ? per : 1));
+    if (dev >= 0 && dev < 64) cache[dev] = r;
+    return r;
+}
+
 }  // namespace
 
 int sort_chunk_size() { return kSortTile; }
 
 void launch_depth_sort(const GeomState& g, int P, cudaStream_t s)
 {
+    // the V visible Gaussians (count on the device, bound P): keys depth_key[0..V), ids sort_ids_b[0..V)
     if (P <= 0) return;
     const uint32_t n = (uint32_t)P;
+    const unsigned long long* V = g.total + 1;
     const uint32_t nch = chunks_of(n, kSortTile);
     const uint32_t hb0 = (n + 1023) / 1024;
     const int hb = (int)(hb0 < 1184u ? hb0 : 1184u);
-    depth_hist_kernel<<<hb, 256, 0, s>>>(g.depth_key, n, g.hist);
+    depth_hist_kernel<<<hb, 256, 0, s>>>(g.depth_key, n, V, g.hist);
+    const uint32_t grid = min(nch, resident_ctas(onesweep_kernel, kSortThreads));
     note_launches(5);
-    // ping-pong: depth_key -> sort_keys_b -> depth_key -> sort_keys_b ; ids a/b
+    // ping-pong: depth_key -> sort_keys_b -> depth_key -> sort_keys_b ; ids b -> a -> b -> a -> b
     const uint32_t* kin[4] = {g.depth_key, g.sort_keys_b, g.depth_key, g.sort_keys_b};
     uint32_t* kout[4] = {g.sort_keys_b, g.depth_key, g.sort_keys_b, nullptr};
-    const uint32_t* vin[4] = {nullptr, g.sort_ids_a, g.sort_ids_b, g.sort_ids_a};
+    const uint32_t* vin[4] = {g.sort_ids_b, g.sort_ids_a, g.sort_ids_b, g.sort_ids_a};
     uint32_t* vout[4] = {g.sort_ids_a, g.sort_ids_b, g.sort_ids_a, g.sort_ids_b};
     for (int pass = 0; pass < 4; pass++) {
-        onesweep_kernel<<<nch, kSortThreads, 0, s>>>(kin[pass], kout[pass], vin[pass], vout[pass], n, 8 * pass, 8,
+        onesweep_kernel<<<grid, kSortThreads, 0, s>>>(kin[pass], kout[pass], vin[pass], vout[pass], n, 8 * pass, 8,
                                                      g.hist + pass * kRadix, g.status + (size_t)pass * nch * kRadix,
-                                                     g.counters + pass, g.err, nullptr, nullptr, nullptr);
+                                                     g.counters + pass, g.err, nullptr, nullptr, V);
     }
 }
 
@@ -341,9 +340,10 @@ void launch_duplicate(const GeomState& g, const BinState& b, uint32_t V, uint32_
     // with an odd number of passes it starts from a, with an even one from b.
     uint32_t* tout = (passes & 1) ? b.tile_a : b.tile_b;
     uint32_t* vout = (passes & 1) ? b.val_a : b.val_b;
-    duplicate_kernel<<<chunks_of(V, 256), 256, 0, s>>>(g.sort_ids_b, g.tiles, g.grec, g.radii, V, gx, gy, tout,
+    const uint32_t grid = min(chunks_of(V, 256), resident_ctas(duplicate_kernel, 256));
+    duplicate_kernel<<<grid, 256, 0, s>>>(g.sort_ids_b, g.tiles, g.grec, g.radii, V, gx, gy, tout,
                                                        vout, K, b.scan_status, g.counters + 8, g.hist + 4 * kRadix,
-                                                       passes, g.err);
+                                                       passes, g.total + 1, g.err);
     note_launches(1);
 }
 
@@ -353,6 +353,7 @@ void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int ti
     if (K <= 0) return;
     const uint32_t n = (uint32_t)K;
     const uint32_t nch = chunks_of(n, kSortTile);
+    const uint32_t grid = min(nch, resident_ctas(onesweep_kernel, kSortThreads));
     const int passes = (tile_bits + 7) / 8;
     const uint32_t* ki = (passes & 1) ? b.tile_a : b.tile_b;
     const uint32_t* vi = (passes & 1) ? b.val_a : b.val_b;
@@ -361,7 +362,7 @@ void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int ti
         const int nbits = min(8, tile_bits - 8 * pass);
         uint32_t* ko = (ki == b.tile_a) ? b.tile_b : b.tile_a;
         uint32_t* vo = (vi == b.val_a) ? b.val_b : b.val_a;
-        onesweep_kernel<<<nch, kSortThreads, 0, s>>>(ki, ko, vi, vo, n, 8 * pass, nbits, g.hist + (4 + pass) * kRadix,
+        onesweep_kernel<<<grid, kSortThreads, 0, s>>>(ki, ko, vi, vo, n, 8 * pass, nbits, g.hist + (4 + pass) * kRadix,
                                                      b.status + (size_t)pass * nch * kRadix, g.counters + 4 + pass,
                                                      g.err, last ? g.grec : nullptr, last ? b.rec : nullptr, n_dev);
         ki = ko;

@@ -57,6 +57,7 @@ GeomCarve carve_geom(void* base, int P)
     r.g.err = c.take<unsigned int>(1);
     r.g.status_words = (size_t)4 * sort_chunks(P) * 256;
     r.g.status = c.take<uint32_t>(r.g.status_words);
+    r.g.chunk_counts = c.take<uint32_t>(2 * (((size_t)P + 255) / 256));
     r.zero_begin = base ? static_cast<char*>(base) + zero_off : nullptr;
     r.zero_bytes = c.off - zero_off;
     r.total = c.off;
@@ -129,7 +130,8 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 int make_params(const fgs_raster_args* a, PreParams& p, bool backward)
 {
     if (!a) return FGS_ERR_ARG;
-    if (a->P < 0 || a->width <= 0 || a->height <= 0) return FGS_ERR_ARG;
+    // P < 2^30: visible counts travel in the 30-bit values of the look-back status words
+    if (a->P < 0 || a->P >= (1 << 30) || a->width <= 0 || a->height <= 0) return FGS_ERR_ARG;
     if (a->P > 0 && (!a->means3D || (!backward && !a->opacities))) return FGS_ERR_ARG;
     if (!a->viewmatrix || !a->projmatrix || !a->background) return FGS_ERR_ARG;
     const bool has_sr = a->scales && a->rotations;
@@ -244,6 +246,9 @@ StageTimer::StageTimer(int st, cudaStream_t s) : stage(st), stream(s), slot(null
 {
     std::lock_guard<std::mutex> lk(g_prof_mu);
     if (!g_prof_on) return;
+    // launches captured into a CUDA graph are not timed (their events would only fire at replay)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
     EventPair* ep = new EventPair{st, pool_event(), pool_event()};
     cudaEventRecord(ep->a, s);
     slot = ep;

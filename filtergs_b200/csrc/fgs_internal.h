@@ -36,13 +36,14 @@ struct GeomState {
     int* radii;                // [P] internal radii (when the caller passes none)
     uint32_t* tiles;           // [P] tiles touched
     uint8_t* clamped;          // [P] SH clamp bits
-    uint32_t* depth_key;       // [P] depth bits (0xffffffff = culled)
-    uint32_t* sort_ids_a;      // [P] depth-sorted ids (ping)
-    uint32_t* sort_ids_b;      // [P] (pong)
+    uint32_t* depth_key;       // [V] depth bits of the visible Gaussians (index order, then sort ping)
+    uint32_t* sort_ids_a;      // [V] depth-sorted ids (ping)
+    uint32_t* sort_ids_b;      // [V] visible ids in index order, then depth-sorted (pong)
     uint32_t* sort_keys_b;     // [P]
     uint32_t* hist;            // [8][256] radix histograms: 4 depth passes + up to 4 tile passes
     uint32_t* status;          // lookback status words, depth passes
-    uint32_t* counters;        // [16] chunk counters / misc
+    uint32_t* chunk_counts;    // [2][ceil(P/256)] preprocess chunk counts: visible (scanned in place), pairs
+    uint32_t* counters;        // [16] chunk counters: 0-3 depth passes, 4-7 tile passes, 8 pairs
     unsigned long long* total; // [4]: 0 = K (pairs), 1 = V (visible count)
     unsigned int* err;         // error bit set
     size_t status_words;

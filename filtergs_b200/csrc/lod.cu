@@ -12,25 +12,11 @@
 //                       sigmoid(opacity) < 1/255), order preserving
 #include "fgs_common.cuh"
 #include "fgs_internal.h"
+#include "fgs_scan.cuh"
 
 namespace fgs {
 
 namespace {
-
-constexpr uint32_t kFlagAgg = 1u << 30;
-constexpr uint32_t kFlagPrefix = 2u << 30;
-constexpr uint32_t kValMask = (1u << 30) - 1;
-
-__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v)
-{
-    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p)
-{
-    uint32_t v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 
 // Ordered exclusive prefix of a per-thread count over a 256-thread chunk plus
 // a decoupled look-back over earlier chunks.  Returns the global exclusive
@@ -55,31 +41,9 @@ __device__ __forceinline__ uint32_t chunk_offset(uint32_t cnt, uint32_t chunk, u
         if (w < warp) wpre += c;
         tot += c;
     }
-    if (threadIdx.x == 0) {
-        uint32_t* mine = status + chunk;
-        uint32_t excl = 0;
-        if (chunk == 0) {
-            st_relaxed(mine, kFlagPrefix | tot);
-        } else {
-            st_relaxed(mine, kFlagAgg | tot);
-            long long j = (long long)chunk - 1, spins = 0;
-            while (j >= 0) {
-                const uint32_t s = ld_relaxed(status + j);
-                const uint32_t f = s & ~kValMask;
-                if (f == 0) {
-                    if (++spins > kSpinLimit) {
-                        set_error(err, FGS_ERR_TIMEOUT);
-                        break;
-                    }
-                    continue;
-                }
-                excl += s & kValMask;
-                if (f == kFlagPrefix) break;
-                --j;
-            }
-            st_relaxed(mine, kFlagPrefix | ((excl + tot) & kValMask));
-        }
-        s_prefix = excl;
+    if (threadIdx.x < 32) {
+        const uint32_t excl = warp_lookback(status, chunk, 1, tot, err);
+        if (threadIdx.x == 0) s_prefix = excl;
     }
     __syncthreads();
     const uint32_t r = s_prefix + wpre + x - cnt;

@@ -2,11 +2,19 @@
 //
 // preprocess: antialias/cuda_rasterizer/forward.cu:266-401 (EWA projection,
 // 2D dilation, OGFS opacity-aware radius, tile rectangle, SH degree<=3
-// colour), plus the optional 3D filter.  Each 256-thread block stages its
+// colour), plus the optional 3D filter.  Each 256-thread chunk stages its
 // slice of the AoS parameter arrays through shared memory with coalesced
-// float4 loads, then every thread works on one Gaussian in registers.  The
-// kernel writes a 48-byte render record per Gaussian, the depth sort key,
-// and accumulates the pair count K and visible count V on the device.
+// float4 loads, then every thread works on one Gaussian in registers.
+//
+// Radii and tiles-touched are written for every Gaussian.  Only the V
+// visible ones (tiles > 0) get the 48-byte render record and SH clamp bits.
+// They are then compacted in index order -- ids into sort_ids_b, depth bits
+// into depth_key -- by reduce-then-scan: each chunk of 256 leaves its visible
+// and pair counts, one CTA scans the chunk counts (and writes K and V to the
+// device), and a scatter pass places the ids.  (A single-pass look-back over
+// the P/256 chunks serialises on its prefix chain at this chunk size; the
+// two extra launches cost a few microseconds.)  The depth sort then runs over
+// V keys instead of P with the same result: equal depths keep index order.
 #include "fgs_common.cuh"
 #include "fgs_internal.h"
 
@@ -33,22 +41,62 @@ __device__ __forceinline__ void stage_rows(const float* __restrict__ g, int row0
     }
 }
 
+// Conservative tile test before the projection (skips only Gaussians whose
+// exact path would touch no tile, so every output is unchanged).  With
+// cov3D = M^T M positive semi-definite, lambda_max(cov3D) <= trace(cov3D), and
+// the 2D covariance T^T cov3D T (T = W J, forward.cu:102-146, with the same
+// clamped t.x / t.y) has trace <= trace(cov3D) (|T_0|^2 + |T_1|^2); dilation
+// adds at most 0.3 per diagonal entry.  The OGFS radius is at most
+// max(1, ratio_min) * 3 sqrt(lambda_max) + 1 pixels.  The 1% + 1e-4 and +1 px
+// margins absorb the float rounding of the exact path.
+__device__ __forceinline__ bool may_touch_tiles(const PreParams& p, float3 t, const float cov3D[6], float px,
+                                                float py)
+{
+    const float* v = p.view;
+    const float limx = 1.3f * p.tanx, limy = 1.3f * p.tany;
+    const float tx = fminf(limx, fmaxf(-limx, t.x / t.z)) * t.z;
+    const float ty = fminf(limy, fmaxf(-limy, t.y / t.z)) * t.z;
+    const float j00 = p.fx / t.z, j20 = -(p.fx * tx) / (t.z * t.z);
+    const float j11 = p.fy / t.z, j21 = -(p.fy * ty) / (t.z * t.z);
+    const float a0 = j00 * v[0] + j20 * v[2], a1 = j00 * v[4] + j20 * v[6], a2 = j00 * v[8] + j20 * v[10];
+    const float b0 = j11 * v[1] + j21 * v[2], b1 = j11 * v[5] + j21 * v[6], b2 = j11 * v[9] + j21 * v[10];
+    const float tr3 = cov3D[0] + cov3D[3] + cov3D[5];
+    const float lam = tr3 * (a0 * a0 + a1 * a1 + a2 * a2 + b0 * b0 + b1 * b1 + b2 * b2) + (p.use_filter ? 0.6f : 0.f);
+    const float r = fmaxf(1.f, p.ratio_min) * 3.f * sqrtf(1.01f * lam + 1e-4f) + 2.f;
+    if (!(r < 1e7f) || !(fabsf(px) < 1e9f) || !(fabsf(py) < 1e9f)) return true;  // no safe bound: exact path
+    const int gx = (p.W + kTileX - 1) / kTileX, gy = (p.H + kTileY - 1) / kTileY;
+    int x0, y0, x1, y1;
+    tile_rect(px, py, (int)ceilf(r), gx, gy, kTileX, kTileY, x0, y0, x1, y1);
+    return (x1 - x0) * (y1 - y0) != 0;
+}
+
 __global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomState g, int* __restrict__ radii_out)
 {
     __shared__ __align__(16) float s_mean[kThreads * 3];
     __shared__ __align__(16) float s_scale[kThreads * 3];
     __shared__ __align__(16) float s_rot[kThreads * 4];
     __shared__ __align__(16) float s_opac[kThreads];
-    __shared__ unsigned long long s_sum[2];
+    __shared__ uint32_t s_wv[kThreads / 32];
+    __shared__ unsigned long long s_wk[kThreads / 32];
+    __shared__ float s_log_lambda_G;
 
-    const int row0 = blockIdx.x * kThreads;
+    const uint32_t chunk = blockIdx.x;
+    const int row0 = (int)chunk * kThreads;
     const int rows = min(kThreads, p.P - row0);
     const bool vec = p.aligned != 0;
     stage_rows<3>(p.means, row0, rows, s_mean, vec);
     stage_rows<1>(p.opac, row0, rows, s_opac, vec);
     if (p.scales) stage_rows<3>(p.scales, row0, rows, s_scale, vec);
     if (p.rots) stage_rows<4>(p.rots, row0, rows, s_rot, vec);
-    if (threadIdx.x < 2) s_sum[threadIdx.x] = 0;
+    if (threadIdx.x == 0) {
+        // forward.cu:345-355: the opacity-independent part of the OGFS radius, once per chunk
+        const float epsilon_pix = 1.0f / 255.0f;
+        const float eps_base = fmaxf(0.0f, 1.0f - epsilon_pix);
+        const float lambda_G_raw = 1.0f - powf(eps_base, static_cast<float>(kOgfsBlockArea));
+        float lambda_G = epsilon_pix + p.eps_scale * (lambda_G_raw - epsilon_pix);
+        lambda_G = fminf(fmaxf(lambda_G, epsilon_pix), p.eps_max);
+        s_log_lambda_G = logf(lambda_G);
+    }
     __syncthreads();
 
     const int t = threadIdx.x;
@@ -56,7 +104,6 @@ __global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomS
     uint32_t tiles = 0;
     if (idx < p.P) {
         int radius_px = 0;
-        uint32_t key = 0xffffffffu;
         uint8_t clamp_bits = 0;
         PairRecord rec;
         rec.a = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -68,6 +115,7 @@ __global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomS
         const float p_w = 1.0f / (p_hom.w + 0.0000001f);
         const float3 p_proj = {p_hom.x * p_w, p_hom.y * p_w, p_hom.z * p_w};
         const float3 p_view = xform_point4x3(p_orig, p.view);
+        const float px = ndc_to_pix(p_proj.x, p.W), py = ndc_to_pix(p_proj.y, p.H);
         bool live = true;
         if (p_view.z <= 0.2f) {
             live = false;
@@ -88,6 +136,9 @@ __global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomS
                 const float v = sf * sf;
                 cov3D[0] += v; cov3D[3] += v; cov3D[5] += v;
             }
+            if (!p.cov3D && !may_touch_tiles(p, p_view, cov3D, px, py)) live = false;
+        }
+        if (live) {
             float3 cov = ewa_cov2d(p_orig, p.fx, p.fy, p.tanx, p.tany, cov3D, p.view);
             if (p.use_filter) {
                 cov.x = dilate_max(cov.x);
@@ -100,12 +151,7 @@ __global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomS
                 const float3 conic = {cov.z * det_inv, -cov.y * det_inv, cov.x * det_inv};
                 // forward.cu:345-369: OGFS radius
                 const float opacity = fmaxf(s_opac[t], 1e-6f);
-                const float epsilon_pix = 1.0f / 255.0f;
-                const float eps_base = fmaxf(0.0f, 1.0f - epsilon_pix);
-                const float lambda_G_raw = 1.0f - powf(eps_base, static_cast<float>(kOgfsBlockArea));
-                float lambda_G = epsilon_pix + p.eps_scale * (lambda_G_raw - epsilon_pix);
-                lambda_G = fminf(fmaxf(lambda_G, epsilon_pix), p.eps_max);
-                const float log_lambda_G = logf(lambda_G);
+                const float log_lambda_G = s_log_lambda_G;
                 const float log_opacity = logf(opacity);
                 const float radius_energy = log_opacity - log_lambda_G;
                 const float energy_clamped = fmaxf(radius_energy, p.energy_floor);
@@ -121,7 +167,6 @@ __global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomS
                 radius_major = fmaxf(radius_major, p.ratio_min * radius_base);
                 const float radius_f = radius_major + 1.0f;
                 const int rpx = max(1, static_cast<int>(ceilf(radius_f)));
-                const float px = ndc_to_pix(p_proj.x, p.W), py = ndc_to_pix(p_proj.y, p.H);
                 const int gx = (p.W + kTileX - 1) / kTileX, gy = (p.H + kTileY - 1) / kTileY;
                 int x0, y0, x1, y1;
                 tile_rect(px, py, rpx, gx, gy, kTileX, kTileY, x0, y0, x1, y1);
@@ -156,36 +201,114 @@ __global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomS
                     }
                     radius_px = rpx;
                     tiles = (uint32_t)extent;
-                    key = __float_as_uint(p_view.z);
                     rec.a = make_float4(px, py, conic.x, conic.y);
                     rec.b = make_float4(conic.z, opacity, rgb.x, rgb.y);
                     rec.c = make_float4(rgb.z, __int_as_float(idx), p_view.z, 0.f);
                 }
             }
         }
-        g.grec[idx] = rec;
+        if (tiles) {
+            g.grec[idx] = rec;
+            g.clamped[idx] = clamp_bits;
+        }
         g.tiles[idx] = tiles;
-        g.depth_key[idx] = key;
-        g.clamped[idx] = clamp_bits;
         g.radii[idx] = radius_px;
         if (radii_out) radii_out[idx] = radius_px;
     }
-    // K (pairs) and V (visible) totals: warp reduce, then one shared atomic per warp.
+    // Per-chunk visible and pair counts (scanned by chunk_scan_kernel).
+    const int lane = t & 31, warp = t >> 5;
+    const unsigned vb = __ballot_sync(0xffffffffu, tiles != 0);
     unsigned long long k = tiles;
-    unsigned v = tiles ? 1u : 0u;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        k += __shfl_xor_sync(0xffffffffu, k, o);
-        v += __shfl_xor_sync(0xffffffffu, v, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&s_sum[0], k);
-        atomicAdd(&s_sum[1], (unsigned long long)v);
+    for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
+    if (lane == 0) {
+        s_wv[warp] = __popc(vb);
+        s_wk[warp] = k;
     }
     __syncthreads();
+    if (t == 0) {
+        uint32_t vtot = 0;
+        unsigned long long ktot = 0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; w++) {
+            vtot += s_wv[w];
+            ktot += s_wk[w];
+        }
+        if (ktot > 0xffffffffull) {
+            set_error(g.err, FGS_ERR_OVERFLOW);
+            ktot = 0xffffffffull;
+        }
+        g.chunk_counts[chunk] = vtot;
+        g.chunk_counts[gridDim.x + chunk] = (uint32_t)ktot;
+    }
+}
+
+// Exclusive scan of the per-chunk visible counts (in place) and the totals
+// K = sum of pair counts, V = sum of visible counts.  One CTA of 1024 threads,
+// each owning a contiguous run of chunks.
+__global__ void __launch_bounds__(1024) chunk_scan_kernel(uint32_t* __restrict__ counts, uint32_t nch,
+                                                         unsigned long long* __restrict__ total)
+{
+    __shared__ unsigned long long s_v[32], s_k[32];
+    const uint32_t per = (nch + 1023) / 1024;
+    const uint32_t b = min(nch, threadIdx.x * per), e = min(nch, b + per);
+    unsigned long long sv = 0, sk = 0;
+    for (uint32_t i = b; i < e; i++) {
+        sv += counts[i];
+        sk += counts[nch + i];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long x = sv;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sk += __shfl_xor_sync(0xffffffffu, sk, o);
+    if (lane == 31) s_v[warp] = x;
+    if (lane == 0) s_k[warp] = sk;
+    __syncthreads();
+    unsigned long long wpre = 0, vtot = 0, ktot = 0;
+    for (int w = 0; w < 32; w++) {
+        if (w < warp) wpre += s_v[w];
+        vtot += s_v[w];
+        ktot += s_k[w];
+    }
+    unsigned long long excl = wpre + x - sv;
+    for (uint32_t i = b; i < e; i++) {
+        const uint32_t c = counts[i];
+        counts[i] = (uint32_t)excl;
+        excl += c;
+    }
     if (threadIdx.x == 0) {
-        if (s_sum[0]) atomicAdd(&g.total[0], s_sum[0]);
-        if (s_sum[1]) atomicAdd(&g.total[1], s_sum[1]);
+        total[0] = ktot;
+        total[1] = vtot;
+    }
+}
+
+// Ordered scatter of the visible ids and their depth bits (the view depth kept
+// in the render record).
+__global__ void __launch_bounds__(kThreads) compact_visible_kernel(int P, const uint32_t* __restrict__ tiles,
+                                                                   const PairRecord* __restrict__ grec,
+                                                                   const uint32_t* __restrict__ chunk_prefix,
+                                                                   uint32_t* __restrict__ ids,
+                                                                   uint32_t* __restrict__ keys)
+{
+    __shared__ uint32_t s_wv[kThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int idx = blockIdx.x * kThreads + t;
+    const bool vis = idx < P && __ldg(tiles + idx) != 0;
+    const unsigned vb = __ballot_sync(0xffffffffu, vis);
+    if (lane == 0) s_wv[warp] = __popc(vb);
+    __syncthreads();
+    uint32_t pos = __ldg(chunk_prefix + blockIdx.x) + __popc(vb & ((1u << lane) - 1u));
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; w++)
+        if (w < warp) pos += s_wv[w];
+    if (vis) {
+        ids[pos] = (uint32_t)idx;
+        keys[pos] = __float_as_uint(grec[idx].c.z);
     }
 }
 
@@ -332,8 +455,12 @@ __global__ void visibility_phase2(int P, const int32_t* __restrict__ node_index,
 void launch_preprocess(const PreParams& p, const GeomState& g, int* radii, cudaStream_t s)
 {
     if (p.P <= 0) return;
-    preprocess_kernel<<<(p.P + kThreads - 1) / kThreads, kThreads, 0, s>>>(p, g, radii);
-    note_launches(1);
+    const uint32_t nch = (uint32_t)((p.P + kThreads - 1) / kThreads);
+    preprocess_kernel<<<nch, kThreads, 0, s>>>(p, g, radii);
+    chunk_scan_kernel<<<1, 1024, 0, s>>>(g.chunk_counts, nch, g.total);
+    compact_visible_kernel<<<nch, kThreads, 0, s>>>(p.P, g.tiles, g.grec, g.chunk_counts, g.sort_ids_b,
+                                                    g.depth_key);
+    note_launches(3);
 }
 
 void launch_compute_radius(int variant, int P, const float* means, const float* scales, const float* rots,

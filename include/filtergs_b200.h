@@ -166,6 +166,13 @@ void *fgs_batch_create(const fgs_raster_args *shared, int nviews, const fgs_view
                        float *dL_dsh, float *dL_dscales, float *dL_drotations, int *status, void *stream);
 int fgs_batch_forward(void *handle, void *stream);
 int fgs_batch_backward(void *handle, void *stream);
+/* Re-target the image output and upstream-gradient input ([3,H,W] each) of `count`
+ * views (view_ids[i] -> out_color[i], dL_dout_color[i]) for the launches that follow on
+ * `stream`.  The compositing kernels read these pointers from device memory, so a graph
+ * captured from fgs_batch_forward/backward follows the change without re-capture
+ * (double-buffered I/O).  dL_dout_color, or an entry of it, may be null (kept).     */
+int fgs_batch_set_view_io(void *handle, int count, const int *view_ids, float *const *out_color,
+                          const float *const *dL_dout_color, void *stream);
 /* Pair counts of the last forward per view (host [nviews]); synchronises. */
 int fgs_batch_pair_counts(void *handle, long long *counts, void *stream);
 /* Synchronise and return the first device-side error of the batch (FGS_OK when none). */

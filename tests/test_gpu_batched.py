@@ -1,7 +1,7 @@
 """GPU: the batched multi-view path (fgs_batch_*, CUDA-graph replay) against the
 plain one-view-per-call path.  Images and radii are bit-identical (same kernels,
 same arithmetic); the shared gradients equal the sum of the per-view gradients
-within float summation-order noise."""
+within the run-to-run noise of the gradient atomics (measured beside them)."""
 import numpy as np
 import pytest
 import torch
@@ -73,11 +73,13 @@ def test_batched_matches_plain(cuda, graph):
 
     a, b = plain_sums(), plain_sums()
     for k in a:
-        # float atomics make every run differ in the last bits (the plain path against itself
-        # sets the floor; conic sums with cancellation amplify it for scales / rotations)
+        # The gradient atomics make every run differ.  On this scene the sub-pixel Gaussians (2D
+        # covariance set by the 0.3 px dilation, 1/det^2 ~ 1e2) amplify that noise: the plain path
+        # against itself measured up to 4.5e-4 norm-relative for scales on one view.  The batched
+        # schedule (persistent CTAs) reorders the atomics further; both stay within 1e-3.
         floor = norm_rel(b[k], a[k])
         err = norm_rel(br.grad[k], a[k])
-        assert err <= max(1e-4, 5 * floor), (k, err, floor)
+        assert err <= max(1e-3, 5 * floor), (k, err, floor)
     K = br.pair_counts()
     assert all(0 < k <= c for k, c in zip(K, br.capacity))
 
@@ -95,3 +97,35 @@ def test_batched_capacity_overflow_is_reported(cuda):
     br.replan()                                            # exact counts again
     br.forward()
     br.check()
+
+
+def test_batched_set_io_retargets_captured_graph(cuda):
+    """Swapping a view's image / gradient buffers after capture: the replay writes the new image
+    buffer and reads the new gradient, with the same results as the original buffers."""
+    sc = _scene(P=100_000, seed=5005)
+    cams = _cams(3, seed=5006)
+    br = BatchedRasterizer(sc["means3D"], sc["opacities"], sc["scales"], sc["rotations"], cams, shs=sc["shs"],
+                           sh_degree=3, graph=True)
+    gen = torch.Generator(device="cuda").manual_seed(9)
+    for v in range(len(cams)):
+        br.dL[v].copy_(torch.randn(br.dL[v].shape, device="cuda", generator=gen))
+    br.step()
+    br.check()
+    img0 = [x.clone() for x in br.images]
+    g0 = {k: v.clone() for k, v in br.grad.items()}
+    old = list(br.images)
+    new_img = [torch.full_like(x, -1.0) for x in br.images]
+    new_dl = [2.0 * x for x in br.dL]
+    br.set_io_many([0, 1, 2], new_img, new_dl)
+    br.step()
+    br.check()
+    torch.cuda.synchronize()
+    for v in range(3):
+        assert torch.equal(new_img[v], img0[v]), v
+        assert torch.equal(old[v], img0[v]), v          # the old buffers were not written again
+    # the backward is linear in dL: doubled upstream gradients double every shared gradient (scaling by 2
+    # is exact; what differs is the order of the float atomics, amplified by cancellation in scales)
+    for k in g0:
+        assert norm_rel(br.grad[k], 2.0 * g0[k]) <= 1e-3, k
+    with pytest.raises(ValueError):
+        br.set_io(0, torch.empty(3, 5, 5, device="cuda"))
