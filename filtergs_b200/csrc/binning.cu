@@ -25,8 +25,10 @@ namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;
+constexpr int kSortItems = 16;                        // keys per thread, at most
+constexpr int kSortItemsMin = 4;                      // keys per thread, at least
+constexpr int kSortTile = kSortThreads * kSortItems;  // largest chunk
+constexpr int kSortTileMin = kSortThreads * kSortItemsMin;
 constexpr int kRadix = 256;
 // Exclusive scan of one value per thread over a 256-thread block.
 __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp /*[8]*/, uint32_t* total)
@@ -81,7 +83,14 @@ __global__ void __launch_bounds__(kSortThreads, 4)
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (n_dev) n = (uint32_t)min((unsigned long long)n, *n_dev);
-    const uint32_t live = (n + kSortTile - 1) / kSortTile;
+    // Keys per thread from the live count: about one chunk per resident CTA, between
+    // kSortItemsMin and kSortItems (a small sort gets more, shorter chunks; a large one
+    // fewer chunks and a shorter look-back chain).  The same on every CTA.
+    const uint32_t per_cta = (n + gridDim.x - 1) / gridDim.x;
+    const int items = (int)min((uint32_t)kSortItems,
+                               max((uint32_t)kSortItemsMin, (per_cta + kSortThreads - 1) / kSortThreads));
+    const uint32_t tile = (uint32_t)items * kSortThreads;
+    const uint32_t live = (n + tile - 1) / tile;
     if (blockIdx.x >= live) return;
     const uint32_t dmask = (1u << nbits) - 1u;
     // global start of every digit in this pass (the same for all chunks)
@@ -96,13 +105,14 @@ __global__ void __launch_bounds__(kSortThreads, 4)
         __syncthreads();
         const uint32_t chunk = s_chunk;
         if (chunk >= live) break;
-        const uint32_t base = chunk * kSortTile;
-        const uint32_t count = min((uint32_t)kSortTile, n - base);
+        const uint32_t base = chunk * tile;
+        const uint32_t count = min(tile, n - base);
 
         uint32_t key[kSortItems], rank[kSortItems];
 #pragma unroll
         for (int i = 0; i < kSortItems; i++) {
-            const uint32_t pos = warp * (kSortItems * 32) + i * 32 + lane;
+            if (i >= items) break;
+            const uint32_t pos = warp * (items * 32) + i * 32 + lane;
             const bool valid = pos < count;
             key[i] = valid ? __ldg(keys_in + base + pos) : 0xffffffffu;
             const uint32_t dg = valid ? ((key[i] >> shift) & dmask) : kRadix;
@@ -132,7 +142,8 @@ __global__ void __launch_bounds__(kSortThreads, 4)
         // local sort of the chunk by digit
 #pragma unroll
         for (int i = 0; i < kSortItems; i++) {
-            const uint32_t pos = warp * (kSortItems * 32) + i * 32 + lane;
+            if (i >= items) break;
+            const uint32_t pos = warp * (items * 32) + i * 32 + lane;
             if (pos < count) {
                 const uint32_t dg = (key[i] >> shift) & dmask;
                 const uint32_t lp = s_start[dg] + s_hist[warp][dg] + rank[i];
@@ -286,25 +297,10 @@ __global__ void ranges_kernel(const uint32_t* __restrict__ tile, uint32_t K, uin
 
 inline uint32_t chunks_of(long long n, int tile) { return (uint32_t)((n + tile - 1) / tile); }
 
-// Resident CTAs of a kernel on this device (persistent grids never exceed it).
-template <typename Kern>
-uint32_t resident_ctas(Kern k, int threads)
-{
-    static uint32_t cache[64] = {};  // per device ordinal; the same value if two threads race
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
-    int sms = 148, per = 1;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, 0);
-    const uint32_t r = (uint32_t)(sms * (per > 0 ? per : 1));
-    if (dev >= 0 && dev < 64) cache[dev] = r;
-    return r;
-}
 
 }  // namespace
 
-int sort_chunk_size() { return kSortTile; }
+int sort_chunk_size() { return kSortTileMin; }  // the smallest chunk: sizes the status words
 
 void launch_depth_sort(const GeomState& g, int P, cudaStream_t s)
 {
@@ -312,7 +308,7 @@ void launch_depth_sort(const GeomState& g, int P, cudaStream_t s)
     if (P <= 0) return;
     const uint32_t n = (uint32_t)P;
     const unsigned long long* V = g.total + 1;
-    const uint32_t nch = chunks_of(n, kSortTile);
+    const uint32_t nch = chunks_of(n, kSortTileMin);
     const uint32_t hb0 = (n + 1023) / 1024;
     const int hb = (int)(hb0 < 1184u ? hb0 : 1184u);
     depth_hist_kernel<<<hb, 256, 0, s>>>(g.depth_key, n, V, g.hist);
@@ -352,7 +348,7 @@ void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int ti
 {
     if (K <= 0) return;
     const uint32_t n = (uint32_t)K;
-    const uint32_t nch = chunks_of(n, kSortTile);
+    const uint32_t nch = chunks_of(n, kSortTileMin);
     const uint32_t grid = min(nch, resident_ctas(onesweep_kernel, kSortThreads));
     const int passes = (tile_bits + 7) / 8;
     const uint32_t* ki = (passes & 1) ? b.tile_a : b.tile_b;

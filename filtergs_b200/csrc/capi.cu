@@ -50,6 +50,7 @@ GeomCarve carve_geom(void* base, int P)
     r.g.sort_ids_a = c.take<uint32_t>(P);
     r.g.sort_ids_b = c.take<uint32_t>(P);
     r.g.sort_keys_b = c.take<uint32_t>(P);
+    r.g.cand_ids = c.take<uint32_t>(P);
     const size_t zero_off = c.off;
     r.g.hist = c.take<uint32_t>(8 * 256);
     r.g.counters = c.take<uint32_t>(16);

@@ -43,7 +43,8 @@ struct GeomState {
     uint32_t* hist;            // [8][256] radix histograms: 4 depth passes + up to 4 tile passes
     uint32_t* status;          // lookback status words, depth passes
     uint32_t* chunk_counts;    // [2][ceil(P/256)] preprocess chunk counts: visible (scanned in place), pairs
-    uint32_t* counters;        // [16] chunk counters: 0-3 depth passes, 4-7 tile passes, 8 pairs
+    uint32_t* cand_ids;        // [P] Gaussians that passed the preprocess tile bound (count in counters[12])
+    uint32_t* counters;        // [16] chunk counters: 0-3 depth passes, 4-7 tile passes, 8 pairs, 12 candidates
     unsigned long long* total; // [4]: 0 = K (pairs), 1 = V (visible count)
     unsigned int* err;         // error bit set
     size_t status_words;
@@ -75,6 +76,22 @@ BinState bin_views(void* base, long long K, int P);
 size_t bin_bytes(long long K, int P);
 
 // ---------------------------------------------------------------- launchers
+// Resident CTAs of a kernel on this device (persistent grids never exceed it).
+template <typename Kern>
+inline uint32_t resident_ctas(Kern k, int threads)
+{
+    static uint32_t cache[64] = {};  // per device ordinal; the same value if two threads race
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
+    int sms = 148, per = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, 0);
+    const uint32_t r = (uint32_t)(sms * (per > 0 ? per : 1));
+    if (dev >= 0 && dev < 64) cache[dev] = r;
+    return r;
+}
+
 void launch_preprocess(const PreParams& p, const GeomState& g, int* radii, cudaStream_t s);
 void launch_depth_sort(const GeomState& g, int P, cudaStream_t s);
 void launch_duplicate(const GeomState& g, const BinState& b, uint32_t V, uint32_t K, int W, int H, int tile_bits,

@@ -2,19 +2,21 @@
 //
 // preprocess: antialias/cuda_rasterizer/forward.cu:266-401 (EWA projection,
 // 2D dilation, OGFS opacity-aware radius, tile rectangle, SH degree<=3
-// colour), plus the optional 3D filter.  Each 256-thread chunk stages its
-// slice of the AoS parameter arrays through shared memory with coalesced
-// float4 loads, then every thread works on one Gaussian in registers.
+// colour), plus the optional 3D filter, in two passes: a cheap pass over all P
+// Gaussians (near plane, and a conservative bound on the tile rectangle that
+// needs no projection of the covariance) appends the few that may touch a
+// tile to a candidate list, and the exact path then runs over the candidates
+// on dense warps.  (In one pass, the ~6% visible Gaussians of a typical view
+// spread over nearly every warp and every warp pays for the exact path.)
 //
 // Radii and tiles-touched are written for every Gaussian.  Only the V
 // visible ones (tiles > 0) get the 48-byte render record and SH clamp bits.
 // They are then compacted in index order -- ids into sort_ids_b, depth bits
-// into depth_key -- by reduce-then-scan: each chunk of 256 leaves its visible
-// and pair counts, one CTA scans the chunk counts (and writes K and V to the
-// device), and a scatter pass places the ids.  (A single-pass look-back over
-// the P/256 chunks serialises on its prefix chain at this chunk size; the
-// two extra launches cost a few microseconds.)  The depth sort then runs over
-// V keys instead of P with the same result: equal depths keep index order.
+// into depth_key -- by reduce-then-scan over chunks of 256 ids: the exact pass
+// adds to its chunk's visible and pair counts, one CTA scans the chunk counts
+// (and writes K and V to the device), and a scatter pass places the ids.  The
+// depth sort then runs over V keys instead of P with the same result: equal
+// depths keep index order.
 #include "fgs_common.cuh"
 #include "fgs_internal.h"
 
@@ -24,21 +26,19 @@ namespace {
 
 constexpr int kThreads = 256;
 
-// Copy rows [row0, row0+rows) of an NF-float-per-row array into shared memory.
-template <int NF>
-__device__ __forceinline__ void stage_rows(const float* __restrict__ g, int row0, int rows, float* s, bool vec)
+// trace(cov3D) for cov3D = M^T M, M = S R (forward.cu:151-185): the sum of the
+// squared entries of M, row r of R scaled by s_r.
+__device__ __forceinline__ float cov3d_trace(float sx, float sy, float sz, float mod, float4 q)
 {
-    const float* src = g + (size_t)row0 * NF;
-    const int nf = rows * NF;
-    if (vec) {
-        const int nv = nf >> 2;
-        const float4* s4 = reinterpret_cast<const float4*>(src);
-        float4* d4 = reinterpret_cast<float4*>(s);
-        for (int v = threadIdx.x; v < nv; v += kThreads) d4[v] = __ldg(s4 + v);
-        for (int f = (nv << 2) + threadIdx.x; f < nf; f += kThreads) s[f] = __ldg(src + f);
-    } else {
-        for (int f = threadIdx.x; f < nf; f += kThreads) s[f] = __ldg(src + f);
-    }
+    const float r = q.x, x = q.y, y = q.z, z = q.w;
+    const float r0 = (1.f - 2.f * (y * y + z * z)) * (1.f - 2.f * (y * y + z * z)) +
+                     4.f * ((x * y + r * z) * (x * y + r * z) + (x * z - r * y) * (x * z - r * y));
+    const float r1 = (1.f - 2.f * (x * x + z * z)) * (1.f - 2.f * (x * x + z * z)) +
+                     4.f * ((x * y - r * z) * (x * y - r * z) + (y * z + r * x) * (y * z + r * x));
+    const float r2 = (1.f - 2.f * (x * x + y * y)) * (1.f - 2.f * (x * x + y * y)) +
+                     4.f * ((x * z + r * y) * (x * z + r * y) + (y * z - r * x) * (y * z - r * x));
+    const float a = mod * sx, b = mod * sy, c = mod * sz;
+    return a * a * r0 + b * b * r1 + c * c * r2;
 }
 
 // Conservative tile test before the projection (skips only Gaussians whose
@@ -49,8 +49,7 @@ __device__ __forceinline__ void stage_rows(const float* __restrict__ g, int row0
 // adds at most 0.3 per diagonal entry.  The OGFS radius is at most
 // max(1, ratio_min) * 3 sqrt(lambda_max) + 1 pixels.  The 1% + 1e-4 and +1 px
 // margins absorb the float rounding of the exact path.
-__device__ __forceinline__ bool may_touch_tiles(const PreParams& p, float3 t, const float cov3D[6], float px,
-                                                float py)
+__device__ __forceinline__ bool may_touch_tiles(const PreParams& p, float3 t, float tr3, float px, float py)
 {
     const float* v = p.view;
     const float limx = 1.3f * p.tanx, limy = 1.3f * p.tany;
@@ -60,7 +59,6 @@ __device__ __forceinline__ bool may_touch_tiles(const PreParams& p, float3 t, co
     const float j11 = p.fy / t.z, j21 = -(p.fy * ty) / (t.z * t.z);
     const float a0 = j00 * v[0] + j20 * v[2], a1 = j00 * v[4] + j20 * v[6], a2 = j00 * v[8] + j20 * v[10];
     const float b0 = j11 * v[1] + j21 * v[2], b1 = j11 * v[5] + j21 * v[6], b2 = j11 * v[9] + j21 * v[10];
-    const float tr3 = cov3D[0] + cov3D[3] + cov3D[5];
     const float lam = tr3 * (a0 * a0 + a1 * a1 + a2 * a2 + b0 * b0 + b1 * b1 + b2 * b2) + (p.use_filter ? 0.6f : 0.f);
     const float r = fmaxf(1.f, p.ratio_min) * 3.f * sqrtf(1.01f * lam + 1e-4f) + 2.f;
     if (!(r < 1e7f) || !(fabsf(px) < 1e9f) || !(fabsf(py) < 1e9f)) return true;  // no safe bound: exact path
@@ -70,26 +68,94 @@ __device__ __forceinline__ bool may_touch_tiles(const PreParams& p, float3 t, co
     return (x1 - x0) * (y1 - y0) != 0;
 }
 
-__global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomState g, int* __restrict__ radii_out)
+// Pass 1, every Gaussian: near plane and the conservative tile bound.  The
+// Gaussians that fail get radius 0 / no tiles here; the rest (typically a
+// small fraction of P) are appended to a candidate list, so that pass 2 --
+// projection, radius, colour -- runs on dense warps instead of on the few
+// live lanes of every warp.
+__global__ void __launch_bounds__(kThreads) preprocess_cull_kernel(PreParams p, GeomState g,
+                                                                   int* __restrict__ radii_out)
 {
-    __shared__ __align__(16) float s_mean[kThreads * 3];
-    __shared__ __align__(16) float s_scale[kThreads * 3];
-    __shared__ __align__(16) float s_rot[kThreads * 4];
-    __shared__ __align__(16) float s_opac[kThreads];
-    __shared__ uint32_t s_wv[kThreads / 32];
-    __shared__ unsigned long long s_wk[kThreads / 32];
-    __shared__ float s_log_lambda_G;
+    // Persistent CTAs collect their candidates in shared memory and reserve room
+    // in the global list once per flush: one atomic per CTA-flush instead of one
+    // per warp (same-address atomics from every warp serialise at L2).
+    constexpr int kList = 8 * kThreads;
+    __shared__ uint32_t s_list[kList];
+    __shared__ uint32_t s_wc[kThreads / 32];
+    __shared__ uint32_t s_n, s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    const int stride = gridDim.x * kThreads;
+    for (int idx0 = blockIdx.x * kThreads; idx0 < p.P; idx0 += stride) {
+        const int idx = idx0 + threadIdx.x;
+        bool cand = false;
+        if (idx < p.P) {
+            const float3 p_orig = {__ldg(p.means + 3 * (size_t)idx), __ldg(p.means + 3 * (size_t)idx + 1),
+                                   __ldg(p.means + 3 * (size_t)idx + 2)};
+            const float3 p_view = xform_point4x3(p_orig, p.view);
+            if (p_view.z <= 0.2f) {  // auxiliary.h:139-164
+                if (p.prefiltered) set_error(g.err, FGS_ERR_PREFILTERED);
+            } else if (p.cov3D) {
+                cand = true;  // no bound for an arbitrary precomputed covariance
+            } else {
+                const float4 p_hom = xform_point4x4(p_orig, p.proj);
+                const float p_w = 1.0f / (p_hom.w + 0.0000001f);
+                const float px = ndc_to_pix(p_hom.x * p_w, p.W), py = ndc_to_pix(p_hom.y * p_w, p.H);
+                const float4 q = p.aligned ? __ldg(reinterpret_cast<const float4*>(p.rots) + idx)
+                                           : make_float4(__ldg(p.rots + 4 * (size_t)idx), __ldg(p.rots + 4 * (size_t)idx + 1),
+                                                         __ldg(p.rots + 4 * (size_t)idx + 2), __ldg(p.rots + 4 * (size_t)idx + 3));
+                float tr = cov3d_trace(__ldg(p.scales + 3 * (size_t)idx), __ldg(p.scales + 3 * (size_t)idx + 1),
+                                       __ldg(p.scales + 3 * (size_t)idx + 2), p.scale_mod, q);
+                if (p.filter3d > 0.f) {
+                    const float sf = p.filter3d * p_view.z / p.fx;
+                    tr += 3.f * sf * sf;
+                }
+                cand = may_touch_tiles(p, p_view, tr, px, py);
+            }
+            if (!cand) {
+                g.tiles[idx] = 0;
+                g.radii[idx] = 0;
+                if (radii_out) radii_out[idx] = 0;
+            }
+        }
+        // append to the CTA's list (the order is irrelevant: the visible set is
+        // compacted in index order afterwards)
+        const unsigned cb = __ballot_sync(0xffffffffu, cand);
+        if (lane == 0) s_wc[warp] = __popc(cb);
+        __syncthreads();
+        uint32_t pos = s_n + __popc(cb & ((1u << lane) - 1u)), tot = 0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; w++) {
+            if (w < warp) pos += s_wc[w];
+            tot += s_wc[w];
+        }
+        if (cand) s_list[pos] = (uint32_t)idx;
+        __syncthreads();
+        const uint32_t n = s_n + tot;
+        const bool last = idx0 + stride >= p.P;
+        if (n > kList - kThreads || last) {
+            if (threadIdx.x == 0) s_base = n ? atomicAdd(g.counters + 12, n) : 0u;
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < n; k += kThreads) g.cand_ids[s_base + k] = s_list[k];
+            __syncthreads();
+            if (threadIdx.x == 0) s_n = 0;
+        } else if (threadIdx.x == 0) {
+            s_n = n;
+        }
+        __syncthreads();
+    }
+}
 
-    const uint32_t chunk = blockIdx.x;
-    const int row0 = (int)chunk * kThreads;
-    const int rows = min(kThreads, p.P - row0);
-    const bool vec = p.aligned != 0;
-    stage_rows<3>(p.means, row0, rows, s_mean, vec);
-    stage_rows<1>(p.opac, row0, rows, s_opac, vec);
-    if (p.scales) stage_rows<3>(p.scales, row0, rows, s_scale, vec);
-    if (p.rots) stage_rows<4>(p.rots, row0, rows, s_rot, vec);
+// Pass 2, the candidates: the exact path (forward.cu:266-401), one Gaussian per
+// thread.  Visible Gaussians add to the per-chunk (256 consecutive ids) visible
+// and pair counts that the ordered compaction scans.
+__global__ void __launch_bounds__(kThreads) preprocess_full_kernel(PreParams p, GeomState g,
+                                                                   int* __restrict__ radii_out)
+{
+    __shared__ float s_log_lambda_G;
     if (threadIdx.x == 0) {
-        // forward.cu:345-355: the opacity-independent part of the OGFS radius, once per chunk
+        // forward.cu:345-355: the opacity-independent part of the OGFS radius, once per CTA
         const float epsilon_pix = 1.0f / 255.0f;
         const float eps_base = fmaxf(0.0f, 1.0f - epsilon_pix);
         const float lambda_G_raw = 1.0f - powf(eps_base, static_cast<float>(kOgfsBlockArea));
@@ -98,148 +164,113 @@ __global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomS
         s_log_lambda_G = logf(lambda_G);
     }
     __syncthreads();
-
-    const int t = threadIdx.x;
-    const int idx = row0 + t;
-    uint32_t tiles = 0;
-    if (idx < p.P) {
+    const uint32_t ncand = *(volatile uint32_t*)(g.counters + 12);
+    const bool vec = p.aligned != 0;
+    for (uint32_t k = blockIdx.x * kThreads + threadIdx.x; k < ncand; k += gridDim.x * kThreads) {
+        const int idx = (int)g.cand_ids[k];
+        uint32_t tiles = 0;
         int radius_px = 0;
         uint8_t clamp_bits = 0;
         PairRecord rec;
-        rec.a = make_float4(0.f, 0.f, 0.f, 0.f);
-        rec.b = rec.a;
-        rec.c = make_float4(0.f, __int_as_float(idx), 0.f, 0.f);
-        const float3 p_orig = {s_mean[3 * t], s_mean[3 * t + 1], s_mean[3 * t + 2]};
-        // auxiliary.h:139-164 (near plane at view z = 0.2)
+        const float3 p_orig = {__ldg(p.means + 3 * (size_t)idx), __ldg(p.means + 3 * (size_t)idx + 1),
+                               __ldg(p.means + 3 * (size_t)idx + 2)};
         const float4 p_hom = xform_point4x4(p_orig, p.proj);
         const float p_w = 1.0f / (p_hom.w + 0.0000001f);
         const float3 p_proj = {p_hom.x * p_w, p_hom.y * p_w, p_hom.z * p_w};
         const float3 p_view = xform_point4x3(p_orig, p.view);
         const float px = ndc_to_pix(p_proj.x, p.W), py = ndc_to_pix(p_proj.y, p.H);
-        bool live = true;
-        if (p_view.z <= 0.2f) {
-            live = false;
-            if (p.prefiltered) set_error(g.err, FGS_ERR_PREFILTERED);
-        }
         float cov3D[6];
-        if (live) {
-            if (p.cov3D) {
+        if (p.cov3D) {
 #pragma unroll
-                for (int k = 0; k < 6; k++) cov3D[k] = __ldg(p.cov3D + (size_t)idx * 6 + k);
-            } else {
-                const float4 q = {s_rot[4 * t], s_rot[4 * t + 1], s_rot[4 * t + 2], s_rot[4 * t + 3]};
-                cov3d_from_scale_rot(s_scale[3 * t], s_scale[3 * t + 1], s_scale[3 * t + 2], p.scale_mod, q, cov3D);
-            }
-            if (p.filter3d > 0.f) {
-                // 3D filter: isotropic variance of a sigma = s * z / focal blur.
-                const float sf = p.filter3d * p_view.z / p.fx;
-                const float v = sf * sf;
-                cov3D[0] += v; cov3D[3] += v; cov3D[5] += v;
-            }
-            if (!p.cov3D && !may_touch_tiles(p, p_view, cov3D, px, py)) live = false;
+            for (int c = 0; c < 6; c++) cov3D[c] = __ldg(p.cov3D + (size_t)idx * 6 + c);
+        } else {
+            const float4 q = vec ? __ldg(reinterpret_cast<const float4*>(p.rots) + idx)
+                                 : make_float4(__ldg(p.rots + 4 * (size_t)idx), __ldg(p.rots + 4 * (size_t)idx + 1),
+                                               __ldg(p.rots + 4 * (size_t)idx + 2), __ldg(p.rots + 4 * (size_t)idx + 3));
+            cov3d_from_scale_rot(__ldg(p.scales + 3 * (size_t)idx), __ldg(p.scales + 3 * (size_t)idx + 1),
+                                 __ldg(p.scales + 3 * (size_t)idx + 2), p.scale_mod, q, cov3D);
         }
-        if (live) {
-            float3 cov = ewa_cov2d(p_orig, p.fx, p.fy, p.tanx, p.tany, cov3D, p.view);
-            if (p.use_filter) {
-                cov.x = dilate_max(cov.x);
-                cov.z = dilate_max(cov.z);
-            }
-            const float det = (cov.x * cov.z - cov.y * cov.y);
-            if (det == 0.0f) live = false;
-            if (live) {
-                const float det_inv = 1.f / det;
-                const float3 conic = {cov.z * det_inv, -cov.y * det_inv, cov.x * det_inv};
-                // forward.cu:345-369: OGFS radius
-                const float opacity = fmaxf(s_opac[t], 1e-6f);
-                const float log_lambda_G = s_log_lambda_G;
-                const float log_opacity = logf(opacity);
-                const float radius_energy = log_opacity - log_lambda_G;
-                const float energy_clamped = fmaxf(radius_energy, p.energy_floor);
-                const float mid = 0.5f * (cov.x + cov.z);
-                const float disc = fmaxf(0.0f, mid * mid - det);
-                const float sqrt_disc = sqrtf(disc);
-                const float lambda1 = mid + sqrt_disc;
-                const float lambda2 = mid - sqrt_disc;
-                const float max_lambda = fmaxf(fmaxf(lambda1, lambda2), 1e-6f);
-                const float radius_base = 3.0f * sqrtf(max_lambda);
-                float radius_major = sqrtf(2.0f * energy_clamped * max_lambda);
-                radius_major = fminf(radius_major, radius_base);
-                radius_major = fmaxf(radius_major, p.ratio_min * radius_base);
-                const float radius_f = radius_major + 1.0f;
-                const int rpx = max(1, static_cast<int>(ceilf(radius_f)));
-                const int gx = (p.W + kTileX - 1) / kTileX, gy = (p.H + kTileY - 1) / kTileY;
-                int x0, y0, x1, y1;
-                tile_rect(px, py, rpx, gx, gy, kTileX, kTileY, x0, y0, x1, y1);
-                const int extent = (x1 - x0) * (y1 - y0);
-                if (extent != 0) {
-                    float3 rgb;
-                    if (p.colors) {
-                        rgb = {__ldg(p.colors + 3 * (size_t)idx), __ldg(p.colors + 3 * (size_t)idx + 1),
-                               __ldg(p.colors + 3 * (size_t)idx + 2)};
+        if (p.filter3d > 0.f) {
+            // 3D filter: isotropic variance of a sigma = s * z / focal blur.
+            const float sf = p.filter3d * p_view.z / p.fx;
+            const float v = sf * sf;
+            cov3D[0] += v; cov3D[3] += v; cov3D[5] += v;
+        }
+        float3 cov = ewa_cov2d(p_orig, p.fx, p.fy, p.tanx, p.tany, cov3D, p.view);
+        if (p.use_filter) {
+            cov.x = dilate_max(cov.x);
+            cov.z = dilate_max(cov.z);
+        }
+        const float det = (cov.x * cov.z - cov.y * cov.y);
+        if (det != 0.0f) {
+            const float det_inv = 1.f / det;
+            const float3 conic = {cov.z * det_inv, -cov.y * det_inv, cov.x * det_inv};
+            // forward.cu:345-369: OGFS radius
+            const float opacity = fmaxf(__ldg(p.opac + idx), 1e-6f);
+            const float log_opacity = logf(opacity);
+            const float radius_energy = log_opacity - s_log_lambda_G;
+            const float energy_clamped = fmaxf(radius_energy, p.energy_floor);
+            const float mid = 0.5f * (cov.x + cov.z);
+            const float disc = fmaxf(0.0f, mid * mid - det);
+            const float sqrt_disc = sqrtf(disc);
+            const float lambda1 = mid + sqrt_disc;
+            const float lambda2 = mid - sqrt_disc;
+            const float max_lambda = fmaxf(fmaxf(lambda1, lambda2), 1e-6f);
+            const float radius_base = 3.0f * sqrtf(max_lambda);
+            float radius_major = sqrtf(2.0f * energy_clamped * max_lambda);
+            radius_major = fminf(radius_major, radius_base);
+            radius_major = fmaxf(radius_major, p.ratio_min * radius_base);
+            const float radius_f = radius_major + 1.0f;
+            const int rpx = max(1, static_cast<int>(ceilf(radius_f)));
+            const int gx = (p.W + kTileX - 1) / kTileX, gy = (p.H + kTileY - 1) / kTileY;
+            int x0, y0, x1, y1;
+            tile_rect(px, py, rpx, gx, gy, kTileX, kTileY, x0, y0, x1, y1);
+            const int extent = (x1 - x0) * (y1 - y0);
+            if (extent != 0) {
+                float3 rgb;
+                if (p.colors) {
+                    rgb = {__ldg(p.colors + 3 * (size_t)idx), __ldg(p.colors + 3 * (size_t)idx + 1),
+                           __ldg(p.colors + 3 * (size_t)idx + 2)};
+                } else {
+                    // SH row: 12 float4 loads when the row is 16-byte aligned.
+                    float sh[48];
+                    const int nf = p.M * 3;
+                    const float* row = p.shs + (size_t)idx * nf;
+                    const int ncoef = (p.D + 1) * (p.D + 1);
+                    const int need = min(nf, ncoef * 3);
+                    if (vec && (nf & 3) == 0) {
+                        const float4* r4 = reinterpret_cast<const float4*>(row);
+#pragma unroll
+                        for (int v = 0; v < 12; v++)
+                            if (4 * v < need) {
+                                const float4 q = __ldg(r4 + v);
+                                sh[4 * v] = q.x; sh[4 * v + 1] = q.y; sh[4 * v + 2] = q.z; sh[4 * v + 3] = q.w;
+                            }
                     } else {
-                        // SH row: 12 float4 loads when the row is 16-byte aligned.
-                        float sh[48];
-                        const int nf = p.M * 3;
-                        const float* row = p.shs + (size_t)idx * nf;
-                        const int ncoef = (p.D + 1) * (p.D + 1);
-                        const int need = min(nf, ncoef * 3);
-                        if (vec && (nf & 3) == 0) {
-                            const float4* r4 = reinterpret_cast<const float4*>(row);
 #pragma unroll
-                            for (int v = 0; v < 12; v++)
-                                if (4 * v < need) {
-                                    const float4 q = __ldg(r4 + v);
-                                    sh[4 * v] = q.x; sh[4 * v + 1] = q.y; sh[4 * v + 2] = q.z; sh[4 * v + 3] = q.w;
-                                }
-                        } else {
-#pragma unroll
-                            for (int f = 0; f < 48; f++)
-                                if (f < need) sh[f] = __ldg(row + f);
-                        }
-                        const float3 cam = {__ldg(p.campos), __ldg(p.campos + 1), __ldg(p.campos + 2)};
-                        rgb = sh_to_rgb(p.D, sh, p_orig, cam, clamp_bits);
+                        for (int f = 0; f < 48; f++)
+                            if (f < need) sh[f] = __ldg(row + f);
                     }
-                    radius_px = rpx;
-                    tiles = (uint32_t)extent;
-                    rec.a = make_float4(px, py, conic.x, conic.y);
-                    rec.b = make_float4(conic.z, opacity, rgb.x, rgb.y);
-                    rec.c = make_float4(rgb.z, __int_as_float(idx), p_view.z, 0.f);
+                    const float3 cam = {__ldg(p.campos), __ldg(p.campos + 1), __ldg(p.campos + 2)};
+                    rgb = sh_to_rgb(p.D, sh, p_orig, cam, clamp_bits);
                 }
+                radius_px = rpx;
+                tiles = (uint32_t)extent;
+                rec.a = make_float4(px, py, conic.x, conic.y);
+                rec.b = make_float4(conic.z, opacity, rgb.x, rgb.y);
+                rec.c = make_float4(rgb.z, __int_as_float(idx), p_view.z, 0.f);
             }
         }
         if (tiles) {
             g.grec[idx] = rec;
             g.clamped[idx] = clamp_bits;
+            const uint32_t nch = (uint32_t)((p.P + kThreads - 1) / kThreads);
+            atomicAdd(g.chunk_counts + idx / kThreads, 1u);
+            atomicAdd(g.chunk_counts + nch + idx / kThreads, tiles);
         }
         g.tiles[idx] = tiles;
         g.radii[idx] = radius_px;
         if (radii_out) radii_out[idx] = radius_px;
-    }
-    // Per-chunk visible and pair counts (scanned by chunk_scan_kernel).
-    const int lane = t & 31, warp = t >> 5;
-    const unsigned vb = __ballot_sync(0xffffffffu, tiles != 0);
-    unsigned long long k = tiles;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(0xffffffffu, k, o);
-    if (lane == 0) {
-        s_wv[warp] = __popc(vb);
-        s_wk[warp] = k;
-    }
-    __syncthreads();
-    if (t == 0) {
-        uint32_t vtot = 0;
-        unsigned long long ktot = 0;
-#pragma unroll
-        for (int w = 0; w < kThreads / 32; w++) {
-            vtot += s_wv[w];
-            ktot += s_wk[w];
-        }
-        if (ktot > 0xffffffffull) {
-            set_error(g.err, FGS_ERR_OVERFLOW);
-            ktot = 0xffffffffull;
-        }
-        g.chunk_counts[chunk] = vtot;
-        g.chunk_counts[gridDim.x + chunk] = (uint32_t)ktot;
     }
 }
 
@@ -249,13 +280,27 @@ __global__ void __launch_bounds__(kThreads) preprocess_kernel(PreParams p, GeomS
 __global__ void __launch_bounds__(1024) chunk_scan_kernel(uint32_t* __restrict__ counts, uint32_t nch,
                                                          unsigned long long* __restrict__ total)
 {
+    // Up to kReg chunks per thread are held in registers, so all loads are in
+    // flight at once (P <= 1024 * kReg * 256 = 4M); larger P loops.
+    constexpr int kReg = 16;
     __shared__ unsigned long long s_v[32], s_k[32];
     const uint32_t per = (nch + 1023) / 1024;
     const uint32_t b = min(nch, threadIdx.x * per), e = min(nch, b + per);
     unsigned long long sv = 0, sk = 0;
-    for (uint32_t i = b; i < e; i++) {
-        sv += counts[i];
-        sk += counts[nch + i];
+    uint32_t v[kReg];
+    if (per <= (uint32_t)kReg) {
+#pragma unroll
+        for (int i = 0; i < kReg; i++) {
+            v[i] = b + i < e ? counts[b + i] : 0u;
+            sk += b + i < e ? counts[nch + b + i] : 0u;
+        }
+#pragma unroll
+        for (int i = 0; i < kReg; i++) sv += v[i];
+    } else {
+        for (uint32_t i = b; i < e; i++) {
+            sv += counts[i];
+            sk += counts[nch + i];
+        }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long x = sv;
@@ -276,10 +321,19 @@ __global__ void __launch_bounds__(1024) chunk_scan_kernel(uint32_t* __restrict__
         ktot += s_k[w];
     }
     unsigned long long excl = wpre + x - sv;
-    for (uint32_t i = b; i < e; i++) {
-        const uint32_t c = counts[i];
-        counts[i] = (uint32_t)excl;
-        excl += c;
+    if (per <= (uint32_t)kReg) {
+#pragma unroll
+        for (int i = 0; i < kReg; i++)
+            if (b + i < e) {
+                counts[b + i] = (uint32_t)excl;
+                excl += v[i];
+            }
+    } else {
+        for (uint32_t i = b; i < e; i++) {
+            const uint32_t c = counts[i];
+            counts[i] = (uint32_t)excl;
+            excl += c;
+        }
     }
     if (threadIdx.x == 0) {
         total[0] = ktot;
@@ -456,11 +510,13 @@ void launch_preprocess(const PreParams& p, const GeomState& g, int* radii, cudaS
 {
     if (p.P <= 0) return;
     const uint32_t nch = (uint32_t)((p.P + kThreads - 1) / kThreads);
-    preprocess_kernel<<<nch, kThreads, 0, s>>>(p, g, radii);
+    preprocess_cull_kernel<<<min(nch, resident_ctas(preprocess_cull_kernel, kThreads)), kThreads, 0, s>>>(
+        p, g, radii);
+    preprocess_full_kernel<<<resident_ctas(preprocess_full_kernel, kThreads), kThreads, 0, s>>>(p, g, radii);
     chunk_scan_kernel<<<1, 1024, 0, s>>>(g.chunk_counts, nch, g.total);
     compact_visible_kernel<<<nch, kThreads, 0, s>>>(p.P, g.tiles, g.grec, g.chunk_counts, g.sort_ids_b,
                                                     g.depth_key);
-    note_launches(3);
+    note_launches(4);
 }
 
 void launch_compute_radius(int variant, int P, const float* means, const float* scales, const float* rots,
