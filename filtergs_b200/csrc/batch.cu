@@ -7,7 +7,9 @@
 // memsets on the caller's stream -- no host synchronisation, no allocation --
 // so the pair can be captured into a CUDA graph and replayed.  Per view the
 // front end (preprocess, depth sort, pair emission, tile sort, ranges) runs
-// with the pair count kept on the device; compositing, forward and backward,
+// with the pair count kept on the device, the views spread over four streams
+// forked from the caller's stream and joined before compositing (those kernels
+// are latency-bound, so views overlap); compositing, forward and backward,
 // is ONE persistent launch per direction over the tiles of all views, fed by a
 // global work queue.  Backward sums every view's gradients into shared dense
 // buffers (views in stream order, so each row has a single writer at a time).
@@ -40,8 +42,20 @@ struct ViewState {
     int* radii_out;
 };
 
+constexpr int kFrontStreams = 4;  // views whose front ends run concurrently
+
 struct Batch {
     int P, V, consistent;
+    // fork/join of the per-view front ends over auxiliary streams (graph-capturable)
+    std::vector<cudaStream_t> aux;
+    std::vector<cudaEvent_t> joined;
+    cudaEvent_t forked = nullptr;
+    ~Batch()
+    {
+        for (cudaStream_t x : aux) cudaStreamDestroy(x);
+        for (cudaEvent_t e : joined) cudaEventDestroy(e);
+        if (forked) cudaEventDestroy(forked);
+    }
     std::vector<ViewState> views;
     TileArgs* d_args_fwd;
     TileArgs* d_args_bwd;
@@ -144,6 +158,22 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
     B->P = P;
     B->V = nviews;
     B->consistent = backward_mode == FGS_BACKWARD_CONSISTENT;
+    {
+        const int ns = nviews < kFrontStreams ? nviews : kFrontStreams;
+        bool ok = cudaEventCreateWithFlags(&B->forked, cudaEventDisableTiming) == cudaSuccess;
+        for (int i = 0; ok && i < ns; i++) {
+            cudaStream_t x = nullptr;
+            cudaEvent_t e = nullptr;
+            ok = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking) == cudaSuccess;
+            if (ok) B->aux.push_back(x);
+            ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+            if (ok) B->joined.push_back(e);
+        }
+        if (!ok) {
+            delete B;
+            return fail(FGS_ERR_CUDA);
+        }
+    }
     B->background = shared->background;
     B->g_means3D = dL_dmeans3D;
     B->g_opacity = dL_dopacity;
@@ -248,28 +278,40 @@ int fgs_batch_forward(void* handle, void* stream)
     Batch* B = static_cast<Batch*>(handle);
     if (!B) return FGS_ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    for (ViewState& v : B->views) {
+    // The per-view front ends are independent and mostly latency-bound (scans with
+    // look-back, small sorts): they run on kFrontStreams streams forked from `s`
+    // and joined back before the one compositing launch over all views.
+    const int ns = (int)B->aux.size();
+    if (cudaEventRecord(B->forked, s) != cudaSuccess) return FGS_ERR_CUDA;
+    for (int i = 0; i < ns; i++) cudaStreamWaitEvent(B->aux[i], B->forked, 0);
+    for (int vi = 0; vi < B->V; vi++) {
+        ViewState& v = B->views[vi];
+        cudaStream_t vs = B->aux[vi % ns];
         {
-            StageTimer t(FGS_STAGE_PREPROCESS, s);
+            StageTimer t(FGS_STAGE_PREPROCESS, vs);
             char* zero_begin = reinterpret_cast<char*>(v.g.hist);
-            cudaMemsetAsync(zero_begin, 0, (size_t)(v.geom_base + v.geom_bytes_v - zero_begin), s);
-            launch_preprocess(v.pre, v.g, v.radii_out, s);
+            cudaMemsetAsync(zero_begin, 0, (size_t)(v.geom_base + v.geom_bytes_v - zero_begin), vs);
+            launch_preprocess(v.pre, v.g, v.radii_out, vs);
         }
-        StageTimer t(FGS_STAGE_DEPTH_SORT, s);
-        launch_depth_sort(v.g, B->P, s);
-    }
-    for (ViewState& v : B->views) {
+        {
+            StageTimer t(FGS_STAGE_DEPTH_SORT, vs);
+            launch_depth_sort(v.g, B->P, vs);
+        }
         if (v.cap > 0) {
             {
-                StageTimer t(FGS_STAGE_DUPLICATE, s);
-                cudaMemsetAsync(v.b.status, 0, sizeof(uint32_t) * (v.b.status_words + v.b.scan_words), s);
-                launch_duplicate(v.g, v.b, (uint32_t)B->P, (uint32_t)v.cap, v.pre.W, v.pre.H, v.tile_bits, s);
+                StageTimer t(FGS_STAGE_DUPLICATE, vs);
+                cudaMemsetAsync(v.b.status, 0, sizeof(uint32_t) * (v.b.status_words + v.b.scan_words), vs);
+                launch_duplicate(v.g, v.b, (uint32_t)B->P, (uint32_t)v.cap, v.pre.W, v.pre.H, v.tile_bits, vs);
             }
-            StageTimer t(FGS_STAGE_TILE_SORT, s);
-            launch_tile_sort(v.g, v.b, v.cap, v.tile_bits, s, v.g.total);
+            StageTimer t(FGS_STAGE_TILE_SORT, vs);
+            launch_tile_sort(v.g, v.b, v.cap, v.tile_bits, vs, v.g.total);
         }
-        StageTimer t(FGS_STAGE_RANGES, s);
-        launch_ranges(v.b, v.im, v.cap, v.num_tiles, s, v.g.total);
+        StageTimer t(FGS_STAGE_RANGES, vs);
+        launch_ranges(v.b, v.im, v.cap, v.num_tiles, vs, v.g.total);
+    }
+    for (int i = 0; i < ns; i++) {
+        cudaEventRecord(B->joined[i], B->aux[i]);
+        cudaStreamWaitEvent(s, B->joined[i], 0);
     }
     StageTimer t(FGS_STAGE_RENDER_FWD, s);
     launch_render_fwd_multi(B->d_args_fwd, B->d_begin, B->V, B->total_tiles, B->d_queue, B->d_err, s);
