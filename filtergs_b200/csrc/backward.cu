@@ -148,17 +148,62 @@ __device__ __forceinline__ float3 sh_backward(int deg, const float* __restrict__
     return dnormvdv(dir_orig, ddir);
 }
 
+// Screen-space gradients of the visible Gaussians: the sum of each Gaussian's
+// per-pair gradients (pgrad rows at its emission indices, its tiles row-major).
+// One warp per Gaussian: lane l takes rows l, l+32, ... (coalesced 36-byte rows,
+// 128 rows in flight per round trip, so a splat over thousands of tiles does not
+// stall the kernel) and a fixed shuffle tree adds them, 32 rows at a time in
+// emission order -- the same sum on every run.  Row layout: dcolor r,g,b |
+// dmean2D x,y | dconic x,y,w | dopacity.
+__global__ void __launch_bounds__(256)
+    pair_grad_gather_kernel(const uint32_t* __restrict__ visible_ids, const unsigned long long* __restrict__ visible_count,
+                            const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ pair_off,
+                            const float* __restrict__ pgrad, float* __restrict__ dmean2D, float* __restrict__ dconic,
+                            float* __restrict__ dcolor, float* __restrict__ dopac)
+{
+    const uint32_t V = (uint32_t)*visible_count;
+    const int lane = threadIdx.x & 31;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < V; j += nwarps) {
+        const int idx = (int)visible_ids[j];
+        const uint32_t e0 = __ldg(pair_off + idx), ne = __ldg(tiles + idx);
+        float acc = 0.f;  // lanes 2q and 2q+1: component q
+        for (uint32_t k = 0; k < ne; k += 128) {
+            float v[4][9];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint32_t r = k + 32 * u + lane;
+                const float* src = pgrad + (size_t)(e0 + r) * 9;
+#pragma unroll
+                for (int q = 0; q < 9; q++) v[u][q] = r < ne ? __ldg(src + q) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (k + 32 * u < ne) acc += warp_transpose_sum9(v[u]);
+        }
+        if (lane < 18 && !(lane & 1)) {
+            const int q = lane >> 1;
+            float* dst = q < 3 ? dcolor + 3 * idx + q
+                       : q < 5 ? dmean2D + 3 * idx + (q - 3)
+                       : q == 7 ? dconic + 4 * idx + 3
+                       : q < 8 ? dconic + 4 * idx + (q - 5)
+                               : dopac + idx;
+            *dst = acc;
+        }
+    }
+}
+
 // kAccum: add this view's gradients into dense buffers shared by several views
 // (views run one after another on a stream, so each row has one writer at a
 // time) and fold the view's opacity gradient into shared_dopac.
 template <bool kAccum>
 __global__ void __launch_bounds__(256)
     preprocess_bwd_kernel(PreParams p, const uint32_t* __restrict__ visible_ids,
-                          const unsigned long long* __restrict__ visible_count, const uint8_t* __restrict__ clamped,
-                          const float* __restrict__ dmean2D, const float* __restrict__ dconic,
-                          const float* __restrict__ dcolor, float* __restrict__ dopac, float* __restrict__ dmean3D,
-                          float* __restrict__ dcov3D, float* __restrict__ dsh, float* __restrict__ dscale,
-                          float* __restrict__ drot, int consistent, float* __restrict__ shared_dopac)
+                          const unsigned long long* __restrict__ visible_count, float* __restrict__ dmean2D,
+                          const float* __restrict__ dconic, float* __restrict__ dopac, float* __restrict__ dmean3D,
+                          float* __restrict__ dcov3D,
+                          float* __restrict__ dscale, float* __restrict__ drot, int consistent,
+                          float* __restrict__ shared_dopac, bool sh_follows)
 {
     // The forward's depth ordering put the V visible Gaussians first; culled
     // rows were zero-filled by the launcher.
@@ -330,7 +375,15 @@ __global__ void __launch_bounds__(256)
             dopac[idx] = 0.f;
         }
     }
-    if (kAccum) {
+    if (kAccum && sh_follows) {
+        // the SH pass adds its term and then accumulates the view's total (the same
+        // sum, in the same order, as the plain backward of this view)
+        dmean2D[3 * idx] = dm.x;
+        dmean2D[3 * idx + 1] = dm.y;
+        dmean2D[3 * idx + 2] = dm.z;
+#pragma unroll
+        for (int k = 0; k < 6; k++) dcov3D[6 * (size_t)idx + k] += dc[k];
+    } else if (kAccum) {
         dmean3D[3 * idx] += dm.x;
         dmean3D[3 * idx + 1] += dm.y;
         dmean3D[3 * idx + 2] += dm.z;
@@ -354,7 +407,8 @@ template <bool kAccum>
 __global__ void __launch_bounds__(256, 3)
     sh_bwd_kernel(PreParams p, const uint32_t* __restrict__ visible_ids,
                   const unsigned long long* __restrict__ visible_count, const uint8_t* __restrict__ clamped,
-                  const float* __restrict__ dcolor, float* __restrict__ dmean3D, float* __restrict__ dsh)
+                  const float* __restrict__ dcolor, const float* __restrict__ dm_geo, float* __restrict__ dmean3D,
+                  float* __restrict__ dsh)
 {
     const uint32_t V = (uint32_t)*visible_count;
     const bool vec = p.aligned && ((p.M * 3) & 3) == 0;
@@ -365,20 +419,24 @@ __global__ void __launch_bounds__(256, 3)
         const float3 dcol = {dcolor[3 * idx], dcolor[3 * idx + 1], dcolor[3 * idx + 2]};
         const float3 dmd = sh_backward<kAccum>(p.D, p.shs + (size_t)idx * p.M * 3, mean, cam, clamped[idx], dcol,
                                                dsh + (size_t)idx * p.M * 3, p.M, vec);
-        dmean3D[3 * idx] += dmd.x;
-        dmean3D[3 * idx + 1] += dmd.y;
-        dmean3D[3 * idx + 2] += dmd.z;
+        if (kAccum) {  // this view's total, then into the shared sum
+            dmean3D[3 * idx] += dm_geo[3 * idx] + dmd.x;
+            dmean3D[3 * idx + 1] += dm_geo[3 * idx + 1] + dmd.y;
+            dmean3D[3 * idx + 2] += dm_geo[3 * idx + 2] + dmd.z;
+        } else {
+            dmean3D[3 * idx] += dmd.x;
+            dmean3D[3 * idx + 1] += dmd.y;
+            dmean3D[3 * idx + 2] += dmd.z;
+        }
     }
 }
 
 }  // namespace
 
-void launch_preprocess_bwd(const PreParams& p, const int* radii, const GeomState& g, const float* dmean2D,
-                           const float* dconic, const float* dcolor, float* dopac, float* dmean3D, float* dcov3D,
-                           float* dsh, float* dscale, float* drot, int consistent, cudaStream_t s, bool accumulate,
-                           float* shared_dopac)
+void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* pgrad, float* dmean2D, float* dconic,
+                           float* dcolor, float* dopac, float* dmean3D, float* dcov3D, float* dsh, float* dscale,
+                           float* drot, int consistent, cudaStream_t s, bool accumulate, float* shared_dopac)
 {
-    (void)radii;
     if (p.P <= 0) return;
     const size_t P = (size_t)p.P;
     if (!accumulate) {
@@ -394,20 +452,22 @@ void launch_preprocess_bwd(const PreParams& p, const int* radii, const GeomState
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int blocks = (int)std::min<size_t>((P + 255) / 256, (size_t)sms * 8);
     const bool sh = p.shs && dsh;
+    pair_grad_gather_kernel<<<blocks, 256, 0, s>>>(g.sort_ids_b, g.total + 1, g.tiles, g.pair_off, pgrad, dmean2D,
+                                                   dconic, dcolor, dopac);
     if (accumulate) {
-        preprocess_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dmean2D, dconic,
-                                                           dcolor, dopac, dmean3D, dcov3D, dsh, dscale, drot,
-                                                           consistent, shared_dopac);
+        preprocess_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, dmean2D, dconic, dopac,
+                                                           dmean3D, dcov3D, dscale, drot, consistent, shared_dopac, sh);
         if (sh)
-            sh_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dcolor, dmean3D, dsh);
+            sh_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dcolor, dmean2D,
+                                                       dmean3D, dsh);
     } else {
-        preprocess_bwd_kernel<false><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dmean2D, dconic,
-                                                            dcolor, dopac, dmean3D, dcov3D, dsh, dscale, drot,
-                                                            consistent, nullptr);
+        preprocess_bwd_kernel<false><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, dmean2D, dconic, dopac,
+                                                            dmean3D, dcov3D, dscale, drot, consistent, nullptr, sh);
         if (sh)
-            sh_bwd_kernel<false><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dcolor, dmean3D, dsh);
+            sh_bwd_kernel<false><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dcolor, nullptr,
+                                                        dmean3D, dsh);
     }
-    note_launches(sh ? 2 : 1);
+    note_launches(sh ? 3 : 2);
 }
 
 }  // namespace fgs

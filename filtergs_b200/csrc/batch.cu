@@ -102,20 +102,6 @@ Layout plan(int P, int V, const fgs_view_args* views)
     return L;
 }
 
-__global__ void zero_visible_rows(const uint32_t* __restrict__ ids, const unsigned long long* __restrict__ count,
-                                  float* __restrict__ dmean2D, float* __restrict__ dconic, float* __restrict__ dopac,
-                                  float* __restrict__ dcolor)
-{
-    const uint32_t V = (uint32_t)*count;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < V; j += gridDim.x * blockDim.x) {
-        const uint32_t i = ids[j];
-        dmean2D[3 * i] = dmean2D[3 * i + 1] = dmean2D[3 * i + 2] = 0.f;
-        dconic[4 * i] = dconic[4 * i + 1] = dconic[4 * i + 2] = dconic[4 * i + 3] = 0.f;
-        dopac[i] = 0.f;
-        dcolor[3 * i] = dcolor[3 * i + 1] = dcolor[3 * i + 2] = 0.f;
-    }
-}
-
 int tile_bits_of(int num_tiles)
 {
     int bits = 1;
@@ -223,8 +209,8 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
         f.out_color = va.out_color; f.final_T = s.im.final_T; f.n_contrib = s.im.n_contrib;
         TileArgs bk = f;
         bk.out_color = nullptr;
-        bk.dL_dpix = va.dL_dout_color; bk.dmean2D = s.dmean2D; bk.dconic = s.dconic; bk.dopac = s.dopac;
-        bk.dcolor = s.dcolor;
+        bk.dL_dpix = va.dL_dout_color;
+        bk.pgrad = s.b.pgrad;
         fa[v] = f;
         ba[v] = bk;
         begin[v + 1] = begin[v] + (uint32_t)s.num_tiles;
@@ -304,7 +290,7 @@ int fgs_batch_forward(void* handle, void* stream)
                 launch_duplicate(v.g, v.b, (uint32_t)B->P, (uint32_t)v.cap, v.pre.W, v.pre.H, v.tile_bits, vs);
             }
             StageTimer t(FGS_STAGE_TILE_SORT, vs);
-            launch_tile_sort(v.g, v.b, v.cap, v.tile_bits, vs, v.g.total);
+            launch_tile_sort(v.g, v.b, v.cap, v.tile_bits, v.pre.W, v.pre.H, vs, v.g.total);
         }
         StageTimer t(FGS_STAGE_RANGES, vs);
         launch_ranges(v.b, v.im, v.cap, v.num_tiles, vs, v.g.total);
@@ -326,7 +312,7 @@ int fgs_batch_backward(void* handle, void* stream)
     const size_t P = (size_t)B->P;
     if (!B->g_means3D || !B->g_opacity) return FGS_ERR_ARG;
     {
-        // dense zeroing of the shared outputs and of the views' visible screen-space rows
+        // dense zeroing of the shared outputs
         StageTimer t(FGS_STAGE_PREPROCESS_BWD, s);
         cudaMemsetAsync(B->g_means3D, 0, sizeof(float) * 3 * P, s);
         cudaMemsetAsync(B->g_opacity, 0, sizeof(float) * P, s);
@@ -334,14 +320,6 @@ int fgs_batch_backward(void* handle, void* stream)
         if (B->g_sh && B->M > 0) cudaMemsetAsync(B->g_sh, 0, sizeof(float) * 3 * (size_t)B->M * P, s);
         if (B->g_scales) cudaMemsetAsync(B->g_scales, 0, sizeof(float) * 3 * P, s);
         if (B->g_rot) cudaMemsetAsync(B->g_rot, 0, sizeof(float) * 4 * P, s);
-        int dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        for (ViewState& v : B->views) {
-            zero_visible_rows<<<sms * 2, 256, 0, s>>>(v.g.sort_ids_b, v.g.total + 1, v.dmean2D, v.dconic, v.dopac,
-                                                      v.dcolor);
-            note_launches(1);
-        }
     }
     {
         StageTimer t(FGS_STAGE_RENDER_BWD, s);
@@ -350,9 +328,10 @@ int fgs_batch_backward(void* handle, void* stream)
     }
     StageTimer t(FGS_STAGE_PREPROCESS_BWD, s);
     for (ViewState& v : B->views) {
-        launch_preprocess_bwd(v.pre, nullptr, v.g, v.dmean2D, v.dconic, v.dcolor, v.dopac, B->g_means3D, B->g_cov3D,
-                              (v.pre.shs && B->g_sh) ? B->g_sh : nullptr, B->has_sr ? B->g_scales : nullptr,
-                              B->has_sr ? B->g_rot : nullptr, B->consistent, s, true, B->g_opacity);
+        launch_preprocess_bwd(v.pre, v.g, v.b.pgrad, v.dmean2D, v.dconic, v.dcolor, v.dopac, B->g_means3D,
+                              B->g_cov3D, (v.pre.shs && B->g_sh) ? B->g_sh : nullptr,
+                              B->has_sr ? B->g_scales : nullptr, B->has_sr ? B->g_rot : nullptr, B->consistent, s,
+                              true, B->g_opacity);
     }
     return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
 }

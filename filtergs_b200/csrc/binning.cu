@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(kSortThreads, 4)
                     const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ vals_out, uint32_t n, int shift,
                     int nbits, const uint32_t* __restrict__ pass_hist, uint32_t* status, uint32_t* chunk_counter,
                     unsigned* err, const PairRecord* __restrict__ grec, PairRecord* __restrict__ rec_out,
-                    const unsigned long long* __restrict__ n_dev)
+                    const unsigned long long* __restrict__ n_dev, const int2* __restrict__ erow, int gx)
 {
     __shared__ uint32_t s_hist[kSortWarps][kRadix];
     __shared__ uint32_t s_keys[kSortTile];
@@ -165,7 +165,19 @@ __global__ void __launch_bounds__(kSortThreads, 4)
             }
             if (keys_out) keys_out[gp] = k;
             vals_out[gp] = v;
-            if (rec_out) rec_out[gp] = grec[v];
+            if (rec_out) {
+                // The record also carries the pair's emission index: the Gaussian's first
+                // pair plus this tile's row-major place in its tile rectangle (the order in
+                // which duplicate_kernel emitted them), from the row base and width that
+                // duplicate_kernel left per Gaussian.  The backward writes the pair's
+                // gradients there, so each Gaussian's pairs are contiguous and are summed
+                // in a fixed order.
+                PairRecord r = grec[v];
+                const int2 er = __ldg(erow + v);
+                const uint32_t ty = k / (uint32_t)gx, tx = k - ty * (uint32_t)gx;
+                r.c.w = __uint_as_float((uint32_t)er.x + ty * (uint32_t)er.y + tx);
+                rec_out[gp] = r;
+            }
         }
         __syncthreads();  // shared buffers are reused by the next chunk
     }
@@ -202,7 +214,8 @@ __global__ void __launch_bounds__(256)
                      const PairRecord* __restrict__ grec, const int* __restrict__ radii, uint32_t V, int gx,
                      int gy, uint32_t* __restrict__ tile_out, uint32_t* __restrict__ val_out, uint32_t K,
                      uint32_t* status, uint32_t* chunk_counter, uint32_t* __restrict__ tile_hist, int tile_passes,
-                     const unsigned long long* __restrict__ V_dev, unsigned* err)
+                     const unsigned long long* __restrict__ V_dev, uint32_t* __restrict__ pair_off,
+                     int2* __restrict__ erow, unsigned* err)
 {
     __shared__ uint32_t s_hist[4][kRadix];
     __shared__ uint32_t s_warp[8];
@@ -237,6 +250,12 @@ __global__ void __launch_bounds__(256)
         }
         __syncthreads();
         const uint32_t off = s_prefix + local;
+        if (cnt) {
+            // first emitted pair, and the emission index of tile (tx, ty) as
+            // erow.x + ty * erow.y + tx (unsigned wrap-around)
+            pair_off[id] = off;
+            erow[id] = make_int2((int)(off - (uint32_t)y0 * (uint32_t)w - (uint32_t)x0), w);
+        }
         // warp-local exclusive prefix of cnt
         uint32_t wx = cnt;
 #pragma unroll
@@ -322,7 +341,7 @@ void launch_depth_sort(const GeomState& g, int P, cudaStream_t s)
     for (int pass = 0; pass < 4; pass++) {
         onesweep_kernel<<<grid, kSortThreads, 0, s>>>(kin[pass], kout[pass], vin[pass], vout[pass], n, 8 * pass, 8,
                                                      g.hist + pass * kRadix, g.status + (size_t)pass * nch * kRadix,
-                                                     g.counters + pass, g.err, nullptr, nullptr, V);
+                                                     g.counters + pass, g.err, nullptr, nullptr, V, nullptr, 1);
     }
 }
 
@@ -339,14 +358,16 @@ void launch_duplicate(const GeomState& g, const BinState& b, uint32_t V, uint32_
     const uint32_t grid = min(chunks_of(V, 256), resident_ctas(duplicate_kernel, 256));
     duplicate_kernel<<<grid, 256, 0, s>>>(g.sort_ids_b, g.tiles, g.grec, g.radii, V, gx, gy, tout,
                                                        vout, K, b.scan_status, g.counters + 8, g.hist + 4 * kRadix,
-                                                       passes, g.total + 1, g.err);
+                                                       passes, g.total + 1, g.pair_off, g.erow, g.err);
     note_launches(1);
 }
 
-void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int tile_bits, cudaStream_t s,
+void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int tile_bits, int W, int H, cudaStream_t s,
                       const unsigned long long* n_dev)
 {
     if (K <= 0) return;
+    const int gx = (W + kTileX - 1) / kTileX;  // tile ids are row-major over gx columns
+    (void)H;
     const uint32_t n = (uint32_t)K;
     const uint32_t nch = chunks_of(n, kSortTileMin);
     const uint32_t grid = min(nch, resident_ctas(onesweep_kernel, kSortThreads));
@@ -360,7 +381,8 @@ void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int ti
         uint32_t* vo = (vi == b.val_a) ? b.val_b : b.val_a;
         onesweep_kernel<<<grid, kSortThreads, 0, s>>>(ki, ko, vi, vo, n, 8 * pass, nbits, g.hist + (4 + pass) * kRadix,
                                                      b.status + (size_t)pass * nch * kRadix, g.counters + 4 + pass,
-                                                     g.err, last ? g.grec : nullptr, last ? b.rec : nullptr, n_dev);
+                                                     g.err, last ? g.grec : nullptr, last ? b.rec : nullptr, n_dev,
+                                                     g.erow, gx);
         ki = ko;
         vi = vo;
     }

@@ -50,6 +50,8 @@ GeomCarve carve_geom(void* base, int P)
     r.g.sort_ids_a = c.take<uint32_t>(P);
     r.g.sort_ids_b = c.take<uint32_t>(P);
     r.g.sort_keys_b = c.take<uint32_t>(P);
+    r.g.pair_off = r.g.sort_keys_b;
+    r.g.erow = c.take<int2>(P);
     r.g.cand_ids = c.take<uint32_t>(P);
     const size_t zero_off = c.off;
     r.g.hist = c.take<uint32_t>(8 * 256);
@@ -70,7 +72,7 @@ struct BinCarve {
     size_t total;
 };
 
-BinCarve carve_bin(void* base, long long K, int P)
+BinCarve carve_bin(void* base, long long K, int P, bool with_grad = true)
 {
     Carver c{static_cast<char*>(base)};
     BinCarve r{};
@@ -86,6 +88,7 @@ BinCarve carve_bin(void* base, long long K, int P)
     // Statistics reuse the sort's scratch buffers, dead once the last pass ran.
     r.b.kv_sum = reinterpret_cast<float*>(r.b.tile_a);
     r.b.kv_cnt = r.b.val_a;
+    r.b.pgrad = with_grad ? c.take<float>((size_t)9 * K) : nullptr;
     r.total = c.off;
     return r;
 }
@@ -291,6 +294,7 @@ size_t image_bytes(int W, int H)
 }
 BinState bin_views(void* base, long long K, int P) { return carve_bin(base, K, P).b; }
 size_t bin_bytes(long long K, int P) { return carve_bin(nullptr, K, P).total; }
+size_t bin_bytes_forward(long long K, int P) { return carve_bin(nullptr, K, P, false).total; }
 
 }  // namespace fgs
 
@@ -395,7 +399,7 @@ int fgs_forward_render(const fgs_raster_args* a, void* geom, void* image, void* 
             launch_duplicate(g, bc.b, (uint32_t)p.P, (uint32_t)K, W, H, tbits, s);
         }
         StageTimer t(FGS_STAGE_TILE_SORT, s);
-        launch_tile_sort(g, bc.b, K, tbits, s);
+        launch_tile_sort(g, bc.b, K, tbits, W, H, s);
     }
     {
         StageTimer t(FGS_STAGE_RANGES, s);
@@ -489,7 +493,7 @@ int fgs_backward(const fgs_raster_args* a, const void* geom, const void* image, 
     GeomState g = geom_views(const_cast<void*>(geom), p.P);
     ImageState im = image_views(const_cast<void*>(image), p.W, p.H);
     BinState b = bin_views(const_cast<void*>(binning), num_rendered, p.P);
-    const int* rad = radii ? radii : g.radii;
+    (void)radii;
     cudaMemsetAsync(dL_dmeans2D, 0, sizeof(float) * 3 * (size_t)p.P, s);
     cudaMemsetAsync(dL_dconic, 0, sizeof(float) * 4 * (size_t)p.P, s);
     cudaMemsetAsync(dL_dopacity, 0, sizeof(float) * (size_t)p.P, s);
@@ -502,12 +506,11 @@ int fgs_backward(const fgs_raster_args* a, const void* geom, const void* image, 
     const int consistent = backward_mode == FGS_BACKWARD_CONSISTENT;
     if (num_rendered > 0) {
         StageTimer t(FGS_STAGE_RENDER_BWD, s);
-        launch_render_bwd(p.W, p.H, im, b, a->background, dL_dout_color, dL_dmeans2D, dL_dconic, dL_dopacity,
-                          dL_dcolors, consistent, g.err, s);
+        launch_render_bwd(p.W, p.H, im, b, a->background, dL_dout_color, consistent, g.err, s);
     }
     {
         StageTimer t_pb(FGS_STAGE_PREPROCESS_BWD, s);
-        launch_preprocess_bwd(p, rad, g, dL_dmeans2D, dL_dconic, dL_dcolors, dL_dopacity, dL_dmeans3D, dL_dcov3D,
+        launch_preprocess_bwd(p, g, b.pgrad, dL_dmeans2D, dL_dconic, dL_dcolors, dL_dopacity, dL_dmeans3D, dL_dcov3D,
                               p.shs ? dL_dsh : nullptr, p.scales ? dL_dscales : nullptr,
                               p.scales ? dL_drotations : nullptr, consistent, s);
     }

@@ -151,6 +151,38 @@ __device__ __forceinline__ float3 ewa_cov2d(const float3& mean, float fx, float 
 __device__ __forceinline__ float dilate_max(float c) { return (float)fmax((double)c, 0.3); }
 __device__ __forceinline__ float dilate_add(float c) { return (float)((double)c + 0.3); }
 
+// Reduce 9 per-lane values over the warp with 16 shuffles instead of 45:
+// a butterfly in which each level halves the values a lane keeps (the rest
+// go to the partner lane).  Lanes 2s and 2s+1 end with the warp total of
+// value s (s < 9; padded to 16 slots).
+__device__ __forceinline__ float warp_transpose_sum9(const float (&g)[9])
+{
+    const unsigned lane = threadIdx.x & 31;
+    float v[8];
+    {
+        const bool hi = lane & 16;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const float lo_v = g[i];
+            const float hi_v = (i + 8 < 9) ? g[i + 8] : 0.f;
+            const float send = hi ? lo_v : hi_v;
+            const float keep = hi ? hi_v : lo_v;
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+    }
+#pragma unroll
+    for (int w = 4, o = 8; w >= 1; w >>= 1, o >>= 1) {
+        const bool hi = lane & o;
+#pragma unroll
+        for (int i = 0; i < w; i++) {
+            const float send = hi ? v[i] : v[i + w];
+            const float keep = hi ? v[i + w] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
 // ---------------------------------------------------------------- SH (forward.cu:48-99)
 __device__ constexpr float kSH_C0 = 0.28209479177387814f;
 __device__ constexpr float kSH_C1 = 0.4886025119029199f;

@@ -40,6 +40,9 @@ struct GeomState {
     uint32_t* sort_ids_a;      // [V] depth-sorted ids (ping)
     uint32_t* sort_ids_b;      // [V] visible ids in index order, then depth-sorted (pong)
     uint32_t* sort_keys_b;     // [P]
+    uint32_t* pair_off;        // [P] first emitted pair of each visible Gaussian (aliases sort_keys_b,
+                               //     dead once the depth sort is done)
+    int2* erow;                // [P] emission index of tile (tx, ty) = erow.x + ty * erow.y + tx
     uint32_t* hist;            // [8][256] radix histograms: 4 depth passes + up to 4 tile passes
     uint32_t* status;          // lookback status words, depth passes
     uint32_t* chunk_counts;    // [2][ceil(P/256)] preprocess chunk counts: visible (scanned in place), pairs
@@ -65,7 +68,8 @@ struct BinState {
     uint32_t* tile_b;   // [K]
     uint32_t* val_a;    // [K]
     uint32_t* val_b;    // [K] final point list
-    PairRecord* rec;    // [K]
+    PairRecord* rec;    // [K] (c.w: the pair's emission index)
+    float* pgrad;       // [K][9] per-pair gradients at the emission index (null in forward-only layouts)
     uint32_t* status;   // lookback words, tile passes
     uint32_t* scan_status; // lookback words of the fused scan
     float* kv_sum;      // [K] (stats)
@@ -74,6 +78,7 @@ struct BinState {
 };
 BinState bin_views(void* base, long long K, int P);
 size_t bin_bytes(long long K, int P);
+size_t bin_bytes_forward(long long K, int P);  // without the per-pair gradients
 
 // ---------------------------------------------------------------- launchers
 // Resident CTAs of a kernel on this device (persistent grids never exceed it).
@@ -98,7 +103,7 @@ void launch_duplicate(const GeomState& g, const BinState& b, uint32_t V, uint32_
                       cudaStream_t s);
 int sort_chunk_size();
 // K is the pair count, or the capacity when n_dev (device-side count) is given.
-void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int tile_bits, cudaStream_t s,
+void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int tile_bits, int W, int H, cudaStream_t s,
                       const unsigned long long* n_dev = nullptr);
 void launch_ranges(const BinState& b, const ImageState& im, long long K, int num_tiles, cudaStream_t s,
                    const unsigned long long* n_dev = nullptr);
@@ -106,12 +111,18 @@ void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, co
                        int* point_id, float* pw_pixel, float* point_weight, bool stats, unsigned* err,
                        cudaStream_t s);
 void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, const float* bg,
-                       const float* dL_dpix, float* dmean2D, float* dconic, float* dopac, float* dcolor,
-                       int consistent, unsigned* err, cudaStream_t s);
-void launch_preprocess_bwd(const PreParams& p, const int* radii, const GeomState& g, const float* dmean2D,
-                           const float* dconic, const float* dcolor, float* dopac, float* dmean3D,
-                           float* dcov3D, float* dsh, float* dscale, float* drot, int consistent,
-                           cudaStream_t s, bool accumulate = false, float* shared_dopac = nullptr);
+                       const float* dL_dpix, int consistent, unsigned* err, cudaStream_t s);
+// Per-Gaussian backward over the visible Gaussians.  Screen-space gradients come from
+// the per-pair gradients (pgrad, at the emission index), summed per Gaussian in
+// emission order.  Plain: dmean2D / dconic / dcolor / dopac are the dense
+// screen-space outputs (visible rows written; the caller zeroes them), the rest are
+// written densely.  accumulate: adds into shared dense buffers (views run one after
+// another on a stream); dcolor and dmean2D ([P,3]) are then this view's scratch and
+// dopac is not used (the opacity gradient goes to shared_dopac).
+void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* pgrad, float* dmean2D, float* dconic,
+                           float* dcolor, float* dopac, float* dmean3D, float* dcov3D, float* dsh, float* dscale,
+                           float* drot, int consistent, cudaStream_t s, bool accumulate = false,
+                           float* shared_dopac = nullptr);
 void launch_kpc_stats(const BinState& b, const ImageState& im, int num_tiles, float used_thresh, double* dev_out,
                       cudaStream_t s);
 
@@ -147,12 +158,9 @@ struct TileArgs {
     float* out_point_weight;
     float* kv_sum;
     uint32_t* kv_cnt;
-    // backward inputs / outputs
+    // backward input / output
     const float* dL_dpix;
-    float* dmean2D;
-    float* dconic;
-    float* dopac;
-    float* dcolor;
+    float* pgrad;  // [K][9] per-pair gradients, indexed by the record's emission index
 };
 
 // Persistent multi-view compositing over the tiles of `nviews` views; begin[v]

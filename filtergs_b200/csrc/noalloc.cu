@@ -108,7 +108,7 @@ int fgs_forward_noalloc(const fgs_raster_args* a, int* radii, float* out_color, 
     if (err) return first_error(err);
     if (tot[0] >= (1ull << 30)) return FGS_ERR_OVERFLOW;
     const long long K = (long long)tot[0];
-    const size_t bb = bin_bytes(K, p.P);
+    const size_t bb = bin_bytes_forward(K, p.P);
     if (gb + ib + bb > kNoAllocScratchBytes) return FGS_ERR_CAPACITY;
     BinState b = bin_views(base + gb + ib, K, p.P);
     const int gx = (p.W + kTileX - 1) / kTileX, gy = (p.H + kTileY - 1) / kTileY;
@@ -119,7 +119,7 @@ int fgs_forward_noalloc(const fgs_raster_args* a, int* radii, float* out_color, 
     if (K > 0) {
         cudaMemsetAsync(b.status, 0, sizeof(uint32_t) * (b.status_words + b.scan_words), s);
         launch_duplicate(g, b, (uint32_t)p.P, (uint32_t)K, p.W, p.H, tbits, s);
-        launch_tile_sort(g, b, K, tbits, s);
+        launch_tile_sort(g, b, K, tbits, p.W, p.H, s);
     }
     launch_ranges(b, im, K, num_tiles, s);
     launch_render_fwd(p.W, p.H, im, b, a->background, out_color, out_point_id, out_point_weight_pixel,

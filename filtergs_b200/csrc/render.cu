@@ -80,38 +80,6 @@ __device__ __forceinline__ void issue_batch(PairRecord* sbuf, uint64_t* bar, con
     bulk_g2s(sbuf, recs + first, bytes, bar);
 }
 
-// Reduce 9 per-lane values over the warp with 16 shuffles instead of 45:
-// a butterfly in which each level halves the values a lane keeps (the rest
-// go to the partner lane).  Lanes 2s and 2s+1 end with the warp total of
-// value s (s < 9; padded to 16 slots).
-__device__ __forceinline__ float warp_transpose_sum9(const float (&g)[9])
-{
-    const unsigned lane = threadIdx.x & 31;
-    float v[8];
-    {
-        const bool hi = lane & 16;
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const float lo_v = g[i];
-            const float hi_v = (i + 8 < 9) ? g[i + 8] : 0.f;
-            const float send = hi ? lo_v : hi_v;
-            const float keep = hi ? hi_v : lo_v;
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-        }
-    }
-#pragma unroll
-    for (int w = 4, o = 8; w >= 1; w >>= 1, o >>= 1) {
-        const bool hi = lane & o;
-#pragma unroll
-        for (int i = 0; i < w; i++) {
-            const float send = hi ? v[i] : v[i + w];
-            const float keep = hi ? v[i + w] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
-        }
-    }
-    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
-}
-
 __device__ __forceinline__ float warp_sum(float v)
 {
 #pragma unroll
@@ -168,11 +136,19 @@ struct FwdSmem {
     uint32_t kcnt[2][kBatch];
 };
 
-template <int kBatch>
+// Per-record gradient sums of a batch: warps 2s and 2s+1 add their warp totals
+// into slot s.  A slot starts at zero and takes at most two additions, and
+// float addition is commutative, so its value does not depend on which warp
+// came first; the slots are then summed in slot order.  The result is the same
+// on every run (no order-dependent float atomics anywhere in the backward).
+template <int PPT>
+constexpr int bwd_slots() { return (256 / PPT / 32) / 2 > 0 ? (256 / PPT / 32) / 2 : 1; }
+
+template <int kBatch, int kSlots>
 struct BwdSmem {
     PairRecord rec[kBufs][kBatch];
     uint64_t bar[kBufs];
-    float acc[9][kBatch];
+    float acc[kSlots][9][kBatch];
     uint32_t max_last;
 };
 
@@ -421,9 +397,10 @@ __global__ void __launch_bounds__(256 / PPT)
 
 // ---------------------------------------------------------------- backward
 template <int PPT, int kBatch>
-__device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch>& sm, const TileArgs& a, int tile, uint32_t& gb,
-                                                int consistent, unsigned* err)
+__device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()>& sm, const TileArgs& a, int tile,
+                                                uint32_t& gb, int consistent, unsigned* err)
 {
+    constexpr int kSlots = bwd_slots<PPT>();
     constexpr int NT = 256 / PPT;
     constexpr int NG = 9;  // dcolor r,g,b ; dmean2D x,y ; dconic x,y,w ; dopacity
     const int tid = threadIdx.x;
@@ -554,28 +531,24 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch>& sm, const TileA
                 if (__any_sync(0xffffffffu, any)) {
                     const float tot = warp_transpose_sum9(gr);
                     const unsigned lane = tid & 31;
-                    if (!(lane & 1) && (lane >> 1) < NG) atomicAdd(&sm.acc[lane >> 1][j], tot);
+                    if (!(lane & 1) && (lane >> 1) < NG) atomicAdd(&sm.acc[(tid >> 5) >> 1][lane >> 1][j], tot);
                 }
             }
         }
         __syncthreads();
+        // this batch's per-pair gradients, at each pair's emission index
         for (uint32_t e = tid; e < cnt; e += NT) {
-            const int id = __float_as_int(R[e].c.y);
-            float v[NG];
+            float* dst = a.pgrad + (size_t)__float_as_uint(R[e].c.w) * NG;
 #pragma unroll
             for (int q = 0; q < NG; q++) {
-                v[q] = sm.acc[q][e];
-                sm.acc[q][e] = 0.f;
+                float v = 0.f;
+#pragma unroll
+                for (int sl = 0; sl < kSlots; sl++) {
+                    v += sm.acc[sl][q][e];
+                    sm.acc[sl][q][e] = 0.f;
+                }
+                dst[q] = v;
             }
-            if (v[0] != 0.f) atomicAdd(a.dcolor + 3 * id, v[0]);
-            if (v[1] != 0.f) atomicAdd(a.dcolor + 3 * id + 1, v[1]);
-            if (v[2] != 0.f) atomicAdd(a.dcolor + 3 * id + 2, v[2]);
-            if (v[3] != 0.f) atomicAdd(a.dmean2D + 3 * id, v[3]);
-            if (v[4] != 0.f) atomicAdd(a.dmean2D + 3 * id + 1, v[4]);
-            if (v[5] != 0.f) atomicAdd(a.dconic + 4 * id, v[5]);
-            if (v[6] != 0.f) atomicAdd(a.dconic + 4 * id + 1, v[6]);
-            if (v[7] != 0.f) atomicAdd(a.dconic + 4 * id + 3, v[7]);
-            if (v[8] != 0.f) atomicAdd(a.dopac + id, v[8]);
         }
         if (tid == 0 && b + 2 < nb) {
             const int nbuf = (int)((g + 2) % kBufs);
@@ -585,12 +558,18 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch>& sm, const TileA
         __syncthreads();
     }
     gb += (uint32_t)nb;
+    // pairs at or past the tile's largest n_contrib touch no pixel: zero gradients
+    for (uint32_t e = n + tid; e < range.y - range.x; e += NT) {
+        float* dst = a.pgrad + (size_t)__float_as_uint(recs[range.x + e].c.w) * NG;
+#pragma unroll
+        for (int q = 0; q < NG; q++) dst[q] = 0.f;
+    }
 }
 
-template <int kBatch>
-__device__ __forceinline__ void bwd_smem_init(BwdSmem<kBatch>& sm, int NT)
+template <int kBatch, int kSlots>
+__device__ __forceinline__ void bwd_smem_init(BwdSmem<kBatch, kSlots>& sm, int NT)
 {
-    for (int e = threadIdx.x; e < 9 * kBatch; e += NT) (&sm.acc[0][0])[e] = 0.f;
+    for (int e = threadIdx.x; e < kSlots * 9 * kBatch; e += NT) (&sm.acc[0][0][0])[e] = 0.f;
     if (threadIdx.x == 0) {
         for (int i = 0; i < kBufs; i++) mbar_init(&sm.bar[i], 1);
         mbar_fence_init();
@@ -598,10 +577,16 @@ __device__ __forceinline__ void bwd_smem_init(BwdSmem<kBatch>& sm, int NT)
     __syncthreads();
 }
 
+// The backward's shared state can pass the 48 KB static limit (8 warps, 256-record
+// batches): it lives in dynamic shared memory.
+template <int PPT, int kBatch>
+using BwdSmemT = BwdSmem<kBatch, bwd_slots<PPT>()>;
+
 template <int PPT, int kBatch>
 __global__ void __launch_bounds__(256 / PPT) render_bwd_kernel(TileArgs a, int consistent, unsigned* err)
 {
-    __shared__ __align__(128) BwdSmem<kBatch> sm;
+    extern __shared__ __align__(128) unsigned char bwd_dyn[];
+    BwdSmemT<PPT, kBatch>& sm = *reinterpret_cast<BwdSmemT<PPT, kBatch>*>(bwd_dyn);
     bwd_smem_init(sm, 256 / PPT);
     uint32_t gb = 0;
     render_bwd_tile<PPT, kBatch>(sm, a, blockIdx.x, gb, consistent, err);
@@ -612,7 +597,8 @@ __global__ void __launch_bounds__(256 / PPT)
     render_bwd_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin, int nviews,
                             uint32_t total, uint32_t* queue, int consistent, unsigned* err)
 {
-    __shared__ __align__(128) BwdSmem<kBatch> sm;
+    extern __shared__ __align__(128) unsigned char bwd_dyn[];
+    BwdSmemT<PPT, kBatch>& sm = *reinterpret_cast<BwdSmemT<PPT, kBatch>*>(bwd_dyn);
     __shared__ uint32_t s_item;
     bwd_smem_init(sm, 256 / PPT);
     uint32_t gb = 0;
@@ -646,16 +632,32 @@ void fwd_launch(int grid, const ImageState& im, const BinState& b, int W, int H,
     render_fwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(a, err);
 }
 
+// Dynamic shared memory of a backward kernel instantiation (opted in once per process
+// and device ordinal; Tag tells the single-view and multi-view kernels apart).
+template <int PPT, int B, int Tag, typename Kern>
+size_t bwd_smem_bytes(Kern k)
+{
+    static bool done[64] = {};
+    const size_t bytes = sizeof(BwdSmemT<PPT, B>);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !done[dev]) {
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (dev >= 0 && dev < 64) done[dev] = true;
+    }
+    return bytes;
+}
+
 template <int PPT, int B>
 void bwd_launch(int grid, const ImageState& im, const BinState& b, int W, int H, const float* bg, const float* dL,
-                float* dmean2D, float* dconic, float* dopac, float* dcolor, int consistent, unsigned* err,
-                cudaStream_t s)
+                int consistent, unsigned* err, cudaStream_t s)
 {
     TileArgs a{};
     a.ranges = im.ranges; a.recs = b.rec; a.W = W; a.H = H; a.bg = bg;
     a.final_T = im.final_T; a.n_contrib = im.n_contrib;
-    a.dL_dpix = dL; a.dmean2D = dmean2D; a.dconic = dconic; a.dopac = dopac; a.dcolor = dcolor;
-    render_bwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(a, consistent, err);
+    a.dL_dpix = dL; a.pgrad = b.pgrad;
+    const size_t smem = bwd_smem_bytes<PPT, B, 0>(render_bwd_kernel<PPT, B>);
+    render_bwd_kernel<PPT, B><<<grid, 256 / PPT, smem, s>>>(a, consistent, err);
 }
 
 #define FGS_RENDER_DISPATCH(FN, PPT_, B_, ...)                                            \
@@ -713,9 +715,11 @@ void bwd_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, 
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_bwd_multi_kernel<PPT, B>, 256 / PPT, 0);
+    const size_t smem = bwd_smem_bytes<PPT, B, 1>(render_bwd_multi_kernel<PPT, B>);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_bwd_multi_kernel<PPT, B>, 256 / PPT, smem);
     const int grid = sms * (per_sm > 0 ? per_sm : 1);
-    render_bwd_multi_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(views, begin, nviews, total, queue, consistent, err);
+    render_bwd_multi_kernel<PPT, B><<<grid, 256 / PPT, smem, s>>>(views, begin, nviews, total, queue, consistent,
+                                                                  err);
 }
 }  // namespace
 
@@ -739,13 +743,11 @@ void launch_render_bwd_multi(const TileArgs* views, const uint32_t* begin, int n
 }
 
 void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, const float* bg,
-                       const float* dL_dpix, float* dmean2D, float* dconic, float* dopac, float* dcolor,
-                       int consistent, unsigned* err, cudaStream_t s)
+                       const float* dL_dpix, int consistent, unsigned* err, cudaStream_t s)
 {
     const int gx = (W + kTileX - 1) / kTileX, gy = (H + kTileY - 1) / kTileY;
     const RenderConfig c = g_cfg;
-    FGS_RENDER_DISPATCH(bwd_launch, c.bwd_ppt, c.bwd_batch, gx * gy, im, b, W, H, bg, dL_dpix, dmean2D, dconic, dopac,
-                        dcolor, consistent, err, s);
+    FGS_RENDER_DISPATCH(bwd_launch, c.bwd_ppt, c.bwd_batch, gx * gy, im, b, W, H, bg, dL_dpix, consistent, err, s);
     note_launches(1);
 }
 

@@ -80,6 +80,20 @@ def test_backward_vs_reference(cuda, ref, name):
         assert norm_rel(a, b) <= GRAD_TOL, (n, norm_rel(a, b))
 
 
+def test_backward_is_deterministic(cuda):
+    """Two backward passes over the same forward give bit-identical gradients: per-pair
+    gradients are written once at their emission index and summed per Gaussian in a fixed
+    order, so no float atomic decides a rounding."""
+    case = small_case(P=20000, seed=1030, W=320, H=240)
+    g = torch.Generator().manual_seed(9)
+    dL = torch.randn(3, case.cam.H, case.cam.W, generator=g).cuda()
+    fwd = run_forward(ours, case)
+    a = run_backward(ours, case, fwd, dL)
+    b = run_backward(ours, case, fwd, dL)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+
+
 def test_forward_vs_oracle(cuda):
     case = small_case()
     mine = run_forward(ours, case)
