@@ -63,6 +63,8 @@ def parse(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-resolution workload")
+    ap.add_argument("--no-lod", action="store_true", help="skip the LoD-tree filter + render workload")
+    ap.add_argument("--lod-nodes", type=int, default=8_000_000)
     ap.add_argument("--no-autotune", action="store_true", help="keep the default render kernel shape")
     ap.add_argument("--render-config", default=None,
                     help="fwd_ppt,fwd_batch,bwd_ppt,bwd_batch (skips the autotuner)")
@@ -195,24 +197,26 @@ def make_batched(scene, views, bg):
     return br
 
 
-# algorithmic bytes per launch (per view) for each stage; K pairs, V visible, P Gaussians, N pixels
-def algo_bytes(stage, P, V, K, N, T, M=16):
+# algorithmic bytes per launch (per view) for each stage; K pairs, V visible, P Gaussians, N pixels, T tiles
+def algo_bytes(stage, P, V, K, N, T, M=16, tile_passes=2):
     if stage == "preprocess":
-        return 44 * P + 4 * M * 3 * V + 56 * V + 4 * P
+        # means/scales/rotations/opacity of every Gaussian, SH rows of the visible ones; radii, tiles (and the
+        # caller's radii) for all, the 48-byte record and clamp bits for the visible, compacted ids and keys
+        return 44 * P + 4 * M * 3 * V + 12 * P + 49 * V + 8 * V
+    if stage == "depth_sort":
+        return 4 * 16 * V + 4 * V          # 4 passes of keys + ids in and out, one histogram read
     if stage == "duplicate":
-        return 8 * P + 12 * K
+        return 28 * V + 12 * V + 8 * K     # ids, tiles, record xy, radius in; pair offsets out; tile + id per pair
     if stage == "tile_sort":
-        return 24 * K * 2
+        return 16 * K * tile_passes + 104 * K   # keys + ids per pass; last pass gathers 48-byte records
     if stage == "ranges":
         return 8 * K + 8 * T
     if stage == "render_fwd":
         return 40 * K + 28 * N
     if stage == "render_bwd":
-        return 40 * K + 20 * N + 44 * V
+        return 76 * K + 20 * N  # records 40 B + per-pair gradient row 36 B; dL/dpix, T, n_contrib
     if stage == "preprocess_bwd":
-        return V * (12 + 24 + 16 + 12 + 12 + 16 + 12 + 3 + 192) + P * 284
-    if stage == "depth_sort":
-        return 4 * 16 * P
+        return 36 * K + V * (12 + 24 + 16 + 12 + 12 + 16 + 12 + 3 + 192) + P * 284
     return 0
 
 
@@ -226,14 +230,15 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(stage):
-    """dram bytes per launch for `stage` from the committed ncu summary (None if absent)."""
+def ncu_traffic(key, pairs):
+    """DRAM bytes of one launch of `key` from the committed ncu summary: per-pair traffic x pairs
+    (None if the summary has no figure for it)."""
     p = os.path.join(ROOT, "profiles", "traffic_urban1080.md")
     try:
         with open(p) as f:
             for ln in f:
-                if ln.startswith("traffic_per_launch[") and ln.split("[")[1].split("]")[0] == stage:
-                    return float(ln.split("=")[1].strip().split()[0])
+                if ln.startswith("traffic_per_pair[") and ln.split("[")[1].split("]")[0] == key:
+                    return float(ln.split("=")[1].strip().split()[0]) * pairs
     except OSError:
         pass
     return None
@@ -407,14 +412,14 @@ def roofline(prof, P, views, K, vis, batched):
 
     if batched and dom in ("render_fwd", "render_bwd"):
         ab = sum(bytes_of(dom, v, K[v], vis[v]) for v in range(len(views)))   # one launch covers all views
-        key = "batched." + dom
+        key, pairs = "batched." + dom, float(sum(K))
     else:
         ab = float(np.mean([bytes_of(dom, v, K[v], vis[v]) for v in range(len(views))]))
-        key = ("batched." if batched else "") + dom
+        key, pairs = ("batched." if batched else "") + dom, float(np.mean(K))
     peak, kind = measured_peak()
     achieved = ab / (per_call_ms / 1000.0) / 1e9
     return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": ncu_traffic(key), "algorithmic_bytes_per_launch": ab,
+            "frac": achieved / peak, "traffic": ncu_traffic(key, pairs), "algorithmic_bytes_per_launch": ab,
             "launch_ms": per_call_ms, "peak_source": f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured"
             else "fallback 6650 GB/s",
             "timing": "CUDA events around each launch, eager pass of the same K steps" if batched
@@ -425,6 +430,104 @@ def roofline(prof, P, views, K, vis, batched):
 def stages_of(prof):
     return {k: {"ms_total": v[0], "launch_groups": v[1], "ms_per_call": (v[0] / v[1]) if v[1] else 0.0}
             for k, v in prof.items() if v[1]}
+
+
+# ---------------------------------------------------------------- LoD tree: filter + render (forward)
+def make_lod(args, dev):
+    """8M-node Gaussian tree (branching min(Poisson(3)+1, 8), depth <= 12, child scale x0.5) centred in the
+    urban area, and a 1920x1080 camera at 150 m altitude, 45 deg pitch, looking at the tree's centre."""
+    from filtergs_b200 import lod, synthetic as S
+    tr = S.lod_tree(P=args.lod_nodes, seed=1002, roots=2, max_depth=12, half_extent=500.0)
+    c = tr["xyz"][tr["roots"]].mean(0)
+    c[2] = 0.0
+    cam = S.look_at_camera(c + np.array([150.0, 0.0, 150.0]), c, W=1920, H=1080, fx=1600.0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    return tr, lod.TreeScene.from_arrays(tr, device=dev), cam, t(cam.viewmatrix), t(cam.projmatrix), t(cam.campos)
+
+
+def measure_lod(args, dev, impl):
+    """Views/s of per-view LoD selection + forward render.  Ours: the FilterGS rule (visibility kernel,
+    ordered compaction, fused gather/activation, rasterizer) and the LoG cut rule (device traversal +
+    culling).  Reference: its visibility kernel, torch.nonzero, torch activations, its rasterizer."""
+    from filtergs_b200 import lod
+    tr, scene, cam, view, proj, cpos = make_lod(args, dev)
+    bg = torch.zeros(3, device=dev)
+    steps = max(3, args.steps // 2)
+    out = {"nodes": int(scene.P), "unit": "views/s", "width": cam.W, "height": cam.H,
+           "rules": {"filtergs": "radius_max 1.5 px, padding 0.1, threshold 700",
+                     "logcut": "min_resolution 1.5 px, cull < 1 px or opacity < 1/255"}}
+    if impl == "ours":
+        def filtergs(_):
+            idx, cnt, *_r = lod.select_filtergs(scene, view, proj, cam, 1.5, 0.1, 700.0)
+            return lod.render_selected(scene, idx, cnt, view, proj, cpos, cam, bg, stats=False), cnt
+
+        def logcut(_):
+            idx, cnt = lod.select_logcut(scene, view, proj, cam, 1.5, 1.0)
+            return lod.render_selected(scene, idx, cnt, view, proj, cpos, cam, bg, stats=False), cnt
+
+        for name, fn in (("filtergs", filtergs), ("logcut", logcut)):
+            for i in range(3):
+                r, cnt = fn(i)
+            ms, _ = timed(fn, steps)
+            out[name] = {"value": steps / (ms / 1000.0), "selected": int(cnt.item()), "pairs_K": int(r[0])}
+    else:
+        from oracle import build_ref
+        ref, v2 = build_ref.load("ref_rasterizer_C"), build_ref.load("ref_compute_radius_v2")
+        if ref is None or v2 is None:
+            return {"unavailable": "reference build oracle/_ref missing"}
+        fx, fy = cam.W / (2 * cam.tanfovx), cam.H / (2 * cam.tanfovy)
+        e = torch.Tensor([])
+        C0, C1 = 0.28209479177387814, 0.4886025119029199
+
+        def filtergs(_):
+            m, _r, _d = v2.compute_visibility_radius(scene.xyz, scene.log_scales, scene.rotations, proj, view,
+                                                     scene.node_index, scene.ancestor_path, fx, fy, cam.tanfovx,
+                                                     cam.tanfovy, 0.1, 1.5, 700.0)
+            ri = torch.nonzero(m, as_tuple=True)[0]
+            xyz = scene.xyz[ri]
+            d = xyz - cpos[None]
+            d = d / torch.norm(d, dim=-1, keepdim=True)
+            rest = scene.shs_rest[ri]
+            col = scene.features_dc[ri] * C0 + 0.5 + (-C1 * d[:, 1:2] * rest[:, 0] + C1 * d[:, 2:3] * rest[:, 1] -
+                                                      C1 * d[:, 0:1] * rest[:, 2])
+            r = ref.rasterize_gaussians(bg, xyz, col, torch.sigmoid(scene.opacity_raw[ri])[:, None],
+                                        torch.exp(scene.log_scales[ri]),
+                                        torch.nn.functional.normalize(scene.rotations[ri]), 1.0, e, view, proj,
+                                        cam.tanfovx, cam.tanfovy, cam.H, cam.W, e, 0, cpos, False, True, False, 0.2,
+                                        0.2, 0.05, 0.7, False)
+            return r, ri.numel()
+
+        for i in range(3):
+            r, n = filtergs(i)
+        ms, _ = timed(filtergs, steps)
+        out["filtergs"] = {"value": steps / (ms / 1000.0), "selected": int(n), "pairs_K": int(r[0])}
+    del scene
+    torch.cuda.empty_cache()
+    return out
+
+
+def fp64_image_error(mod, dev):
+    """Part of the CPU-baseline leg: the FP32 CUDA image of the CPU-runnable scene (10,000 Gaussians,
+    256x256, SH 3, identity camera) against an FP64 evaluation of the same splat equations by the CPU
+    port (it differs from the CUDA path only in precision)."""
+    from oracle import oracle as O
+    from filtergs_b200 import synthetic as S
+    sc, cam = S.small_scene(P=10000, seed=1000)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    bg = torch.zeros(3, device=dev)
+    e = torch.empty(0, device=dev)
+    out = mod.rasterize_gaussians(bg, t(sc["means3D"]), e, t(sc["opacities"]), t(sc["scales"]), t(sc["rotations"]),
+                                  1.0, e, t(cam.viewmatrix), t(cam.projmatrix), cam.tanfovx, cam.tanfovy, cam.H, cam.W,
+                                  t(sc["shs"]), 3, t(cam.campos), False, True, False, 0.2, 0.2, 0.05, 0.7, False)
+    img = out[1].cpu().numpy().astype(np.float64)
+    f64 = lambda a: np.asarray(a, np.float64)  # noqa: E731
+    s64 = O.Scene(f64(sc["means3D"]), f64(sc["opacities"]), cam.W, cam.H, cam.tanfovx, cam.tanfovy,
+                  f64(cam.viewmatrix).reshape(-1), f64(cam.projmatrix).reshape(-1), f64(cam.campos),
+                  shs=f64(sc["shs"]), sh_degree=3, scales=f64(sc["scales"]), rotations=f64(sc["rotations"]))
+    ref = O.forward(s64, dtype=np.float64)["color"]
+    d = np.abs(img - ref)
+    return {"max_abs": float(d.max()), "mean_abs": float(d.mean()),
+            "workload": "10,000 Gaussians SH3, 256x256 (CPU-runnable scene), FP32 CUDA vs FP64 CPU port"}
 
 
 def main():
@@ -501,6 +604,9 @@ def main():
                  "plain_value": n_ranks * nv * args.steps / (mp["ms"] / 1000.0),
                  "unit": "views/s", "batched_render_config": mb["tuned"], "plain_render_config": mp["tuned"],
                  "pairs_K": mb["K"], "visible_V": mb["vis"], "altitude_m": "80-300", "pitch_deg": "30-75"}
+    lod_res = None
+    if not args.no_lod and rank == 0:
+        lod_res = measure_lod(args, dev, args.impl)
     if clocks:
         clocks.stop()
 
@@ -540,6 +646,9 @@ def main():
                 res["e2e"] = e2e
             if not args.no_cpu_baseline:
                 res["cpu_baseline"] = cpu_baseline(sc, views[0]["cam"], os.cpu_count() or 1)
+                res["cpu_baseline"]["fp64_image_error"] = fp64_image_error(mod, dev)
+        if lod_res:
+            res["lod_tree"] = lod_res
         if head["clocks"]:
             res["clocks"] = head["clocks"]
         print(json.dumps(res), flush=True)
