@@ -40,6 +40,16 @@ class RasterArgs(C.Structure):
     ]
 
 
+class AdamArgs(C.Structure):
+    """Mirror of struct fgs_adam_args."""
+    _fields_ = [("P", i32), ("M", i32), ("lr", f32 * 5), ("beta1", C.c_double), ("beta2", C.c_double),
+                ("eps", f32)] + [
+        (n, vp) for n in ("xyz", "shs", "opac_logit", "log_scale", "rot_raw", "opac", "scale", "rot",
+                          "g_xyz", "g_shs", "g_opac", "g_scale", "g_rot",
+                          "m_xyz", "m_shs", "m_opac", "m_scale", "m_rot",
+                          "v_xyz", "v_shs", "v_opac", "v_scale", "v_rot")]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "fgs_status_string": (C.c_char_p, [i32]),
@@ -81,6 +91,12 @@ SIGNATURES = {
     "fgs_batch_pair_counts": (i32, [vp, vp, vp]),
     "fgs_batch_check": (i32, [vp, vp]),
     "fgs_batch_destroy": (None, [vp]),
+    "fgs_batch_set_densify": (i32, [vp, vp, vp, vp]),
+    "fgs_loss_scratch_bytes": (sz, [i32, i32]),
+    "fgs_loss_l1_ssim": (i32, [i32, i32, vp, vp, vp, f32, f32, vp, vp, vp]),
+    "fgs_train_activate": (i32, [i32, vp, vp, vp, vp, vp, vp, vp]),
+    "fgs_densify_dense": (i32, [i32, vp, vp, vp, vp, vp, vp]),
+    "fgs_adam_step": (i32, [C.POINTER(AdamArgs), vp, vp, vp]),
     "fgs_get_render_config": (i32, [vp]),
     "fgs_forward_noalloc": (i32, [C.POINTER(RasterArgs), vp, vp, vp, vp, vp, C.POINTER(i64), vp]),
 }

@@ -159,7 +159,8 @@ __global__ void __launch_bounds__(256)
     pair_grad_gather_kernel(const uint32_t* __restrict__ visible_ids, const unsigned long long* __restrict__ visible_count,
                             const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ pair_off,
                             const float* __restrict__ pgrad, float* __restrict__ dmean2D, float* __restrict__ dconic,
-                            float* __restrict__ dcolor, float* __restrict__ dopac)
+                            float* __restrict__ dcolor, float* __restrict__ dopac, float* __restrict__ dens_grad,
+                            int* __restrict__ dens_count, uint8_t* __restrict__ dens_flag)
 {
     const uint32_t V = (uint32_t)*visible_count;
     const int lane = threadIdx.x & 31;
@@ -180,6 +181,15 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
             for (int u = 0; u < 4; u++)
                 if (k + 32 * u < ne) acc += warp_transpose_sum9(v[u]);
+        }
+        if (dens_grad) {
+            // densification statistics (LoG/model/counter.py): |dL/dmean2D[:2]| and visibility
+            const float gx = __shfl_sync(0xffffffffu, acc, 6), gy = __shfl_sync(0xffffffffu, acc, 8);
+            if (lane == 0) {
+                dens_grad[idx] += sqrtf(gx * gx + gy * gy);
+                dens_count[idx] += 1;
+                dens_flag[idx] = 1;
+            }
         }
         if (lane < 18 && !(lane & 1)) {
             const int q = lane >> 1;
@@ -435,7 +445,8 @@ __global__ void __launch_bounds__(256, 3)
 
 void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* pgrad, float* dmean2D, float* dconic,
                            float* dcolor, float* dopac, float* dmean3D, float* dcov3D, float* dsh, float* dscale,
-                           float* drot, int consistent, cudaStream_t s, bool accumulate, float* shared_dopac)
+                           float* drot, int consistent, cudaStream_t s, bool accumulate, float* shared_dopac,
+                           const DensifyStats* dens)
 {
     if (p.P <= 0) return;
     const size_t P = (size_t)p.P;
@@ -453,7 +464,8 @@ void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* 
     const int blocks = (int)std::min<size_t>((P + 255) / 256, (size_t)sms * 8);
     const bool sh = p.shs && dsh;
     pair_grad_gather_kernel<<<blocks, 256, 0, s>>>(g.sort_ids_b, g.total + 1, g.tiles, g.pair_off, pgrad, dmean2D,
-                                                   dconic, dcolor, dopac);
+                                                   dconic, dcolor, dopac, dens ? dens->grad_sum : nullptr,
+                                                   dens ? dens->count : nullptr, dens ? dens->flag : nullptr);
     if (accumulate) {
         preprocess_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, dmean2D, dconic, dopac,
                                                            dmean3D, dcov3D, dscale, drot, consistent, shared_dopac, sh);

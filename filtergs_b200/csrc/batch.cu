@@ -66,6 +66,7 @@ struct Batch {
     uint32_t total_tiles;
     const float* background;
     float *g_means3D, *g_opacity, *g_sh, *g_scales, *g_rot, *g_cov3D;
+    DensifyStats dens{nullptr, nullptr, nullptr};  // optional (fgs_batch_set_densify)
     int M;
     bool has_sr;
 };
@@ -331,9 +332,19 @@ int fgs_batch_backward(void* handle, void* stream)
         launch_preprocess_bwd(v.pre, v.g, v.b.pgrad, v.dmean2D, v.dconic, v.dcolor, v.dopac, B->g_means3D,
                               B->g_cov3D, (v.pre.shs && B->g_sh) ? B->g_sh : nullptr,
                               B->has_sr ? B->g_scales : nullptr, B->has_sr ? B->g_rot : nullptr, B->consistent, s,
-                              true, B->g_opacity);
+                              true, B->g_opacity, B->dens.grad_sum ? &B->dens : nullptr);
     }
     return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
+}
+
+int fgs_batch_set_densify(void* handle, float* grad_sum, int* vis_count, unsigned char* flag)
+{
+    Batch* B = static_cast<Batch*>(handle);
+    if (!B) return FGS_ERR_ARG;
+    if ((grad_sum == nullptr) != (vis_count == nullptr) || (grad_sum == nullptr) != (flag == nullptr))
+        return FGS_ERR_ARG;
+    B->dens = DensifyStats{grad_sum, vis_count, flag};
+    return FGS_OK;
 }
 
 int fgs_batch_pair_counts(void* handle, long long* counts, void* stream)

@@ -119,10 +119,16 @@ void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, co
 // written densely.  accumulate: adds into shared dense buffers (views run one after
 // another on a stream); dcolor and dmean2D ([P,3]) are then this view's scratch and
 // dopac is not used (the opacity gradient goes to shared_dopac).
+// Densification statistics a training step keeps per Gaussian (null pointers: off).
+struct DensifyStats {
+    float* grad_sum;   // += |dL/dmean2D[:2]| per view that sees the Gaussian
+    int* count;        // += 1 per such view
+    uint8_t* flag;     // = 1 (visible in this step)
+};
 void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* pgrad, float* dmean2D, float* dconic,
                            float* dcolor, float* dopac, float* dmean3D, float* dcov3D, float* dsh, float* dscale,
                            float* drot, int consistent, cudaStream_t s, bool accumulate = false,
-                           float* shared_dopac = nullptr);
+                           float* shared_dopac = nullptr, const DensifyStats* dens = nullptr);
 void launch_kpc_stats(const BinState& b, const ImageState& im, int num_tiles, float used_thresh, double* dev_out,
                       cudaStream_t s);
 

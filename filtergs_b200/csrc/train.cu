@@ -1,0 +1,417 @@
+// Training-step kernels around the rasterizer (the loss, the optimizer and the
+// densification statistics of LoG's training loop):
+//
+//   loss       LoG/render/loss.py:6-44 (SSIM, 11x11 Gaussian window, sigma 1.5,
+//              no padding: "valid" outputs) and renderer.py:260-273
+//              (0.8 * L1 + 0.2 * (1 - SSIM)), forward and gradient in two tiled
+//              kernels per image channel, partial sums reduced in a fixed order.
+//   activate   LoG/model/activation.py (exp scale, sigmoid opacity, normalised
+//              quaternion) from the raw parameters.
+//   adam       LoG/model/sparse_optimizer.py:41-78,163-196: Adam with bias
+//              correction from the global step, eps 1e-15, on the rows that were
+//              visible this step only; the gradients w.r.t. the activated values
+//              are chained through the activations first, and the activated values
+//              of the updated rows are rewritten for the next forward.
+//   densify    LoG/model/counter.py:36-83 (reduced to the two statistics the
+//              training step keeps): sum of |dL/dmean2D[:, :2]| and the visibility
+//              count per Gaussian, plus this step's visible flag.
+#include <cmath>
+
+#include "fgs_common.cuh"
+#include "fgs_internal.h"
+
+namespace fgs {
+
+namespace {
+
+constexpr int kWin = 11;           // SSIM window
+constexpr int kHalo = kWin - 1;    // valid outputs lose kHalo rows / columns
+constexpr int kTX = 32, kTY = 16;  // output (or pixel) tile of one CTA
+constexpr float kC1 = 0.01f * 0.01f, kC2 = 0.03f * 0.03f;
+
+struct Window {
+    float g[kWin];
+};
+
+// ---------------------------------------------------------------- SSIM forward + coefficient maps
+// One CTA: a kTX x kTY tile of valid outputs of one channel.  The input tile with
+// its halo is staged in shared memory, the 11-tap Gaussian is applied along rows,
+// then along columns (separable) to x, y, x^2, y^2 and x*y.  Per output q the loss
+// gradient w.r.t. the five local means is kept as three maps (d/dmu_x, d/dE[x^2],
+// d/dE[xy]); the SSIM values of the tile are summed in a fixed order.
+__global__ void __launch_bounds__(kTX* kTY)
+    ssim_forward_kernel(int W, int H, const float* __restrict__ pred, const float* __restrict__ target, Window win,
+                        float ssim_grad_scale, float* __restrict__ gmap, float* __restrict__ partial)
+{
+    __shared__ float sx[kTY + kHalo][kTX + kHalo + 1];
+    __shared__ float sy[kTY + kHalo][kTX + kHalo + 1];
+    __shared__ float hq[5][kTY + kHalo][kTX];
+    __shared__ float red[kTX * kTY / 32];
+    const int Wo = W - kHalo, Ho = H - kHalo;
+    const int c = blockIdx.z;
+    const int ox0 = blockIdx.x * kTX, oy0 = blockIdx.y * kTY;
+    const float* x = pred + (size_t)c * W * H;
+    const float* y = target + (size_t)c * W * H;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < (kTY + kHalo) * (kTX + kHalo); i += kTX * kTY) {
+        const int r = i / (kTX + kHalo), cc = i % (kTX + kHalo);
+        const int gy = oy0 + r, gx = ox0 + cc;
+        const bool in = gy < H && gx < W;
+        sx[r][cc] = in ? __ldg(x + (size_t)gy * W + gx) : 0.f;
+        sy[r][cc] = in ? __ldg(y + (size_t)gy * W + gx) : 0.f;
+    }
+    __syncthreads();
+    for (int i = tid; i < (kTY + kHalo) * kTX; i += kTX * kTY) {
+        const int r = i / kTX, cc = i % kTX;
+        float a = 0.f, b = 0.f, aa = 0.f, bb = 0.f, ab = 0.f;
+#pragma unroll
+        for (int j = 0; j < kWin; j++) {
+            const float u = sx[r][cc + j], v = sy[r][cc + j], w = win.g[j];
+            a += w * u;
+            b += w * v;
+            aa += w * (u * u);
+            bb += w * (v * v);
+            ab += w * (u * v);
+        }
+        hq[0][r][cc] = a; hq[1][r][cc] = b; hq[2][r][cc] = aa; hq[3][r][cc] = bb; hq[4][r][cc] = ab;
+    }
+    __syncthreads();
+    const int tx = tid % kTX, ty = tid / kTX;
+    const int ox = ox0 + tx, oy = oy0 + ty;
+    float s = 0.f;
+    if (ox < Wo && oy < Ho) {
+        float m[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int i = 0; i < kWin; i++) {
+            const float w = win.g[i];
+#pragma unroll
+            for (int q = 0; q < 5; q++) m[q] += w * hq[q][ty + i][tx];
+        }
+        const float m1 = m[0], m2 = m[1];
+        const float s11 = m[2] - m1 * m1, s22 = m[3] - m2 * m2, s12 = m[4] - m1 * m2;
+        const float A = 2.f * m1 * m2 + kC1, B = 2.f * s12 + kC2;
+        const float Cc = m1 * m1 + m2 * m2 + kC1, D = s11 + s22 + kC2;
+        const float CD = Cc * D;
+        s = (A * B) / CD;
+        // d ssim / d(mu_x, E[x^2], E[xy]); the loss is 0.2 (1 - mean ssim): scale by -ssim_grad_scale
+        const float d_m1 = (2.f * m2 * B - 2.f * m2 * A) / CD - s * (2.f * m1 / Cc - 2.f * m1 / D);
+        const float d_e11 = -s / D;
+        const float d_e12 = 2.f * A / CD;
+        const size_t plane = (size_t)Wo * Ho, o = (size_t)oy * Wo + ox;
+        float* gm = gmap + (size_t)c * 3 * plane;
+        gm[o] = -ssim_grad_scale * d_m1;
+        gm[plane + o] = -ssim_grad_scale * d_e11;
+        gm[2 * plane + o] = -ssim_grad_scale * d_e12;
+    }
+    // fixed-order block sum of the tile's SSIM values
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((tid & 31) == 0) red[tid >> 5] = s;
+    __syncthreads();
+    if (tid == 0) {
+        float t = 0.f;
+        for (int w = 0; w < kTX * kTY / 32; w++) t += red[w];
+        partial[((size_t)c * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// ---------------------------------------------------------------- loss gradient per pixel
+// dL/dx_p = sum over the outputs q whose window covers p of w(q, p) *
+// (G1(q) + 2 x_p G11(q) + y_p G12(q)), a transposed separable convolution of the
+// three coefficient maps, plus the L1 term w_l1 * sign(x_p - y_p).  One CTA: a
+// kTX x kTY pixel tile of one channel; also sums |x - y| over the tile.
+__global__ void __launch_bounds__(kTX* kTY)
+    loss_grad_kernel(int W, int H, const float* __restrict__ pred, const float* __restrict__ target, Window win,
+                     const float* __restrict__ gmap, float l1_grad_scale, float* __restrict__ dpred,
+                     float* __restrict__ partial)
+{
+    __shared__ float sg[3][kTY + kHalo][kTX + kHalo + 1];
+    __shared__ float hv[3][kTY + kHalo][kTX];
+    __shared__ float red[kTX * kTY / 32];
+    const int Wo = W - kHalo, Ho = H - kHalo;
+    const int c = blockIdx.z;
+    const int px0 = blockIdx.x * kTX, py0 = blockIdx.y * kTY;
+    const size_t plane = (size_t)Wo * Ho;
+    const float* gm = gmap + (size_t)c * 3 * plane;
+    const int tid = threadIdx.x;
+    // outputs q in [p - kHalo, p]: rows py0 - kHalo .. py0 + kTY - 1
+    for (int i = tid; i < (kTY + kHalo) * (kTX + kHalo); i += kTX * kTY) {
+        const int r = i / (kTX + kHalo), cc = i % (kTX + kHalo);
+        const int qy = py0 - kHalo + r, qx = px0 - kHalo + cc;
+        const bool in = qy >= 0 && qx >= 0 && qy < Ho && qx < Wo;
+        const size_t o = (size_t)qy * Wo + qx;
+#pragma unroll
+        for (int k = 0; k < 3; k++) sg[k][r][cc] = in ? __ldg(gm + k * plane + o) : 0.f;
+    }
+    __syncthreads();
+    // along rows: T(r, p) = sum_j g_j G(r, p - j)
+    for (int i = tid; i < (kTY + kHalo) * kTX; i += kTX * kTY) {
+        const int r = i / kTX, cc = i % kTX;
+        float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+#pragma unroll
+        for (int j = 0; j < kWin; j++) {
+            const float w = win.g[j];
+            t0 += w * sg[0][r][cc + kHalo - j];
+            t1 += w * sg[1][r][cc + kHalo - j];
+            t2 += w * sg[2][r][cc + kHalo - j];
+        }
+        hv[0][r][cc] = t0; hv[1][r][cc] = t1; hv[2][r][cc] = t2;
+    }
+    __syncthreads();
+    const int tx = tid % kTX, ty = tid / kTX;
+    const int px = px0 + tx, py = py0 + ty;
+    float l1 = 0.f;
+    if (px < W && py < H) {
+        float s1 = 0.f, s11 = 0.f, s12 = 0.f;
+#pragma unroll
+        for (int i = 0; i < kWin; i++) {
+            const float w = win.g[i];
+            s1 += w * hv[0][ty + kHalo - i][tx];
+            s11 += w * hv[1][ty + kHalo - i][tx];
+            s12 += w * hv[2][ty + kHalo - i][tx];
+        }
+        const size_t o = (size_t)c * W * H + (size_t)py * W + px;
+        const float xv = __ldg(pred + o), yv = __ldg(target + o);
+        const float d = xv - yv;
+        const float sgn = d > 0.f ? 1.f : (d < 0.f ? -1.f : 0.f);
+        dpred[o] = s1 + 2.f * xv * s11 + yv * s12 + l1_grad_scale * sgn;
+        l1 = fabsf(d);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l1 += __shfl_xor_sync(0xffffffffu, l1, o);
+    if ((tid & 31) == 0) red[tid >> 5] = l1;
+    __syncthreads();
+    if (tid == 0) {
+        float t = 0.f;
+        for (int w = 0; w < kTX * kTY / 32; w++) t += red[w];
+        partial[((size_t)c * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
+    }
+}
+
+// sums[0] += sum(l1 partials), sums[1] += sum(ssim partials), in index order (one thread)
+__global__ void loss_reduce_kernel(const float* __restrict__ l1p, int nl1, const float* __restrict__ sp, int ns,
+                                   double* __restrict__ sums)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < nl1; i++) a += l1p[i];
+    for (int i = 0; i < ns; i++) b += sp[i];
+    sums[0] += a;
+    sums[1] += b;
+}
+
+// ---------------------------------------------------------------- activation, densification, Adam
+__device__ __forceinline__ float sigmoidf(float x) { return 1.f / (1.f + expf(-x)); }
+
+__global__ void activate_kernel(int P, const float* __restrict__ log_scale, const float* __restrict__ rot_raw,
+                                const float* __restrict__ opac_logit, float* __restrict__ scale,
+                                float* __restrict__ rot, float* __restrict__ opac)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) scale[3 * i + k] = expf(log_scale[3 * i + k]);
+        const float q0 = rot_raw[4 * i], q1 = rot_raw[4 * i + 1], q2 = rot_raw[4 * i + 2], q3 = rot_raw[4 * i + 3];
+        const float n = fmaxf(sqrtf(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3), 1e-12f);
+        rot[4 * i] = q0 / n; rot[4 * i + 1] = q1 / n; rot[4 * i + 2] = q2 / n; rot[4 * i + 3] = q3 / n;
+        opac[i] = sigmoidf(opac_logit[i]);
+    }
+}
+
+// Plain path: one view's dense screen-space gradient and radii.
+__global__ void densify_dense_kernel(int P, const int* __restrict__ radii, const float* __restrict__ dmean2D,
+                                     float* __restrict__ grad_sum, int* __restrict__ vis_count,
+                                     uint8_t* __restrict__ flag)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+        if (radii[i] <= 0) continue;
+        const float gx = dmean2D[3 * i], gy = dmean2D[3 * i + 1];
+        grad_sum[i] += sqrtf(gx * gx + gy * gy);
+        vis_count[i] += 1;
+        flag[i] = 1;
+    }
+}
+
+struct AdamRow {
+    float* p;
+    float* m;
+    float* v;
+};
+
+// sparse_optimizer.py:54-76 with torch's float32 arithmetic: the Python-float
+// coefficients beta and 1 - beta (formed in double) are rounded to float.
+__device__ __forceinline__ void adam_update(float& p, float& m, float& v, float g, float b1, float omb1, float b2,
+                                            float omb2, float step_size, float bc2_sqrt, float eps)
+{
+    m = m * b1 + g * omb1;
+    v = v * b2 + omb2 * g * g;
+    const float denom = sqrtf(v) / bc2_sqrt + eps;
+    p = p + (-step_size) * (m / denom);
+}
+
+}  // namespace
+
+__global__ void adam_kernel(fgs_adam_args a, const uint8_t* __restrict__ flag, const int* __restrict__ step)
+{
+    const int t = *step;
+    const double bc1 = 1.0 - pow(a.beta1, (double)t);
+    const double bc2 = 1.0 - pow(a.beta2, (double)t);
+    const float bc2s = (float)sqrt(bc2);
+    const float b1 = (float)a.beta1, b2 = (float)a.beta2, eps = a.eps;
+    const float omb1 = (float)(1.0 - a.beta1), omb2 = (float)(1.0 - a.beta2);
+    const int F = 3 * a.M;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.P; i += gridDim.x * blockDim.x) {
+        if (!flag[i]) continue;
+        // means (as given)
+        {
+            const float ss = (float)(a.lr[0] / bc1);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const size_t j = 3 * (size_t)i + k;
+                adam_update(a.xyz[j], a.m_xyz[j], a.v_xyz[j], a.g_xyz[j], b1, omb1, b2, omb2, ss, bc2s, eps);
+            }
+        }
+        // SH coefficients (as given)
+        if (a.shs) {
+            const float ss = (float)(a.lr[1] / bc1);
+            for (int k = 0; k < F; k++) {
+                const size_t j = (size_t)F * i + k;
+                adam_update(a.shs[j], a.m_shs[j], a.v_shs[j], a.g_shs[j], b1, omb1, b2, omb2, ss, bc2s, eps);
+            }
+        }
+        // opacity: d/dlogit = d/dopacity * s (1 - s)
+        {
+            const float ss = (float)(a.lr[2] / bc1);
+            const float s = a.opac[i];
+            const float g = a.g_opac[i] * (s * (1.f - s));
+            adam_update(a.opac_logit[i], a.m_opac[i], a.v_opac[i], g, b1, omb1, b2, omb2, ss, bc2s, eps);
+            a.opac[i] = sigmoidf(a.opac_logit[i]);
+        }
+        // scale: d/dlog = d/dscale * scale
+        {
+            const float ss = (float)(a.lr[3] / bc1);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const size_t j = 3 * (size_t)i + k;
+                const float g = a.g_scale[j] * a.scale[j];
+                adam_update(a.log_scale[j], a.m_scale[j], a.v_scale[j], g, b1, omb1, b2, omb2, ss, bc2s, eps);
+                a.scale[j] = expf(a.log_scale[j]);
+            }
+        }
+        // rotation: d/dq = (d/dq_hat - q_hat (q_hat . d/dq_hat)) / |q|
+        {
+            const float ss = (float)(a.lr[4] / bc1);
+            float q[4], qh[4], gq[4];
+            float n2 = 0.f, dot = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                q[k] = a.rot_raw[4 * (size_t)i + k];
+                n2 += q[k] * q[k];
+            }
+            const float n = fmaxf(sqrtf(n2), 1e-12f);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                qh[k] = a.rot[4 * (size_t)i + k];
+                dot += qh[k] * a.g_rot[4 * (size_t)i + k];
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) gq[k] = (a.g_rot[4 * (size_t)i + k] - qh[k] * dot) / n;
+            float m2 = 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const size_t j = 4 * (size_t)i + k;
+                adam_update(a.rot_raw[j], a.m_rot[j], a.v_rot[j], gq[k], b1, omb1, b2, omb2, ss, bc2s, eps);
+                m2 += a.rot_raw[j] * a.rot_raw[j];
+            }
+            const float nn = fmaxf(sqrtf(m2), 1e-12f);
+#pragma unroll
+            for (int k = 0; k < 4; k++) a.rot[4 * (size_t)i + k] = a.rot_raw[4 * (size_t)i + k] / nn;
+        }
+    }
+}
+
+__global__ void step_tick_kernel(int* step) { *step += 1; }
+
+namespace {
+Window make_window()
+{
+    // loss.py:7-10: exp(-(x - 5)^2 / (2 * 1.5^2)) in double, stored as float32, normalised in float32
+    Window w;
+    float sum = 0.f;
+    for (int i = 0; i < kWin; i++) {
+        w.g[i] = (float)std::exp(-(double)((i - kWin / 2) * (i - kWin / 2)) / (2.0 * 1.5 * 1.5));
+        sum += w.g[i];
+    }
+    for (int i = 0; i < kWin; i++) w.g[i] = w.g[i] / sum;
+    return w;
+}
+}  // namespace
+
+}  // namespace fgs
+
+using namespace fgs;
+
+extern "C" {
+
+size_t fgs_loss_scratch_bytes(int width, int height)
+{
+    if (width <= kHalo || height <= kHalo) return 0;
+    const size_t Wo = (size_t)width - kHalo, Ho = (size_t)height - kHalo;
+    const size_t nso = 3 * ((Wo + kTX - 1) / kTX) * ((Ho + kTY - 1) / kTY);
+    const size_t nl1 = 3 * (((size_t)width + kTX - 1) / kTX) * (((size_t)height + kTY - 1) / kTY);
+    return sizeof(float) * (9 * Wo * Ho + nso + nl1) + 256;
+}
+
+int fgs_loss_l1_ssim(int width, int height, const float* pred, const float* target, float* dL_dpred,
+                     float l1_grad_scale, float ssim_grad_scale, double* sums, void* scratch, void* stream)
+{
+    if (width <= kHalo || height <= kHalo || !pred || !target || !dL_dpred || !sums || !scratch) return FGS_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int Wo = width - kHalo, Ho = height - kHalo;
+    float* gmap = static_cast<float*>(scratch);
+    const dim3 go((Wo + kTX - 1) / kTX, (Ho + kTY - 1) / kTY, 3);
+    const dim3 gp((width + kTX - 1) / kTX, (height + kTY - 1) / kTY, 3);
+    float* sp = gmap + (size_t)9 * Wo * Ho;
+    float* l1p = sp + (size_t)go.x * go.y * go.z;
+    static const Window win = make_window();
+    ssim_forward_kernel<<<go, kTX * kTY, 0, s>>>(width, height, pred, target, win, ssim_grad_scale, gmap, sp);
+    loss_grad_kernel<<<gp, kTX * kTY, 0, s>>>(width, height, pred, target, win, gmap, l1_grad_scale, dL_dpred, l1p);
+    loss_reduce_kernel<<<1, 32, 0, s>>>(l1p, (int)(gp.x * gp.y * gp.z), sp, (int)(go.x * go.y * go.z), sums);
+    note_launches(3);
+    return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
+}
+
+int fgs_train_activate(int P, const float* log_scale, const float* rot_raw, const float* opac_logit, float* scale,
+                       float* rot, float* opac, void* stream)
+{
+    if (P < 0 || (P > 0 && (!log_scale || !rot_raw || !opac_logit || !scale || !rot || !opac))) return FGS_ERR_ARG;
+    if (P == 0) return FGS_OK;
+    activate_kernel<<<(P + 255) / 256 < 4096 ? (P + 255) / 256 : 4096, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        P, log_scale, rot_raw, opac_logit, scale, rot, opac);
+    note_launches(1);
+    return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
+}
+
+int fgs_densify_dense(int P, const int* radii, const float* dL_dmeans2D, float* grad_sum, int* vis_count,
+                      unsigned char* flag, void* stream)
+{
+    if (P < 0 || (P > 0 && (!radii || !dL_dmeans2D || !grad_sum || !vis_count || !flag))) return FGS_ERR_ARG;
+    if (P == 0) return FGS_OK;
+    densify_dense_kernel<<<(P + 255) / 256 < 4096 ? (P + 255) / 256 : 4096, 256, 0,
+                           static_cast<cudaStream_t>(stream)>>>(P, radii, dL_dmeans2D, grad_sum, vis_count, flag);
+    note_launches(1);
+    return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
+}
+
+int fgs_adam_step(const fgs_adam_args* a, const unsigned char* flag, int* step, void* stream)
+{
+    if (!a || !flag || !step || a->P < 0 || a->M < 0) return FGS_ERR_ARG;
+    if (!a->xyz || !a->opac_logit || !a->log_scale || !a->rot_raw || !a->opac || !a->scale || !a->rot) return FGS_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    step_tick_kernel<<<1, 1, 0, s>>>(step);
+    if (a->P > 0)
+        adam_kernel<<<(a->P + 255) / 256 < 4096 ? (a->P + 255) / 256 : 4096, 256, 0, s>>>(*a, flag, step);
+    note_launches(2);
+    return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -178,6 +178,48 @@ int fgs_batch_pair_counts(void *handle, long long *counts, void *stream);
 /* Synchronise and return the first device-side error of the batch (FGS_OK when none). */
 int fgs_batch_check(void *handle, void *stream);
 void fgs_batch_destroy(void *handle);
+/* Optional training statistics, accumulated by every fgs_batch_backward (views in order):
+ * grad_sum[P] += |dL/dmeans2D[:2]| and vis_count[P] += 1 per view that sees the Gaussian,
+ * flag[P] = 1 (the caller zeroes the flags between steps).  All null: off.
+ * LoG/model/counter.py:36-83 (the two statistics the training step keeps).            */
+int fgs_batch_set_densify(void *handle, float *grad_sum, int *vis_count, unsigned char *flag);
+
+/* ------------------------------------------------------------------ training step
+ * The loss, optimizer and statistics of LoG's training loop around the rasterizer.   */
+/* Scratch bytes of fgs_loss_l1_ssim for one [3,H,W] image (0 if the image is smaller than
+ * the 11x11 window). */
+size_t fgs_loss_scratch_bytes(int width, int height);
+/* LoG/render/loss.py:6-44 + renderer.py:260-273.  For one view: writes
+ *   dL_dpred = l1_grad_scale * sign(pred - target) + ssim_grad_scale * d(1 - ssim_sum)/dpred
+ * (SSIM: 11x11 Gaussian window, sigma 1.5, no padding) and adds the view's sum |pred - target|
+ * to sums[0] and its sum of SSIM map values to sums[1] (doubles on the device, in a fixed
+ * order).  For the loss 0.8 L1 + 0.2 (1 - SSIM) over a batch: l1_grad_scale =
+ * 0.8 / (batch * 3 * H * W), ssim_grad_scale = 0.2 / (batch * 3 * (H-10) * (W-10)).    */
+int fgs_loss_l1_ssim(int width, int height, const float *pred, const float *target, float *dL_dpred,
+                     float l1_grad_scale, float ssim_grad_scale, double *sums, void *scratch, void *stream);
+/* LoG/model/activation.py: scale = exp(log_scale), rot = normalize(rot_raw), opac = sigmoid(logit). */
+int fgs_train_activate(int P, const float *log_scale, const float *rot_raw, const float *opac_logit, float *scale,
+                       float *rot, float *opac, void *stream);
+/* One view of the plain path: for radii > 0, grad_sum += |dL_dmeans2D[:2]|, vis_count += 1, flag = 1. */
+int fgs_densify_dense(int P, const int *radii, const float *dL_dmeans2D, float *grad_sum, int *vis_count,
+                      unsigned char *flag, void *stream);
+/* LoG/model/sparse_optimizer.py:41-78,163-196: one Adam step (the device step counter is
+ * incremented first; bias corrections from it; eps as given) on the rows with flag set.
+ * Gradients are w.r.t. the rasterizer's inputs (means, SH, activated opacity / scale,
+ * normalised rotation) and are chained through the activations; the activated values of
+ * the updated rows are rewritten.  lr: means, SH, opacity, scale, rotation.             */
+typedef struct fgs_adam_args {
+    int P, M;                     /* Gaussians, SH coefficients per channel (0: no SH) */
+    float lr[5];
+    double beta1, beta2;          /* as the reference's Python floats: 1 - beta is formed in double */
+    float eps;
+    float *xyz, *shs, *opac_logit, *log_scale, *rot_raw;      /* raw parameters (updated) */
+    float *opac, *scale, *rot;                                /* activated (rewritten) */
+    const float *g_xyz, *g_shs, *g_opac, *g_scale, *g_rot;    /* gradients */
+    float *m_xyz, *m_shs, *m_opac, *m_scale, *m_rot;          /* first moments */
+    float *v_xyz, *v_shs, *v_opac, *v_scale, *v_rot;          /* second moments */
+} fgs_adam_args;
+int fgs_adam_step(const fgs_adam_args *a, const unsigned char *flag, int *step, void *stream);
 
 /* ------------------------------------------------------------------ LoD selection and gather
  * gather_attributes_cuda (FilterGS/cuda/gather_attributes_kernel.cu:70-145): rows of xyz/scaling [.,3],
