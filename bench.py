@@ -12,7 +12,10 @@ One step = forward + backward of all 16 views:
   plain (beside it):  16 calls of the one-view-per-call `_C` operator path.
 A second workload (the mixed-resolution batch: 16 cameras with resolutions drawn from
 {640x360, 1280x720, 1600x900, 1920x1080}, altitudes 80-300 m, pitch 30-75 deg) is
-measured the same way and reported under `mixed_resolution`.
+measured the same way and reported under `mixed_resolution`; `lod_tree` is the per-view
+LoD selection + forward render of an 8M-node Gaussian tree, and `train_step` the ms per
+iteration of a full training step (4M Gaussians, 4 views 1600x900, L1 + SSIM, backward,
+Adam) batched vs plain.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--path batched|plain]
 
@@ -64,6 +67,8 @@ def parse(argv=None):
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-resolution workload")
     ap.add_argument("--no-lod", action="store_true", help="skip the LoD-tree filter + render workload")
+    ap.add_argument("--no-train", action="store_true", help="skip the training-step workload")
+    ap.add_argument("--train-gaussians", type=int, default=4_000_000)
     ap.add_argument("--lod-nodes", type=int, default=8_000_000)
     ap.add_argument("--no-autotune", action="store_true", help="keep the default render kernel shape")
     ap.add_argument("--render-config", default=None,
@@ -434,11 +439,11 @@ def stages_of(prof):
 
 # ---------------------------------------------------------------- LoD tree: filter + render (forward)
 def make_lod(args, dev):
-    """8M-node Gaussian tree (branching min(Poisson(3)+1, 8), depth <= 12, child scale x0.5) centred in the
-    urban area, and a 1920x1080 camera at 150 m altitude, 45 deg pitch, looking at the tree's centre."""
+    """8M-node Gaussian tree (branching min(Poisson(3)+1, 8), depth <= 12, child scale x0.5) over the urban
+    area, and a 1920x1080 camera at 150 m altitude, 45 deg pitch, looking at the first root's subtree."""
     from filtergs_b200 import lod, synthetic as S
     tr = S.lod_tree(P=args.lod_nodes, seed=1002, roots=2, max_depth=12, half_extent=500.0)
-    c = tr["xyz"][tr["roots"]].mean(0)
+    c = tr["xyz"][tr["roots"][0]].astype(np.float64)   # aim at the first root's subtree
     c[2] = 0.0
     cam = S.look_at_camera(c + np.array([150.0, 0.0, 150.0]), c, W=1920, H=1080, fx=1600.0)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
@@ -503,6 +508,56 @@ def measure_lod(args, dev, impl):
         out["filtergs"] = {"value": steps / (ms / 1000.0), "selected": int(n), "pairs_K": int(r[0])}
     del scene
     torch.cuda.empty_cache()
+    return out
+
+
+# ---------------------------------------------------------------- training step (loss, backward, Adam)
+def measure_train(args, dev):
+    """ms per training iteration: 4M Gaussians (the urban generator on 2 km x 2 km with 1,200 buildings),
+    4 views 1600x900 (altitude 80-300 m, pitch 30-75 deg), targets = renders of a perturbed copy (means
+    + N(0, 0.05 m), SH DC + N(0, 0.1)), loss 0.8 L1 + 0.2 (1 - SSIM), backward, FP32 Adam on the visible
+    Gaussians, densification statistics.  Batched (one CUDA graph per iteration) vs plain (one view per
+    call)."""
+    from filtergs_b200 import synthetic as S, train as TR
+    from filtergs_b200.batched import Camera
+    from filtergs_b200._C import rasterize_gaussians
+    P = args.train_gaussians
+    sc = S.urban_scene(P=P, seed=1004, half_extent=1000.0, buildings=1200)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    state_args = (t(sc["means3D"]), torch.log(t(sc["scales"])), t(sc["rotations"]),
+                  torch.logit(t(sc["opacities"]).clamp(1e-6, 1 - 1e-6)), t(sc["shs"]))
+    del sc
+    rng = np.random.default_rng(5004)
+    cams = []
+    for _ in range(4):
+        c = S.aerial_camera(rng, W=1600, H=900, fx=1600.0 * 1600 / 1920, altitude=float(rng.uniform(80, 300)),
+                            pitch_deg=float(rng.uniform(30, 75)), xy_range=600.0)
+        cams.append(Camera(c.W, c.H, c.tanfovx, c.tanfovy, t(c.viewmatrix), t(c.projmatrix), t(c.campos)))
+    g = torch.Generator(device=dev).manual_seed(6004)
+    pert = TR.TrainState(state_args[0] + 0.05 * torch.randn(P, 3, device=dev, generator=g), *state_args[1:4],
+                         state_args[4] + torch.cat([0.1 * torch.randn(P, 1, 3, device=dev, generator=g),
+                                                    torch.zeros(P, state_args[4].shape[1] - 1, 3, device=dev)], 1))
+    e = torch.empty(0, device=dev)
+    bg = torch.zeros(3, device=dev)
+    targets = [rasterize_gaussians(bg, pert.xyz, e, pert.opac, pert.scale, pert.rot, 1.0, e, c.viewmatrix,
+                                   c.projmatrix, c.tanfovx, c.tanfovy, c.H, c.W, pert.shs, 3, c.campos, False, True,
+                                   False, 0.2, 0.2, 0.05, 0.7, False)[1].clone() for c in cams]
+    del pert
+    out = {"gaussians": P, "views_per_step": 4, "width": 1600, "height": 900, "unit": "ms/iteration",
+           "loss": "0.8 L1 + 0.2 (1 - SSIM 11x11, sigma 1.5)", "optimizer": "FP32 Adam on visible Gaussians"}
+    for name in ("batched", "plain"):
+        st = TR.TrainState(*state_args)
+        tr = TR.BatchedTrainer(st, cams, targets, bg=bg) if name == "batched" else TR.PlainTrainer(st, cams, targets,
+                                                                                                     bg=bg)
+        for _ in range(max(3, args.warmup)):
+            tr.step()
+        first = tr.loss.value()
+        ms, _ = timed(lambda i: tr.step(), args.steps)
+        if name == "batched":
+            tr.check()
+        out[name] = {"ms_per_iteration": ms / args.steps, "loss_after_warmup": first, "loss_last": tr.loss.value()}
+        del tr, st
+        torch.cuda.empty_cache()
     return out
 
 
@@ -604,9 +659,11 @@ def main():
                  "plain_value": n_ranks * nv * args.steps / (mp["ms"] / 1000.0),
                  "unit": "views/s", "batched_render_config": mb["tuned"], "plain_render_config": mp["tuned"],
                  "pairs_K": mb["K"], "visible_V": mb["vis"], "altitude_m": "80-300", "pitch_deg": "30-75"}
-    lod_res = None
+    lod_res = train_res = None
     if not args.no_lod and rank == 0:
         lod_res = measure_lod(args, dev, args.impl)
+    if not args.no_train and rank == 0 and args.impl == "ours":
+        train_res = measure_train(args, dev)
     if clocks:
         clocks.stop()
 
@@ -649,6 +706,8 @@ def main():
                 res["cpu_baseline"]["fp64_image_error"] = fp64_image_error(mod, dev)
         if lod_res:
             res["lod_tree"] = lod_res
+        if train_res:
+            res["train_step"] = train_res
         if head["clocks"]:
             res["clocks"] = head["clocks"]
         print(json.dumps(res), flush=True)
