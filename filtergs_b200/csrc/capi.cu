@@ -246,6 +246,28 @@ cudaEvent_t pool_event()
 
 void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+uint32_t resident_ctas_query(const void* kernel, int threads)
+{
+    struct Entry {
+        const void* k;
+        int threads, dev;
+        uint32_t ctas;
+    };
+    static std::mutex mu;
+    static std::vector<Entry> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    for (const Entry& e : cache)
+        if (e.k == kernel && e.threads == threads && e.dev == dev) return e.ctas;
+    int sms = 148, per = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+    const uint32_t r = (uint32_t)(sms * (per > 0 ? per : 1));
+    cache.push_back(Entry{kernel, threads, dev, r});
+    return r;
+}
+
 StageTimer::StageTimer(int st, cudaStream_t s) : stage(st), stream(s), slot(nullptr)
 {
     std::lock_guard<std::mutex> lk(g_prof_mu);

@@ -82,19 +82,13 @@ size_t bin_bytes_forward(long long K, int P);  // without the per-pair gradients
 
 // ---------------------------------------------------------------- launchers
 // Resident CTAs of a kernel on this device (persistent grids never exceed it).
+// Cached per (kernel, block size, device): kernels of the same signature have
+// their own entries.
+uint32_t resident_ctas_query(const void* kernel, int threads);
 template <typename Kern>
 inline uint32_t resident_ctas(Kern k, int threads)
 {
-    static uint32_t cache[64] = {};  // per device ordinal; the same value if two threads race
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && cache[dev]) return cache[dev];
-    int sms = 148, per = 1;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, threads, 0);
-    const uint32_t r = (uint32_t)(sms * (per > 0 ? per : 1));
-    if (dev >= 0 && dev < 64) cache[dev] = r;
-    return r;
+    return resident_ctas_query(reinterpret_cast<const void*>(k), threads);
 }
 
 void launch_preprocess(const PreParams& p, const GeomState& g, int* radii, cudaStream_t s);

@@ -124,20 +124,26 @@ __global__ void __launch_bounds__(kThreads) preprocess_cull_kernel(PreParams p, 
         const unsigned cb = __ballot_sync(0xffffffffu, cand);
         if (lane == 0) s_wc[warp] = __popc(cb);
         __syncthreads();
-        uint32_t pos = s_n + __popc(cb & ((1u << lane) - 1u)), tot = 0;
+        // s_n is read once, before the barrier: thread 0 rewrites it after the
+        // barrier, and every thread must take the same flush decision from n.
+        const uint32_t n0 = s_n;
+        uint32_t pos = n0 + __popc(cb & ((1u << lane) - 1u)), tot = 0;
 #pragma unroll
         for (int w = 0; w < kThreads / 32; w++) {
             if (w < warp) pos += s_wc[w];
             tot += s_wc[w];
         }
         if (cand) s_list[pos] = (uint32_t)idx;
+        const uint32_t n = n0 + tot;
         __syncthreads();
-        const uint32_t n = s_n + tot;
         const bool last = idx0 + stride >= p.P;
         if (n > kList - kThreads || last) {
             if (threadIdx.x == 0) s_base = n ? atomicAdd(g.counters + 12, n) : 0u;
             __syncthreads();
-            for (uint32_t k = threadIdx.x; k < n; k += kThreads) g.cand_ids[s_base + k] = s_list[k];
+            for (uint32_t k = threadIdx.x; k < n; k += kThreads) {
+                if (s_base + k < (uint32_t)p.P) g.cand_ids[s_base + k] = s_list[k];
+                else set_error(g.err, FGS_ERR_OVERFLOW);  // a list longer than P: never write past it
+            }
             __syncthreads();
             if (threadIdx.x == 0) s_n = 0;
         } else if (threadIdx.x == 0) {
@@ -164,7 +170,7 @@ __global__ void __launch_bounds__(kThreads) preprocess_full_kernel(PreParams p, 
         s_log_lambda_G = logf(lambda_G);
     }
     __syncthreads();
-    const uint32_t ncand = *(volatile uint32_t*)(g.counters + 12);
+    const uint32_t ncand = min(*(volatile uint32_t*)(g.counters + 12), (uint32_t)p.P);
     const bool vec = p.aligned != 0;
     for (uint32_t k = blockIdx.x * kThreads + threadIdx.x; k < ncand; k += gridDim.x * kThreads) {
         const int idx = (int)g.cand_ids[k];
