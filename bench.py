@@ -471,10 +471,13 @@ def measure_lod(args, dev, impl):
             return lod.render_selected(scene, idx, cnt, view, proj, cpos, cam, bg, stats=False), cnt
 
         for name, fn in (("filtergs", filtergs), ("logcut", logcut)):
+            # the compositing launch shape for this view (small, dense splats favour 1 pixel per thread)
+            tuned = autotune(args, fn, ("lod", name), 0)
             for i in range(3):
                 r, cnt = fn(i)
             ms, _ = timed(fn, steps)
-            out[name] = {"value": steps / (ms / 1000.0), "selected": int(cnt.item()), "pairs_K": int(r[0])}
+            out[name] = {"value": steps / (ms / 1000.0), "selected": int(cnt.item()), "pairs_K": int(r[0]),
+                         "render_config": tuned}
     else:
         from oracle import build_ref
         ref, v2 = build_ref.load("ref_rasterizer_C"), build_ref.load("ref_compute_radius_v2")

@@ -83,6 +83,7 @@ SIGNATURES = {
     "fgs_log_cut_scratch_bytes": (sz, [i32, i32, i32, i32]),
     "fgs_log_cut": (i32, [i32, vp, i32, vp, vp, i32, vp, f32, i32, vp, vp, vp, vp]),
     "fgs_cull": (i32, [vp, vp, i32, vp, vp, f32, vp, vp, vp, vp]),
+    "fgs_ancestor_path": (i32, [i32, vp, vp, i32, vp, vp, vp]),
     "fgs_batch_workspace_bytes": (sz, [i32, i32, vp]),
     "fgs_batch_create": (vp, [C.POINTER(RasterArgs), i32, vp, vp, sz, i32, vp, vp, vp, vp, vp, C.POINTER(i32), vp]),
     "fgs_batch_forward": (i32, [vp, vp]),

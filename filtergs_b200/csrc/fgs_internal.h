@@ -199,6 +199,8 @@ void launch_log_cut(int P, const int32_t* roots, int nroots, const int32_t* node
 void launch_cull(const int32_t* in, const uint32_t* n_in, uint32_t cap, const float* radius, const float* opac_raw,
                  float min_px, int64_t* out, unsigned long long* n_out, uint32_t* scratch, unsigned* err,
                  cudaStream_t s);
+void launch_ancestor_path(int P, const int32_t* parent, const int32_t* depth, int L, int32_t* out, unsigned* err,
+                          cudaStream_t s);
 
 // Kernel-launch accounting (fgs_launch_count) and per-stage event timing.
 void note_launches(int n);

@@ -291,6 +291,39 @@ __global__ void radius_raw_kernel(int P, const float* __restrict__ means, const 
     radius[idx] = 3.f * sqrtf(fmaxf(lambda1, lambda2));
 }
 
+// rebuild_ancestor_path (apps/ancestor.py:21-73) without its level loop.  The
+// reference visits depths 1..max in order and, for each node i at depth d with
+// a parent p >= 0, copies row(p) as it stands at that moment and sets column
+// d-1 to p (a node with p < 0 keeps a row of -1).  row(p) is final when
+// 1 <= depth(p) < d, and still all -1 otherwise (not yet visited, or visited in
+// the same level, whose gather precedes its scatter).  So row(i) is the chain
+// i -> p -> ... followed while depths strictly decrease and stay >= 1, each
+// step writing its own column: one thread per node walks it (at most L steps;
+// the -1 fill is a memset).  The reference raises on a parent id >= P and on a
+// column d-1 >= L; both are reported through err.
+__global__ void __launch_bounds__(256) ancestor_path_kernel(int P, const int32_t* __restrict__ parent,
+                                                            const int32_t* __restrict__ depth, int L,
+                                                            int32_t* __restrict__ out, unsigned* err)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+        int cur = i, dc = __ldg(depth + i);
+        int32_t* row = out + (size_t)i * L;
+        while (dc >= 1) {
+            const int p = __ldg(parent + cur);
+            if (p < 0) break;  // orphan: its row is all -1
+            if (p >= P || dc - 1 >= L) {
+                set_error(err, FGS_ERR_ARG);
+                break;
+            }
+            row[dc - 1] = p;
+            const int dp = __ldg(depth + p);
+            if (dp >= dc) break;  // the parent's row is still -1 when this level is visited
+            cur = p;
+            dc = dp;
+        }
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
@@ -401,6 +434,16 @@ void launch_cull(const int32_t* in, const uint32_t* n_in, uint32_t cap, const fl
     note_launches(1);
 }
 
+void launch_ancestor_path(int P, const int32_t* parent, const int32_t* depth, int L, int32_t* out, unsigned* err,
+                          cudaStream_t s)
+{
+    cudaMemsetAsync(out, 0xff, sizeof(int32_t) * (size_t)P * (size_t)L, s);  // -1 everywhere
+    const uint32_t want = ((uint32_t)P + 255) / 256;
+    const uint32_t grid = min(want, 8 * resident_ctas(ancestor_path_kernel, 256));
+    ancestor_path_kernel<<<grid, 256, 0, s>>>(P, parent, depth, L, out, err);
+    note_launches(1);
+}
+
 }  // namespace fgs
 
 using namespace fgs;
@@ -496,6 +539,17 @@ int fgs_log_cut(int P, const int32_t* roots, int num_roots, const int32_t* node_
     launch_log_cut(P, roots, num_roots, node_index, tree, max_child, radius, min_resolution_pixel, levels, out, sc,
                    err, s);
     cudaMemcpyAsync(out_count_dev, sc + (levels & 1), sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+    return launch_status();
+}
+
+int fgs_ancestor_path(int P, const int32_t* index_parent, const int32_t* depth, int L, int32_t* out,
+                      unsigned* err_dev, void* stream)
+{
+    if (P < 0 || L < 0 || !err_dev || (P > 0 && L > 0 && (!index_parent || !depth || !out))) return FGS_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaMemsetAsync(err_dev, 0, sizeof(unsigned), s);
+    // an empty table (L == 0) is returned as is, without the level loop (apps/ancestor.py:51-55)
+    if (P > 0 && L > 0) launch_ancestor_path(P, index_parent, depth, L, out, err_dev, s);
     return launch_status();
 }
 

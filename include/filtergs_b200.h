@@ -263,6 +263,14 @@ int fgs_log_cut(int P, const int32_t *roots, int num_roots, const int32_t *node_
  * *out_count_dev.  scratch: fgs_compact_scratch_bytes(cap) bytes.                                   */
 int fgs_cull(const int32_t *ids, const uint32_t *count_dev, int cap, const float *radius, const float *opacity_raw,
              float min_px, int64_t *out, unsigned long long *out_count_dev, void *scratch, void *stream);
+/* ancestor_path of a LoG tree (replaces rebuild_ancestor_path, apps/ancestor.py:21-73, a per-level
+ * torch loop): out[i, k] = id of node i's ancestor at depth k, -1 elsewhere, [P, L] int32 row-major,
+ * from index_parent [P] and depth [P] (int32).  Same result as the reference's level order, also for
+ * trees whose depths disagree with their parents'.  Where the reference raises (a parent id >= P, or a
+ * node with a parent at depth > L) the kernel leaves FGS_ERR_ARG in *err_dev (bit 1 << code, zeroed
+ * here) and the row unfinished.  No host synchronisation.                                             */
+int fgs_ancestor_path(int P, const int32_t *index_parent, const int32_t *depth, int L, int32_t *out,
+                      unsigned *err_dev, void *stream);
 
 /* ------------------------------------------------------------------ test accessors
  * Sorted (tile|depth) keys and Gaussian ids of a forward, in the reference's

@@ -19,6 +19,7 @@
  *   cov2D / preprocess backward .. backward.cu:20-396
  *   LoD visibility mask .......... FilterGS/cuda/compute_radius_kernel_v2.cu:109-169,231-353
  *   LoG cut traversal ............ LoG/model/tensor_tree.py:133-187
+ *   ancestor_path builder ........ apps/ancestor.py:21-73
  *   KPC/GTC statistics ........... rasterizer_impl.cu:450-556
  *
  * Parity pins: the FP32 restatement is checked against fixtures produced by
@@ -931,6 +932,46 @@ long long SFX(orc_log_cut)(int num_roots, const int32_t *roots, const int32_t *n
         level++;
     }
     return n;
+}
+
+/* ---------------------------------------------------------------- ancestor_path */
+
+/* apps/ancestor.py:21-73 (rebuild_ancestor_path), level by level as written:
+ * for level = 1 .. max(depth), the nodes at that level with a parent p >= 0
+ * take a copy of row(p) as it stands before this level's writes, then column
+ * level-1 = p; nodes with p < 0 keep -1.  The gather of a level is finished
+ * before its scatter (torch evaluates the right-hand side first), so a node
+ * whose parent sits in the same level copies the parent's old row.  Returns 0,
+ * or -1 where the reference raises an index error (parent id >= P, or column
+ * level-1 >= L for a node with a parent).  out: [P, L], scratch: [P * L]. */
+int SFX(orc_ancestor_path)(int P, const int32_t *parent, const int32_t *depth, int L, int32_t *out,
+                           int32_t *scratch)
+{
+    for (size_t k = 0; k < (size_t)P * (size_t)L; k++) out[k] = -1;
+    if (P == 0 || L == 0) return 0;
+    int max_depth = 0;
+    for (int i = 0; i < P; i++)
+        if (depth[i] > max_depth) max_depth = depth[i];
+    for (int level = 1; level <= max_depth; level++) {
+        /* gather: rows of the parents as they are now */
+        for (int i = 0; i < P; i++) {
+            if (depth[i] != level || parent[i] < 0) continue;
+            if (parent[i] >= P) return -1;
+            memcpy(scratch + (size_t)i * L, out + (size_t)parent[i] * L, sizeof(int32_t) * (size_t)L);
+        }
+        /* scatter */
+        for (int i = 0; i < P; i++) {
+            if (depth[i] != level) continue;
+            if (parent[i] < 0) {
+                for (int k = 0; k < L; k++) out[(size_t)i * L + k] = -1;
+                continue;
+            }
+            if (level - 1 >= L) return -1;
+            memcpy(out + (size_t)i * L, scratch + (size_t)i * L, sizeof(int32_t) * (size_t)L);
+            out[(size_t)i * L + level - 1] = parent[i];
+        }
+    }
+    return 0;
 }
 
 /* ---------------------------------------------------------------- activations + gather */

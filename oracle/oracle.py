@@ -281,6 +281,20 @@ def log_cut(roots, node_index, tree, radius, min_res, max_depth=1000, dtype=np.f
     return out[:n].astype(np.int64)
 
 
+def ancestor_path(parent, depth, L):
+    """rebuild_ancestor_path (apps/ancestor.py:21-73) -> int32 [P, L], or None where the reference raises."""
+    lib = _lib(np.float32)
+    par = np.ascontiguousarray(parent, np.int32)
+    dep = np.ascontiguousarray(depth, np.int32)
+    P = par.shape[0]
+    out = np.zeros((P, L), np.int32)
+    scratch = np.zeros((P, L), np.int32)
+    f = lib.orc_ancestor_path_f32
+    f.restype = C.c_int
+    rc = f(C.c_int(P), _p(par), _p(dep), C.c_int(L), _p(out), _p(scratch))
+    return None if rc else out
+
+
 def gather_activate(index, xyz, lscale, rot, opac, dc, shs_rest, sh_deg, campos, dtype=np.float32):
     lib = _lib(dtype)
     index = np.ascontiguousarray(index, np.int64)

@@ -107,8 +107,57 @@ def tree_case():
                         ancestor_path=anc.numpy(), max_depth=max_depth, radius=radius, cut=cut.numpy())
 
 
+def ancestor_case():
+    """rebuild_ancestor_path on trees built to reach every branch of its level loop: a consistent
+    tree with a wider stored table, the same without one (width = max depth + 1), a tree whose
+    depths disagree with its parents' (orphans, parents in the same or a deeper level, depth-0
+    nodes with parents, negative depths and parents), the old key name, and two inputs on which the
+    reference raises (a parent id past the table, a depth past the stored width)."""
+    anc_mod = _load("apps/ancestor.py", "ref_ancestor")
+    rng = np.random.default_rng(2204)
+    out = {}
+
+    def run(name, parent, depth, old=None, key="tree.ancestor_path"):
+        sd = {"tree.index_parent": torch.from_numpy(parent.astype(np.int32)),
+              "tree.depth": torch.from_numpy(depth.astype(np.int8))}
+        if old is not None:
+            sd[key] = torch.from_numpy(old)
+        out[name + "_parent"] = parent.astype(np.int32)
+        out[name + "_depth"] = depth.astype(np.int32)
+        out[name + "_width"] = np.int32(old.shape[1] if old is not None else (int(depth.max()) + 1 if depth.size else 1))
+        try:
+            anc, md = anc_mod.rebuild_ancestor_path(sd)
+            out[name + "_ancestor"] = anc.numpy().astype(np.int32)
+            out[name + "_max_depth"] = np.int32(md)
+            out[name + "_raises"] = np.int32(0)
+        except (IndexError, RuntimeError):
+            out[name + "_raises"] = np.int32(1)
+
+    tr = S.lod_tree(P=3000, seed=2205, roots=2, max_depth=5, half_extent=40.0)
+    run("consistent", tr["parent"], tr["level"], old=np.zeros((3000, 8), np.int32))
+    run("noold", tr["parent"], tr["level"])
+    P = 2000
+    parent = rng.integers(-3, P, P)
+    depth = rng.integers(-1, 7, P)
+    run("messy", parent, depth, old=np.zeros((P, 7), np.int32))
+    run("oldkey", parent, depth, old=np.zeros((P, 9), np.int32), key="tree.ancestor")
+    # a chain that climbs the levels in order, then nodes hanging off it at mixed depths
+    chain = np.arange(-1, 9)
+    run("chain", chain, np.arange(0, 10), old=np.zeros((10, 10), np.int32))
+    bad = parent.copy()
+    bad[17] = P + 5
+    depth2 = depth.copy()
+    depth2[17] = 3
+    run("err_parent", bad, depth2, old=np.zeros((P, 7), np.int32))
+    deep = depth.copy()
+    deep[np.nonzero(parent >= 0)[0][0]] = 9
+    run("err_width", parent, deep, old=np.zeros((P, 7), np.int32))
+    np.savez_compressed(os.path.join(HERE, "torchref_ancestor.npz"), **out)
+
+
 if __name__ == "__main__":
     geometry_case()
     activation_case()
     tree_case()
+    ancestor_case()
     print("torchref fixtures written")

@@ -80,3 +80,41 @@ def test_install_dropin():
     assert sys.modules["diff_gaussian_rasterization_wodilate"] is dgr
     import diff_gaussian_rasterization_wodilate as alias
     assert alias.GaussianRasterizer is GaussianRasterizer
+
+
+def test_checkpoint_loader_on_cpu(tmp_path):
+    """LoG checkpoint parsing (LoG/utils/command.py:12-16 unwrap, the gaussian.* / tree.* keys) with a
+    stored ancestor table; the rebuild itself is a device pass and refuses a CPU device."""
+    import numpy as np
+    from filtergs_b200 import checkpoint as CK
+    from filtergs_b200 import synthetic as S
+    tr = S.lod_tree(P=500, seed=41, roots=2, max_depth=4, half_extent=20.0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a))  # noqa: E731
+    sd = {"gaussian.xyz": t(tr["xyz"]), "gaussian.scaling": t(tr["log_scales"]),
+          "gaussian.rotation": t(tr["rotations"]), "gaussian.opacity": t(tr["opacity_raw"]),
+          "gaussian.colors": t(tr["features_dc"]), "gaussian.shs": t(tr["shs_rest"]),
+          "tree.root_index": t(tr["roots"]).to(torch.int32), "tree.node_index": t(tr["node_index"]),
+          "tree.index_parent": t(tr["parent"]), "tree.depth": t(tr["level"]).to(torch.int8),
+          "tree.tree": t(tr["tree"]), "tree.ancestor": t(tr["ancestor_path"])}
+    for wrapped in (True, False):
+        path = tmp_path / f"c{int(wrapped)}.pth"
+        torch.save({"state_dict": sd, "global_iterations": 3} if wrapped else sd, path)
+        got = CK.load_statedict(str(path))
+        assert set(got) == set(sd)
+        scene = CK.tree_scene(got, device="cpu")
+        assert scene.P == 500 and scene.sh_degree == 1
+        assert torch.equal(scene.ancestor_path, t(tr["ancestor_path"]))
+        assert torch.equal(scene.opacity_raw, t(tr["opacity_raw"]).reshape(-1))
+    assert CK.tree_scene(sd, device="cpu", sh_degree=0).shs_rest is None
+    with pytest.raises(ValueError):
+        CK.tree_scene(sd, device="cpu", sh_degree=2)
+    with pytest.raises(ValueError):
+        CK.tree_scene(sd, device="cpu", rebuild_ancestors=True)   # the builder runs on a GPU only
+    bare = {k: v for k, v in sd.items() if k != "tree.ancestor"}
+    with pytest.raises(KeyError):
+        CK.tree_scene(bare, device="cpu", rebuild_ancestors=False)
+    with pytest.raises(KeyError):
+        CK.rebuild_ancestor_path({"tree.depth": sd["tree.depth"]})
+    assert CK.sh_degree_of(torch.zeros(4, 15, 3)) == 3 and CK.sh_degree_of(None) == 0
+    with pytest.raises(ValueError):
+        CK.sh_degree_of(torch.zeros(4, 5, 3))

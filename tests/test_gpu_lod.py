@@ -155,3 +155,67 @@ def test_filtergs_selected_render_vs_reference_pipeline(cuda, v2, ref):
     assert abs(mine[0] - theirs[0]) <= max(2, 1e-3 * theirs[0])
     assert (mine[5] != theirs[5]).float().mean().item() <= 1e-3
     assert (mine[1] - theirs[1]).abs().max().item() <= 2e-4
+
+
+# ---------------------------------------------------------------- ancestor_path builder, checkpoints
+ANCESTOR_CASES = ["consistent", "noold", "messy", "oldkey", "chain", "err_parent", "err_width"]
+
+
+@pytest.mark.parametrize("case", ANCESTOR_CASES)
+def test_ancestor_path_vs_reference(cuda, case):
+    """fgs_ancestor_path against apps/ancestor.py's own output (tests/golden/torchref_ancestor.npz):
+    consistent trees, trees whose depths disagree with their parents', and the two inputs on which
+    the reference raises."""
+    import os
+    from filtergs_b200 import checkpoint as CK
+    a = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "torchref_ancestor.npz"))
+    par, dep, width = _t(a[case + "_parent"]), _t(a[case + "_depth"]), int(a[case + "_width"])
+    if int(a[case + "_raises"]):
+        with pytest.raises(IndexError):
+            CK.ancestor_path_table(par, dep, width)
+    else:
+        out = CK.ancestor_path_table(par, dep, width)
+        assert np.array_equal(out.cpu().numpy(), a[case + "_ancestor"])
+
+
+def test_ancestor_path_large_tree_vs_generator(cuda):
+    """2M-node tree: the device table equals the generator's (which the CPU tests pin to apps/ancestor.py)."""
+    from filtergs_b200 import checkpoint as CK
+    tr = S.lod_tree(P=2_000_000, seed=3111, roots=4, max_depth=11, half_extent=300.0)
+    out = CK.ancestor_path_table(_t(tr["parent"]), _t(tr["level"]), tr["ancestor_path"].shape[1])
+    assert torch.equal(out, _t(tr["ancestor_path"]))
+
+
+def _log_state_dict(tr, with_ancestor):
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a))  # noqa: E731
+    sd = {"gaussian.xyz": t(tr["xyz"]), "gaussian.scaling": t(tr["log_scales"]),
+          "gaussian.rotation": t(tr["rotations"]), "gaussian.opacity": t(tr["opacity_raw"]),
+          "gaussian.colors": t(tr["features_dc"]), "gaussian.shs": t(tr["shs_rest"]),
+          "tree.root_index": t(tr["roots"]).to(torch.int32), "tree.node_index": t(tr["node_index"]),
+          "tree.index_parent": t(tr["parent"]), "tree.depth": t(tr["level"]).to(torch.int8),
+          "tree.tree": t(tr["tree"])}
+    if with_ancestor:
+        sd["tree.ancestor_path"] = t(tr["ancestor_path"])
+    return sd
+
+
+def test_checkpoint_without_ancestors_selects_like_the_arrays(cuda, tmp_path):
+    """A LoG checkpoint with no ancestor table: the loader rebuilds it on the device and the
+    FilterGS selection and render equal those of the scene built from the generator's arrays."""
+    from filtergs_b200 import checkpoint as CK
+    tr, cam = _tree(P=40000, seed=3112)
+    path = tmp_path / "log.pth"
+    torch.save({"state_dict": _log_state_dict(tr, with_ancestor=False), "global_iterations": 7}, path)
+    sd = CK.load_statedict(str(path))
+    scene = CK.tree_scene(sd, device="cuda")
+    ref_scene = lod.TreeScene.from_arrays(tr, device="cuda")
+    assert torch.equal(scene.ancestor_path, ref_scene.ancestor_path)
+    view, proj, cpos = _t(cam.viewmatrix), _t(cam.projmatrix), _t(cam.campos)
+    i1, c1, *_ = lod.select_filtergs(scene, view, proj, cam, 1.5, 0.1, 700.0)
+    i2, c2, *_ = lod.select_filtergs(ref_scene, view, proj, cam, 1.5, 0.1, 700.0)
+    n = int(c1.item())
+    assert n == int(c2.item()) and n > 100 and torch.equal(i1[:n], i2[:n])
+    bg = torch.zeros(3, device="cuda")
+    r1 = lod.render_selected(scene, i1, c1, view, proj, cpos, cam, bg)
+    r2 = lod.render_selected(ref_scene, i2, c2, view, proj, cpos, cam, bg)
+    assert r1[0] == r2[0] and torch.equal(r1[1], r2[1])

@@ -62,6 +62,20 @@ def test_ancestor_format_and_cut_order_vs_reference():
     assert len(cut) > 1000
 
 
+ANCESTOR_CASES = ["consistent", "noold", "messy", "oldkey", "chain", "err_parent", "err_width"]
+
+
+@pytest.mark.parametrize("case", ANCESTOR_CASES)
+def test_oracle_ancestor_path_vs_reference(case):
+    """rebuild_ancestor_path (apps/ancestor.py) on consistent, inconsistent and failing trees."""
+    a = _load("torchref_ancestor.npz")
+    out = O.ancestor_path(a[case + "_parent"], a[case + "_depth"], int(a[case + "_width"]))
+    if int(a[case + "_raises"]):
+        assert out is None
+    else:
+        assert out is not None and np.array_equal(out, a[case + "_ancestor"])
+
+
 # ---------------------------------------------------------------- reference CUDA build
 def _raster_fixtures():
     return sorted(glob.glob(os.path.join(GOLD, "ref_*.npz")))
