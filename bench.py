@@ -341,17 +341,22 @@ def profiled(fn, steps):
 def autotune(args, fn, key, rank):
     from filtergs_b200 import _lib
     if args.render_config:
-        _lib.set_render_config(*[int(x) for x in args.render_config.split(",")])
+        vals = [int(x) for x in args.render_config.split(",")]
+        _lib.set_render_config(*vals[:4])
+        if len(vals) > 4:
+            _lib.set_render_split(*vals[4:6])
         return None
     if args.no_autotune:
         return None
     from filtergs_b200.autotune import tune_render
     it = iter(range(1 << 30))
-    tuned, table = tune_render(lambda: fn(next(it)), key=key)
+    tuned, table = tune_render(lambda: fn(next(it)), key=key,
+                               splits=((0, 0), (512, 0), (512, 1), (512, 2), (512, 3), (4096, 2)))
     if rank == 0:
-        print(f"autotune {key[0]} (ppt,batch)->(fwd ms, bwd ms): " +
-              ", ".join(f"{k}:{v[0]:.3f}/{v[1]:.3f}" for k, v in sorted(table.items())), file=sys.stderr)
-    return list(tuned)
+        print(f"autotune {key[0]} (ppt,batch)->(fwd ms, bwd ms), then long-tile split->fwd ms: " +
+              ", ".join(f"{k}:{v[0]:.3f}/{v[1]:.3f}" for k, v in sorted(table.items(), key=lambda kv: str(kv[0]))),
+              file=sys.stderr)
+    return list(tuned) + list(_lib.get_render_split())
 
 
 def measure_plain(args, mod, scene, views, bg, dev, dist, rank, ours=True, clocks=None, profile=False):

@@ -99,6 +99,8 @@ SIGNATURES = {
     "fgs_densify_dense": (i32, [i32, vp, vp, vp, vp, vp, vp]),
     "fgs_adam_step": (i32, [C.POINTER(AdamArgs), vp, vp, vp]),
     "fgs_get_render_config": (i32, [vp]),
+    "fgs_set_render_split": (i32, [i32, i32]),
+    "fgs_get_render_split": (i32, [vp]),
     "fgs_forward_noalloc": (i32, [C.POINTER(RasterArgs), vp, vp, vp, vp, vp, C.POINTER(i64), vp]),
 }
 
@@ -157,6 +159,22 @@ def profile_read(reset=True):
 def set_render_config(fwd_ppt=2, fwd_batch=256, bwd_ppt=2, bwd_batch=256):
     check(lib().fgs_set_render_config(int(fwd_ppt), int(fwd_batch), int(bwd_ppt), int(bwd_batch)),
           "fgs_set_render_config")
+
+
+BAND_SHAPES = {0: (16, 2), 1: (8, 4), 2: (4, 4), 3: (4, 2)}
+
+
+def set_render_split(min_records=0, band_shape=0):
+    """Forward tiles with at least min_records pairs are rendered in bands (0: never) of
+    BAND_SHAPES[band_shape] pixels, one warp each."""
+    check(lib().fgs_set_render_split(int(min_records), int(band_shape)), "fgs_set_render_split")
+
+
+def get_render_split():
+    """(min_records, band_shape) of the forward's long-tile bands."""
+    cfg = (C.c_int * 2)()
+    check(lib().fgs_get_render_split(C.cast(cfg, vp)), "fgs_get_render_split")
+    return int(cfg[0]), int(cfg[1])
 
 
 def get_render_config():

@@ -62,6 +62,7 @@ struct Batch {
     std::vector<TileArgs> h_args;  // host copy of d_args_fwd ++ d_args_bwd (sources of pointer updates)
     uint32_t* d_begin;
     uint32_t* d_queue;
+    uint32_t* d_long;  // long-tile bins [32][total_tiles], then their 34 counters
     unsigned* d_err;
     uint32_t total_tiles;
     const float* background;
@@ -74,7 +75,7 @@ struct Batch {
 struct Layout {
     size_t total;
     std::vector<size_t> geom_off, img_off, bin_off, grad_off;
-    size_t args_off, begin_off, misc_off, cov_off;
+    size_t args_off, begin_off, misc_off, cov_off, long_off;
 };
 
 Layout plan(int P, int V, const fgs_view_args* views)
@@ -99,6 +100,11 @@ Layout plan(int P, int V, const fgs_view_args* views)
     off = align_up(off + 64);
     L.cov_off = off;
     off = align_up(off + sizeof(float) * 6 * (size_t)P);
+    size_t tiles = 0;
+    for (int v = 0; v < V; v++)
+        tiles += (size_t)((views[v].width + kTileX - 1) / kTileX) * ((views[v].height + kTileY - 1) / kTileY);
+    L.long_off = off;  // long-tile bins [32][tiles] + 34 counters
+    off = align_up(off + sizeof(uint32_t) * (32 * tiles + 34));
     L.total = off;
     return L;
 }
@@ -225,6 +231,7 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
     B->d_begin = reinterpret_cast<uint32_t*>(base + L.begin_off);
     B->d_queue = reinterpret_cast<uint32_t*>(base + L.misc_off);
     B->d_err = reinterpret_cast<unsigned*>(base + L.misc_off + 16);
+    B->d_long = reinterpret_cast<uint32_t*>(base + L.long_off);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (cudaMemcpyAsync(B->d_args_fwd, fa.data(), sizeof(TileArgs) * nviews, cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(B->d_args_bwd, ba.data(), sizeof(TileArgs) * nviews, cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -301,7 +308,8 @@ int fgs_batch_forward(void* handle, void* stream)
         cudaStreamWaitEvent(s, B->joined[i], 0);
     }
     StageTimer t(FGS_STAGE_RENDER_FWD, s);
-    launch_render_fwd_multi(B->d_args_fwd, B->d_begin, B->V, B->total_tiles, B->d_queue, B->d_err, s);
+    launch_render_fwd_multi(B->d_args_fwd, B->d_begin, B->V, B->total_tiles, B->d_queue, B->d_long,
+                            B->d_long + 32 * (size_t)B->total_tiles, B->d_err, s);
     return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
 }
 

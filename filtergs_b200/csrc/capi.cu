@@ -302,6 +302,8 @@ ImageState image_views(void* base, int W, int H)
     s.final_T = c.take<float>(N);
     s.n_contrib = c.take<uint32_t>(N);
     s.ranges = c.take<uint2>(T);
+    s.long_list = c.take<uint32_t>(32 * T);
+    s.long_ctr = c.take<uint32_t>(2 + 32);
     return s;
 }
 size_t image_bytes(int W, int H)
@@ -312,6 +314,8 @@ size_t image_bytes(int W, int H)
     c.take<float>(N);
     c.take<uint32_t>(N);
     c.take<uint2>(T);
+    c.take<uint32_t>(32 * T);
+    c.take<uint32_t>(2 + 32);
     return c.off;
 }
 BinState bin_views(void* base, long long K, int P) { return carve_bin(base, K, P).b; }
@@ -429,7 +433,7 @@ int fgs_forward_render(const fgs_raster_args* a, void* geom, void* image, void* 
     }
     {
         StageTimer t_render(FGS_STAGE_RENDER_FWD, s);
-        launch_render_fwd(W, H, im, bc.b, a->background, out_color, out_point_id, out_point_weight_pixel,
+        launch_render_fwd(W, H, im, bc.b, K, a->background, out_color, out_point_id, out_point_weight_pixel,
                           out_point_weight, stats && K > 0, g.err, s);
     }
     if ((st = check_launch())) return st;
@@ -690,9 +694,29 @@ long long fgs_launch_count(void) { return g_launches.load(std::memory_order_rela
 
 int fgs_set_render_config(int fwd_ppt, int fwd_batch, int bwd_ppt, int bwd_batch)
 {
-    const RenderConfig c{fwd_ppt, fwd_batch, bwd_ppt, bwd_batch};
+    const RenderConfig cur = get_render_config();
+    const RenderConfig c{fwd_ppt, fwd_batch, bwd_ppt, bwd_batch, cur.fwd_split, cur.fwd_band};
     if (!valid_render_config(c)) return FGS_ERR_ARG;
     set_render_config(c);
+    return FGS_OK;
+}
+
+int fgs_set_render_split(int min_records, int band_shape)
+{
+    RenderConfig c = get_render_config();
+    c.fwd_split = min_records;
+    c.fwd_band = band_shape;
+    if (!valid_render_config(c)) return FGS_ERR_ARG;
+    set_render_config(c);
+    return FGS_OK;
+}
+
+int fgs_get_render_split(int* cfg)
+{
+    if (!cfg) return FGS_ERR_ARG;
+    const RenderConfig c = get_render_config();
+    cfg[0] = c.fwd_split;
+    cfg[1] = c.fwd_band;
     return FGS_OK;
 }
 

@@ -59,6 +59,8 @@ struct ImageState {
     float* final_T;     // [N]
     uint32_t* n_contrib; // [N]
     uint2* ranges;      // [tiles]
+    uint32_t* long_list; // [32][tiles] tiles rendered in bands, binned by log2(records) (render.cu)
+    uint32_t* long_ctr;  // [34] 0: long tiles, 1: band queue, 2 + b: tiles in bin b
 };
 ImageState image_views(void* base, int W, int H);
 size_t image_bytes(int W, int H);
@@ -101,9 +103,10 @@ void launch_tile_sort(const GeomState& g, const BinState& b, long long K, int ti
                       const unsigned long long* n_dev = nullptr);
 void launch_ranges(const BinState& b, const ImageState& im, long long K, int num_tiles, cudaStream_t s,
                    const unsigned long long* n_dev = nullptr);
-void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, const float* bg, float* out_color,
-                       int* point_id, float* pw_pixel, float* point_weight, bool stats, unsigned* err,
-                       cudaStream_t s);
+// K: the pair count (or capacity) of b, for the statistics' zeroing when long tiles are split.
+void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, long long K, const float* bg,
+                       float* out_color, int* point_id, float* pw_pixel, float* point_weight, bool stats,
+                       unsigned* err, cudaStream_t s);
 void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, const float* bg,
                        const float* dL_dpix, int consistent, unsigned* err, cudaStream_t s);
 // Per-Gaussian backward over the visible Gaussians.  Screen-space gradients come from
@@ -166,14 +169,17 @@ struct TileArgs {
 // Persistent multi-view compositing over the tiles of `nviews` views; begin[v]
 // is the first work item of view v (begin[nviews] == total_tiles); queue is a
 // device counter (zeroed here).
+// long_list: [32 * total_tiles] scratch, long_ctr: [34] scratch (bands of long tiles; statistics must be off).
 void launch_render_fwd_multi(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total_tiles,
-                             uint32_t* queue, unsigned* err, cudaStream_t s);
+                             uint32_t* queue, uint32_t* long_list, uint32_t* long_ctr, unsigned* err, cudaStream_t s);
 void launch_render_bwd_multi(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total_tiles,
                              uint32_t* queue, int consistent, unsigned* err, cudaStream_t s);
 
 // Render kernel shape: pixels per thread {1,2,4} and records per shared-memory batch {64,128,256}.
 struct RenderConfig {
     int fwd_ppt, fwd_batch, bwd_ppt, bwd_batch;
+    int fwd_split;  // forward: tiles with at least this many records are rendered in bands (0: never)
+    int fwd_band;   // band shape: 0 = 16x2, 1 = 8x4, 2 = 4x4, 3 = 4x2 pixels per warp
 };
 bool valid_render_config(const RenderConfig& c);
 void set_render_config(const RenderConfig& c);

@@ -122,7 +122,7 @@ int fgs_forward_noalloc(const fgs_raster_args* a, int* radii, float* out_color, 
         launch_tile_sort(g, b, K, tbits, p.W, p.H, s);
     }
     launch_ranges(b, im, K, num_tiles, s);
-    launch_render_fwd(p.W, p.H, im, b, a->background, out_color, out_point_id, out_point_weight_pixel,
+    launch_render_fwd(p.W, p.H, im, b, K, a->background, out_color, out_point_id, out_point_weight_pixel,
                       out_point_weight, false, g.err, s);
     cudaMemcpyAsync(&err, g.err, sizeof(err), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) return FGS_ERR_CUDA;

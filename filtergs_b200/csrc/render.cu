@@ -153,6 +153,90 @@ struct BwdSmem {
 };
 
 // ---------------------------------------------------------------- forward
+// One (pixel, record) step of the compositing loop (forward.cu:466-544), in two
+// parts.  fwd_alpha: the Gaussian's alpha at the pixel centre, or 0 where the
+// reference skips the record (power > 0, alpha < 1/255); it does not depend on
+// the pixel's state, so a renderer may evaluate several records ahead.
+// fwd_accumulate: early termination below T = 1e-4, the colour and
+// transmittance update and the pixel's strongest contributor; returns the
+// weight T * alpha the record took (> 0), or 0 when it did not contribute.
+//
+// The multiply-adds are spelled out with round-to-nearest intrinsics (the
+// contraction a compiler would pick for the reference's expressions), so that
+// the compiler cannot fuse them differently in different renderers: the tile
+// path at any pixels-per-thread and the band path produce the same bits.
+__device__ __forceinline__ float fwd_alpha(const float4 ra, const float4 rb, float pxf, float pyf)
+{
+    const float dx = ra.x - pxf, dy = ra.y - pyf;
+    // -0.5 * (a dx^2 + c dy^2) - b dx dy; the dx-only products are shared by the
+    // pixels of one column (several per thread on the tile path)
+    const float q = __fmaf_rn(__fmul_rn(rb.x, dy), dy, __fmul_rn(__fmul_rn(ra.z, dx), dx));
+    const float power = __fmaf_rn(-0.5f, q, -__fmul_rn(__fmul_rn(ra.w, dx), dy));
+    if (power > 0.0f) return 0.f;
+    const float alpha = fminf(0.99f, __fmul_rn(rb.y, expf(power)));
+    return alpha < 1.0f / 255.0f ? 0.f : alpha;
+}
+
+__device__ __forceinline__ float fwd_accumulate(float alpha, const float4 rb, const PairRecord& rec,
+                                                uint32_t position, float& T, float (&C)[3], float& wmax, int& maxid,
+                                                uint32_t& last, bool& done)
+{
+    if (done || alpha == 0.f) return 0.f;
+    const float test_T = __fmul_rn(T, 1.0f - alpha);
+    if (test_T < 0.0001f) {
+        done = true;
+        return 0.f;
+    }
+    const float4 rc = rec.c;
+    C[0] = __fmaf_rn(__fmul_rn(rb.z, alpha), T, C[0]);
+    C[1] = __fmaf_rn(__fmul_rn(rb.w, alpha), T, C[1]);
+    C[2] = __fmaf_rn(__fmul_rn(rc.x, alpha), T, C[2]);
+    const float w = __fmul_rn(T, alpha);
+    if (w > wmax) {
+        wmax = w;
+        maxid = __float_as_int(rc.y);
+    }
+    T = test_T;
+    last = position;
+    return w;
+}
+
+// fwd_alpha + fwd_accumulate in one pass with early exits (the tile path: no
+// record is evaluated ahead), the same arithmetic.  A contribution also goes into
+// the caller's per-record sums (max weight, weight sum, count).
+__device__ __forceinline__ void fwd_pixel_step(const float4 ra, const float4 rb, const PairRecord& rec, float pxf,
+                                               float pyf, uint32_t position, float& T, float (&C)[3], float& wmax,
+                                               int& maxid, uint32_t& last, bool& done, float& wj, float& ksum,
+                                               uint32_t& kc)
+{
+    if (done) return;
+    const float dx = ra.x - pxf, dy = ra.y - pyf;
+    const float q = __fmaf_rn(__fmul_rn(rb.x, dy), dy, __fmul_rn(__fmul_rn(ra.z, dx), dx));
+    const float power = __fmaf_rn(-0.5f, q, -__fmul_rn(__fmul_rn(ra.w, dx), dy));
+    if (power > 0.0f) return;
+    const float alpha = fminf(0.99f, __fmul_rn(rb.y, expf(power)));
+    if (alpha < 1.0f / 255.0f) return;
+    const float test_T = __fmul_rn(T, 1.0f - alpha);
+    if (test_T < 0.0001f) {
+        done = true;
+        return;
+    }
+    const float4 rc = rec.c;
+    C[0] = __fmaf_rn(__fmul_rn(rb.z, alpha), T, C[0]);
+    C[1] = __fmaf_rn(__fmul_rn(rb.w, alpha), T, C[1]);
+    C[2] = __fmaf_rn(__fmul_rn(rc.x, alpha), T, C[2]);
+    const float w = __fmul_rn(T, alpha);
+    if (w > wmax) {
+        wmax = w;
+        maxid = __float_as_int(rc.y);
+    }
+    wj = fmaxf(wj, w);
+    ksum += w;
+    kc += 1;
+    T = test_T;
+    last = position;
+}
+
 // One tile.  Callers guarantee every thread of the CTA is synchronised on
 // entry and that no bulk copy is in flight.  `gb` counts the record batches
 // this CTA has ever waited for: batch g lives in buffer g % 3 and completes
@@ -160,7 +244,7 @@ struct BwdSmem {
 // once per CTA and keep their phase across tiles.
 template <int PPT, int kBatch>
 __device__ __forceinline__ void render_fwd_tile(FwdSmem<kBatch>& sm, const TileArgs& a, int tile, uint32_t& gb,
-                                                unsigned* err)
+                                                uint32_t split_min, unsigned* err)
 {
     constexpr int NT = 256 / PPT;
     const int tid = threadIdx.x;
@@ -171,6 +255,7 @@ __device__ __forceinline__ void render_fwd_tile(FwdSmem<kBatch>& sm, const TileA
     const int px = bx * kTileX + lx;
     const uint2 range = a.ranges[tile];
     const uint32_t n = range.y - range.x;
+    if (split_min && n >= split_min) return;  // rendered in bands (render_fwd_band)
     const int nb = (int)((n + kBatch - 1) / kBatch);
     const bool stats = a.kv_sum != nullptr;
     const PairRecord* recs = a.recs;
@@ -236,33 +321,9 @@ __device__ __forceinline__ void render_fwd_tile(FwdSmem<kBatch>& sm, const TileA
                     float wj = 0.f, ksum = 0.f;
                     uint32_t kc = 0;
 #pragma unroll
-                    for (int k = 0; k < PPT; k++) {
-                        if (done[k]) continue;
-                        const float2 d = {ra.x - pxf, ra.y - pyf[k]};
-                        const float power = -0.5f * (ra.z * d.x * d.x + rb.x * d.y * d.y) - ra.w * d.x * d.y;
-                        if (power > 0.0f) continue;
-                        const float alpha = min(0.99f, rb.y * exp(power));
-                        if (alpha < 1.0f / 255.0f) continue;
-                        const float test_T = T[k] * (1 - alpha);
-                        if (test_T < 0.0001f) {
-                            done[k] = true;
-                            continue;
-                        }
-                        const float4 rc = R[j].c;
-                        C[k][0] += rb.z * alpha * T[k];
-                        C[k][1] += rb.w * alpha * T[k];
-                        C[k][2] += rc.x * alpha * T[k];
-                        const float w = T[k] * alpha;
-                        if (w > wmax[k]) {
-                            wmax[k] = w;
-                            maxid[k] = __float_as_int(rc.y);
-                        }
-                        wj = fmaxf(wj, w);
-                        ksum += w;
-                        kc += 1;
-                        T[k] = test_T;
-                        last[k] = position;
-                    }
+                    for (int k = 0; k < PPT; k++)
+                        fwd_pixel_step(ra, rb, R[j], pxf, pyf[k], position, T[k], C[k], wmax[k], maxid[k], last[k],
+                                       done[k], wj, ksum, kc);
                     bool ad = true;
 #pragma unroll
                     for (int k = 0; k < PPT; k++) ad = ad && done[k];
@@ -338,9 +399,9 @@ __device__ __forceinline__ void render_fwd_tile(FwdSmem<kBatch>& sm, const TileA
             const int pix = W * py + px;
             a.final_T[pix] = T[k];
             a.n_contrib[pix] = last[k];
-            a.out_color[pix] = C[k][0] + T[k] * a.bg[0];
-            a.out_color[H * W + pix] = C[k][1] + T[k] * a.bg[1];
-            a.out_color[2 * H * W + pix] = C[k][2] + T[k] * a.bg[2];
+            a.out_color[pix] = __fmaf_rn(T[k], a.bg[0], C[k][0]);
+            a.out_color[H * W + pix] = __fmaf_rn(T[k], a.bg[1], C[k][1]);
+            a.out_color[2 * H * W + pix] = __fmaf_rn(T[k], a.bg[2], C[k][2]);
             if (a.out_point_id) a.out_point_id[pix] = maxid[k];
             if (a.out_pw_pixel) a.out_pw_pixel[pix] = wmax[k];
         }
@@ -362,21 +423,34 @@ __device__ __forceinline__ void fwd_smem_init(FwdSmem<kBatch>& sm, int NT)
     __syncthreads();
 }
 
+// Resident CTAs per SM the forward kernels are compiled for (a register cap of
+// 65536 / (CTAs x threads)): 24 warps per SM at 2 pixels per thread, 20 at 4.
+template <int PPT>
+constexpr int fwd_min_ctas() { return PPT == 1 ? 3 : (PPT == 2 ? 6 : 10); }
+
 template <int PPT, int kBatch>
-__global__ void __launch_bounds__(256 / PPT) render_fwd_kernel(TileArgs a, unsigned* err)
+__global__ void __launch_bounds__(256 / PPT, fwd_min_ctas<PPT>())
+    render_fwd_kernel(TileArgs a, uint32_t split_min, unsigned* err)
 {
     __shared__ __align__(128) FwdSmem<kBatch> sm;
     fwd_smem_init(sm, 256 / PPT);
     uint32_t gb = 0;
-    render_fwd_tile<PPT, kBatch>(sm, a, blockIdx.x, gb, err);
+    render_fwd_tile<PPT, kBatch>(sm, a, blockIdx.x, gb, split_min, err);
 }
 
 // Persistent multi-view forward: CTAs pop work items from one queue; item i is
 // tile (i - begin[v]) of view v.  Views are laid out in the caller's order.
+__device__ __forceinline__ int view_of(const uint32_t* __restrict__ begin, int nviews, uint32_t item)
+{
+    int v = 0;
+    while (v + 1 < nviews && begin[v + 1] <= item) v++;
+    return v;
+}
+
 template <int PPT, int kBatch>
-__global__ void __launch_bounds__(256 / PPT)
+__global__ void __launch_bounds__(256 / PPT, fwd_min_ctas<PPT>())
     render_fwd_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin, int nviews,
-                            uint32_t total, uint32_t* queue, unsigned* err)
+                            uint32_t total, uint32_t* queue, uint32_t split_min, unsigned* err)
 {
     __shared__ __align__(128) FwdSmem<kBatch> sm;
     __shared__ uint32_t s_item;
@@ -387,11 +461,258 @@ __global__ void __launch_bounds__(256 / PPT)
         __syncthreads();
         const uint32_t item = s_item;
         if (item >= total) break;
-        int v = 0;
-        while (v + 1 < nviews && begin[v + 1] <= item) v++;
+        const int v = view_of(begin, nviews, item);
         const TileArgs a = views[v];
-        render_fwd_tile<PPT, kBatch>(sm, a, (int)(item - begin[v]), gb, err);
+        render_fwd_tile<PPT, kBatch>(sm, a, (int)(item - begin[v]), gb, split_min, err);
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- long tiles in bands
+// A tile with a long record list (dense small splats: distant LoD levels, a
+// horizon) is the critical path of the one-CTA-per-tile render: its few warps
+// walk every record while the rest of the GPU has finished.  Tiles with at
+// least split_min records are rendered instead as bands of BW x BH pixels, one
+// warp each and every warp on its own, longest tiles first.  The warp pulls the
+// tile's records through its own ring of kBandRing shared-memory chunks of 32
+// records (one bulk copy per chunk, completed on the slot's mbarrier, two chunks
+// in flight), culls each chunk against its band (one record per lane, then a
+// ballot), and composites the touched records with the tile path's per-pixel
+// functions, one pixel per lane (lanes past BW x BH only cull).  A long tile so
+// spreads over 256 / (BW BH) warps on different SMs, each culling against a
+// small rectangle, and each warp evaluates the alphas of two touched records
+// before it accumulates them, so that the exp of one overlaps the other's
+// arithmetic.  Every pixel composites the same records in the same order with
+// the same arithmetic as on the tile path.  Per record, a contributing lane
+// folds its weight into the record's shared slot; the slots leave once per chunk
+// (atomicMax into the per-Gaussian max weight, atomicAdd into the statistics,
+// which are zeroed before the launch when on).
+//
+// Order: long tiles are binned by floor(log2(records)) (kLongBuckets bins of
+// capacity `cap` each); the band queue hands out the bins from the longest down.
+constexpr int kBandWarps = 8;  // warps per CTA of the band kernel
+constexpr int kBandRing = 3;   // chunks per warp: one being composited, two in flight
+constexpr int kLongBuckets = 32;
+
+struct BandSmem {
+    PairRecord rec[kBandRing][32];
+    uint64_t bar[kBandRing];
+    uint32_t wmax[32];  // per record of the current chunk: max weight over this band's pixels
+    float ksum[32];     // statistics: weight sum and count over this band's pixels
+    uint32_t kcnt[32];
+};
+
+__device__ __forceinline__ void band_smem_init(BandSmem& sm)
+{
+    const int lane = threadIdx.x & 31;
+    sm.wmax[lane] = 0;
+    sm.ksum[lane] = 0.f;
+    sm.kcnt[lane] = 0;
+    if (lane == 0) {
+        for (int i = 0; i < kBandRing; i++) mbar_init(&sm.bar[i], 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void band_fold(BandSmem& sm, uint32_t j, float w, bool stats)
+{
+    if (w > 0.f) {
+        atomicMax(&sm.wmax[j], __float_as_uint(w));
+        if (stats) {
+            atomicAdd(&sm.ksum[j], w);
+            atomicAdd(&sm.kcnt[j], 1u);
+        }
+    }
+}
+
+// `g` counts the chunks this warp has ever waited for: chunk g lives in slot
+// g % kBandRing and completes phase (g / kBandRing) & 1 of that slot's barrier.
+template <int BW, int BH>
+__device__ __forceinline__ void render_fwd_band(BandSmem& sm, const TileArgs& a, int tile, int band, uint32_t& g,
+                                                unsigned* err)
+{
+    static_assert(BW * BH <= 32 && kTileX % BW == 0 && kTileY % BH == 0, "band shape");
+    constexpr int kPerRow = kTileX / BW;
+    const int lane = threadIdx.x & 31;
+    const int W = a.W, H = a.H;
+    const int gx = (W + kTileX - 1) / kTileX;
+    const int bx = tile % gx, by = tile / gx;
+    const int ox = bx * kTileX + (band % kPerRow) * BW, oy = by * kTileY + (band / kPerRow) * BH;
+    const bool mine = lane < BW * BH;
+    const int px = ox + lane % BW, py = oy + lane / BW;
+    const uint2 range = a.ranges[tile];
+    const uint32_t n = range.y - range.x;
+    const uint32_t nc = (n + 31) / 32;
+    const bool stats = a.kv_sum != nullptr;
+    const PairRecord* recs = a.recs + range.x;
+    const float pxf = (float)px, pyf = (float)py;
+    const float rx0 = (float)ox, rx1 = rx0 + (BW - 1);
+    const float ry0 = (float)oy, ry1 = ry0 + (BH - 1);
+    float T = 1.0f, C[3] = {0.f, 0.f, 0.f}, wmax = 0.f;
+    uint32_t last = 0;
+    int maxid = -1;
+    bool done = !(mine && px < W && py < H);
+
+    if (!__all_sync(0xffffffffu, done)) {
+        uint32_t issued = nc < (uint32_t)(kBandRing - 1) ? nc : (uint32_t)(kBandRing - 1);
+        if (lane == 0)
+            for (uint32_t c = 0; c < issued; c++) {
+                const uint32_t q = (g + c) % kBandRing;
+                issue_batch(sm.rec[q], &sm.bar[q], recs, c * 32, min(32u, n - c * 32));
+            }
+        uint32_t c = 0;
+        for (; c < nc; c++) {
+            // keep two chunks in flight: the slot refilled here was released at the end of chunk c-1
+            if (lane == 0 && issued < nc) {
+                const uint32_t q = (g + issued) % kBandRing;
+                issue_batch(sm.rec[q], &sm.bar[q], recs, issued * 32, min(32u, n - issued * 32));
+            }
+            if (issued < nc) issued++;
+            const uint32_t q = (g + c) % kBandRing;
+            if (!mbar_wait(&sm.bar[q], ((g + c) / kBandRing) & 1, err)) done = true;
+            const PairRecord* R = sm.rec[q];
+            const uint32_t k0 = c * 32;
+            const uint32_t e = k0 + lane;
+            bool t = false;
+            if (e < n) {
+                const float4 ea = R[lane].a, eb = R[lane].b;
+                t = may_touch(ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, rx0, rx1, ry0, ry1);
+            }
+            uint32_t live = __ballot_sync(0xffffffffu, t);
+            while (live) {
+                const uint32_t j1 = (uint32_t)(__ffs(live) - 1);
+                live &= live - 1;
+                const bool two = live != 0;
+                const uint32_t j2 = two ? (uint32_t)(__ffs(live) - 1) : j1;
+                if (two) live &= live - 1;
+                const float4 ra1 = R[j1].a, rb1 = R[j1].b, ra2 = R[j2].a, rb2 = R[j2].b;
+                const float al1 = done ? 0.f : fwd_alpha(ra1, rb1, pxf, pyf);
+                const float al2 = (done || !two) ? 0.f : fwd_alpha(ra2, rb2, pxf, pyf);
+                band_fold(sm, j1, fwd_accumulate(al1, rb1, R[j1], k0 + j1 + 1, T, C, wmax, maxid, last, done),
+                          stats);
+                band_fold(sm, j2, fwd_accumulate(al2, rb2, R[j2], k0 + j2 + 1, T, C, wmax, maxid, last, done),
+                          stats);
+            }
+            __syncwarp();
+            const uint32_t wm = sm.wmax[lane];
+            if (wm) {
+                if (a.out_point_weight)
+                    atomicMax(reinterpret_cast<unsigned*>(a.out_point_weight) + __float_as_int(R[lane].c.y), wm);
+                sm.wmax[lane] = 0;
+            }
+            if (stats && e < n && sm.kcnt[lane]) {
+                atomicAdd(a.kv_sum + range.x + e, sm.ksum[lane]);
+                atomicAdd(a.kv_cnt + range.x + e, sm.kcnt[lane]);
+                sm.ksum[lane] = 0.f;
+                sm.kcnt[lane] = 0;
+            }
+            __syncwarp();  // every lane is done with slot q before it is refilled
+            if (__all_sync(0xffffffffu, done)) {
+                c++;
+                break;
+            }
+        }
+        // drain the chunks still in flight, so that every slot's phase count stays in step
+        if (lane == 0)
+            for (uint32_t k = c; k < issued; k++) mbar_wait(&sm.bar[(g + k) % kBandRing], ((g + k) / kBandRing) & 1, err);
+        __syncwarp();
+        g += issued;
+    }
+    if (mine && px < W && py < H) {
+        const int pix = W * py + px;
+        a.final_T[pix] = T;
+        a.n_contrib[pix] = last;
+        a.out_color[pix] = __fmaf_rn(T, a.bg[0], C[0]);
+        a.out_color[H * W + pix] = __fmaf_rn(T, a.bg[1], C[1]);
+        a.out_color[2 * H * W + pix] = __fmaf_rn(T, a.bg[2], C[2]);
+        if (a.out_point_id) a.out_point_id[pix] = maxid;
+        if (a.out_pw_pixel) a.out_pw_pixel[pix] = wmax;
+    }
+}
+
+__device__ __forceinline__ void long_tile_push(uint32_t n, uint32_t id, uint32_t cap, uint32_t* __restrict__ list,
+                                               uint32_t* __restrict__ ctr)
+{
+    const int b = 31 - __clz(n);
+    const uint32_t slot = atomicAdd(ctr + 2 + b, 1u);
+    list[(size_t)b * cap + slot] = id;
+    atomicAdd(ctr, 1u);
+}
+
+// The long tiles of one view (ids are tiles) or of a multi-view batch (ids are
+// global work items, mapped to (view, tile) by begin[]).  ctr: [0] long tiles,
+// [1] band queue, [2 + b] tiles in bin b.
+__global__ void long_tiles_kernel(const uint2* __restrict__ ranges, uint32_t num_tiles, uint32_t split_min,
+                                  uint32_t* __restrict__ list, uint32_t* __restrict__ ctr)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= num_tiles) return;
+    const uint2 r = ranges[t];
+    if (r.y - r.x >= split_min) long_tile_push(r.y - r.x, t, num_tiles, list, ctr);
+}
+
+__global__ void long_tiles_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin,
+                                        int nviews, uint32_t total, uint32_t split_min, uint32_t* __restrict__ list,
+                                        uint32_t* __restrict__ ctr)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int v = view_of(begin, nviews, i);
+    const uint2 r = views[v].ranges[i - begin[v]];
+    if (r.y - r.x >= split_min) long_tile_push(r.y - r.x, i, total, list, ctr);
+}
+
+// Band item -> long tile id, longest bins first.  False when the queue is empty.
+template <int kBandsPerTile>
+__device__ __forceinline__ bool next_band(uint32_t* ctr, const uint32_t* __restrict__ list, uint32_t cap,
+                                          uint32_t& id, int& band)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(ctr + 1, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    const uint32_t total = *(volatile uint32_t*)ctr;
+    if (item >= total * kBandsPerTile) return false;
+    uint32_t r = item / kBandsPerTile;
+    band = (int)(item % kBandsPerTile);
+    for (int b = kLongBuckets - 1; b >= 0; b--) {
+        const uint32_t c = *(volatile uint32_t*)(ctr + 2 + b);
+        if (r < c) {
+            id = list[(size_t)b * cap + r];
+            return true;
+        }
+        r -= c;
+    }
+    return false;
+}
+
+template <int BW, int BH>
+__global__ void __launch_bounds__(32 * kBandWarps)
+    render_fwd_band_kernel(TileArgs a, const uint32_t* __restrict__ list, uint32_t* ctr, uint32_t cap, unsigned* err)
+{
+    __shared__ __align__(128) BandSmem sm[kBandWarps];
+    BandSmem& my = sm[threadIdx.x >> 5];
+    band_smem_init(my);
+    uint32_t g = 0, id = 0;
+    int band = 0;
+    while (next_band<kTileX * kTileY / (BW * BH)>(ctr, list, cap, id, band))
+        render_fwd_band<BW, BH>(my, a, (int)id, band, g, err);
+}
+
+template <int BW, int BH>
+__global__ void __launch_bounds__(32 * kBandWarps)
+    render_fwd_band_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin, int nviews,
+                                 const uint32_t* __restrict__ list, uint32_t* ctr, uint32_t cap, unsigned* err)
+{
+    __shared__ __align__(128) BandSmem sm[kBandWarps];
+    BandSmem& my = sm[threadIdx.x >> 5];
+    band_smem_init(my);
+    uint32_t g = 0, id = 0;
+    int band = 0;
+    while (next_band<kTileX * kTileY / (BW * BH)>(ctr, list, cap, id, band)) {
+        const int v = view_of(begin, nviews, id);
+        render_fwd_band<BW, BH>(my, views[v], (int)(id - begin[v]), band, g, err);
     }
 }
 
@@ -618,18 +939,63 @@ __global__ void __launch_bounds__(256 / PPT)
 }  // namespace
 
 namespace {
-RenderConfig g_cfg{2, 256, 2, 256};
+RenderConfig g_cfg{2, 256, 2, 256, 0, 0};
+
+// Band shapes (fgs_set_render_split): 0 = 16x2, 1 = 8x4, 2 = 4x4, 3 = 4x2 pixels per warp.
+template <int BW, int BH>
+void band_launch(const TileArgs& a, const uint32_t* list, uint32_t* ctr, uint32_t cap, unsigned* err, cudaStream_t s)
+{
+    render_fwd_band_kernel<BW, BH><<<resident_ctas(render_fwd_band_kernel<BW, BH>, 32 * kBandWarps), 32 * kBandWarps,
+                                     0, s>>>(a, list, ctr, cap, err);
+}
+void launch_band_kernel(int shape, const TileArgs& a, const uint32_t* list, uint32_t* ctr, uint32_t cap, unsigned* err,
+                        cudaStream_t s)
+{
+    if (shape == 1) band_launch<8, 4>(a, list, ctr, cap, err, s);
+    else if (shape == 2) band_launch<4, 4>(a, list, ctr, cap, err, s);
+    else if (shape == 3) band_launch<4, 2>(a, list, ctr, cap, err, s);
+    else band_launch<16, 2>(a, list, ctr, cap, err, s);
+}
+template <int BW, int BH>
+void band_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, const uint32_t* list, uint32_t* ctr,
+                       uint32_t cap, unsigned* err, cudaStream_t s)
+{
+    render_fwd_band_multi_kernel<BW, BH>
+        <<<resident_ctas(render_fwd_band_multi_kernel<BW, BH>, 32 * kBandWarps), 32 * kBandWarps, 0, s>>>(
+            views, begin, nviews, list, ctr, cap, err);
+}
+void launch_band_multi_kernel(int shape, const TileArgs* views, const uint32_t* begin, int nviews,
+                              const uint32_t* list, uint32_t* ctr, uint32_t cap, unsigned* err, cudaStream_t s)
+{
+    if (shape == 1) band_multi_launch<8, 4>(views, begin, nviews, list, ctr, cap, err, s);
+    else if (shape == 2) band_multi_launch<4, 4>(views, begin, nviews, list, ctr, cap, err, s);
+    else if (shape == 3) band_multi_launch<4, 2>(views, begin, nviews, list, ctr, cap, err, s);
+    else band_multi_launch<16, 2>(views, begin, nviews, list, ctr, cap, err, s);
+}
 
 template <int PPT, int B>
-void fwd_launch(int grid, const ImageState& im, const BinState& b, int W, int H, const float* bg, float* out_color,
-                int* point_id, float* pw_pixel, float* point_weight, bool stats, unsigned* err, cudaStream_t s)
+void fwd_launch(int grid, const ImageState& im, const BinState& b, long long K, int W, int H, const float* bg,
+                float* out_color, int* point_id, float* pw_pixel, float* point_weight, bool stats, int split,
+                int band_shape, unsigned* err, cudaStream_t s)
 {
     TileArgs a{};
     a.ranges = im.ranges; a.recs = b.rec; a.W = W; a.H = H; a.bg = bg;
     a.out_color = out_color; a.final_T = im.final_T; a.n_contrib = im.n_contrib; a.out_point_id = point_id;
     a.out_pw_pixel = pw_pixel; a.out_point_weight = point_weight;
     a.kv_sum = stats ? b.kv_sum : nullptr; a.kv_cnt = stats ? b.kv_cnt : nullptr;
-    render_fwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(a, err);
+    if (split > 0) {
+        // long tiles first, in bands; the tile kernel then skips them
+        cudaMemsetAsync(im.long_ctr, 0, (2 + kLongBuckets) * sizeof(uint32_t), s);
+        if (stats && K > 0) {
+            cudaMemsetAsync(b.kv_sum, 0, sizeof(float) * (size_t)K, s);
+            cudaMemsetAsync(b.kv_cnt, 0, sizeof(uint32_t) * (size_t)K, s);
+        }
+        long_tiles_kernel<<<(grid + 255) / 256, 256, 0, s>>>(im.ranges, (uint32_t)grid, (uint32_t)split, im.long_list,
+                                                             im.long_ctr);
+        launch_band_kernel(band_shape, a, im.long_list, im.long_ctr, (uint32_t)grid, err, s);
+        note_launches(2);
+    }
+    render_fwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(a, (uint32_t)(split > 0 ? split : 0), err);
 }
 
 // Dynamic shared memory of a backward kernel instantiation (opted in once per process
@@ -679,33 +1045,39 @@ bool valid_render_config(const RenderConfig& c)
 {
     auto ok_p = [](int v) { return v == 1 || v == 2 || v == 4; };
     auto ok_b = [](int v) { return v == 64 || v == 128 || v == 256; };
-    return ok_p(c.fwd_ppt) && ok_p(c.bwd_ppt) && ok_b(c.fwd_batch) && ok_b(c.bwd_batch);
+    return ok_p(c.fwd_ppt) && ok_p(c.bwd_ppt) && ok_b(c.fwd_batch) && ok_b(c.bwd_batch) && c.fwd_split >= 0 &&
+           c.fwd_band >= 0 && c.fwd_band <= 3;
 }
 void set_render_config(const RenderConfig& c) { g_cfg = c; }
 RenderConfig get_render_config() { return g_cfg; }
 
-void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, const float* bg, float* out_color,
-                       int* point_id, float* pw_pixel, float* point_weight, bool stats, unsigned* err,
-                       cudaStream_t s)
+void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, long long K, const float* bg,
+                       float* out_color, int* point_id, float* pw_pixel, float* point_weight, bool stats,
+                       unsigned* err, cudaStream_t s)
 {
     const int gx = (W + kTileX - 1) / kTileX, gy = (H + kTileY - 1) / kTileY;
     const RenderConfig c = g_cfg;
-    FGS_RENDER_DISPATCH(fwd_launch, c.fwd_ppt, c.fwd_batch, gx * gy, im, b, W, H, bg, out_color, point_id, pw_pixel,
-                        point_weight, stats, err, s);
+    FGS_RENDER_DISPATCH(fwd_launch, c.fwd_ppt, c.fwd_batch, gx * gy, im, b, K, W, H, bg, out_color, point_id,
+                        pw_pixel, point_weight, stats, c.fwd_split, c.fwd_band, err, s);
     note_launches(1);
 }
 
 namespace {
 template <int PPT, int B>
 void fwd_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total, uint32_t* queue,
-                      unsigned* err, cudaStream_t s)
+                      uint32_t* long_list, uint32_t* long_ctr, int split, int band_shape, unsigned* err,
+                      cudaStream_t s)
 {
-    int dev = 0, sms = 148, per_sm = 1;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_fwd_multi_kernel<PPT, B>, 256 / PPT, 0);
-    const int grid = sms * (per_sm > 0 ? per_sm : 1);
-    render_fwd_multi_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(views, begin, nviews, total, queue, err);
+    if (split > 0) {
+        cudaMemsetAsync(long_ctr, 0, (2 + kLongBuckets) * sizeof(uint32_t), s);
+        long_tiles_multi_kernel<<<(total + 255) / 256, 256, 0, s>>>(views, begin, nviews, total, (uint32_t)split,
+                                                                    long_list, long_ctr);
+        launch_band_multi_kernel(band_shape, views, begin, nviews, long_list, long_ctr, total, err, s);
+        note_launches(2);
+    }
+    const int grid = (int)resident_ctas(render_fwd_multi_kernel<PPT, B>, 256 / PPT);
+    render_fwd_multi_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(views, begin, nviews, total, queue,
+                                                               (uint32_t)(split > 0 ? split : 0), err);
 }
 
 template <int PPT, int B>
@@ -724,11 +1096,12 @@ void bwd_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, 
 }  // namespace
 
 void launch_render_fwd_multi(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total_tiles,
-                             uint32_t* queue, unsigned* err, cudaStream_t s)
+                             uint32_t* queue, uint32_t* long_list, uint32_t* long_ctr, unsigned* err, cudaStream_t s)
 {
     cudaMemsetAsync(queue, 0, sizeof(uint32_t), s);
     const RenderConfig c = g_cfg;
-    FGS_RENDER_DISPATCH(fwd_multi_launch, c.fwd_ppt, c.fwd_batch, views, begin, nviews, total_tiles, queue, err, s);
+    FGS_RENDER_DISPATCH(fwd_multi_launch, c.fwd_ppt, c.fwd_batch, views, begin, nviews, total_tiles, queue, long_list,
+                        long_ctr, c.fwd_split, c.fwd_band, err, s);
     note_launches(1);
 }
 

@@ -126,3 +126,27 @@ def test_batched_set_io_retargets_captured_graph(cuda):
         assert torch.equal(br.grad[k], 2.0 * g0[k]), k
     with pytest.raises(ValueError):
         br.set_io(0, torch.empty(3, 5, 5, device="cuda"))
+
+
+def test_batched_long_tile_bands(cuda):
+    """The multi-view forward with long tiles split into bands (a low threshold, so that most tiles
+    of every view take the band path): images equal the unsplit batch's."""
+    sc = _scene(P=200_000, seed=5011)
+    cams = _cams(3, seed=5012)
+    bg = torch.zeros(3, device="cuda")
+    was = _lib.get_render_split()
+    out = []
+    try:
+        for split in (0, 64):
+            _lib.set_render_split(split, 2)
+            br = BatchedRasterizer(sc["means3D"], sc["opacities"], sc["scales"], sc["rotations"], cams,
+                                   shs=sc["shs"], sh_degree=3, bg=bg, graph=False)
+            br.forward()
+            br.check()
+            torch.cuda.synchronize()
+            out.append([im.clone() for im in br.images])
+            del br
+    finally:
+        _lib.set_render_split(*was)
+    for x, y in zip(*out):
+        assert torch.equal(x, y)
