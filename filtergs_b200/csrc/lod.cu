@@ -51,8 +51,24 @@ __device__ __forceinline__ uint32_t chunk_offset(uint32_t cnt, uint32_t chunk, u
     return r;
 }
 
+// Ordered compaction, kCompactItems items per thread (a chunk of 4096 per CTA):
+// a thread's items are consecutive, so its survivors are written as one run at
+// its exclusive offset, and one look-back per 4096 items orders the chunks.
+constexpr int kCompactItems = 16;
+constexpr uint32_t kCompactChunk = 256u * kCompactItems;
+
+// Writes the indices base + k of the set bits k of `bits` at out[off...] in order.
+__device__ __forceinline__ void write_run(uint32_t bits, uint32_t base, uint32_t off, int64_t* __restrict__ out)
+{
+    while (bits) {
+        const int k = __ffs(bits) - 1;
+        bits &= bits - 1;
+        out[off++] = (int64_t)(base + (uint32_t)k);
+    }
+}
+
 // mask[n] (bytes) -> ordered indices (int64) of the nonzero entries; count to *count.
-__global__ void __launch_bounds__(256) compact_kernel(const uint8_t* __restrict__ mask, uint32_t n,
+__global__ void __launch_bounds__(256) compact_kernel(const uint8_t* __restrict__ mask, uint32_t n, int vec,
                                                       int64_t* __restrict__ out, unsigned long long* count,
                                                       uint32_t* status, uint32_t* counter, unsigned* err)
 {
@@ -60,11 +76,24 @@ __global__ void __launch_bounds__(256) compact_kernel(const uint8_t* __restrict_
     if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1u);
     __syncthreads();
     const uint32_t chunk = s_chunk;
-    const uint32_t i = chunk * 256 + threadIdx.x;
-    const uint32_t f = (i < n && mask[i]) ? 1u : 0u;
-    const uint32_t off = chunk_offset(f, chunk, status, err);
-    if (f) out[off] = (int64_t)i;
-    if (chunk == gridDim.x - 1 && threadIdx.x == 255) *count = off + f;  // the last chunk knows the total
+    const uint32_t base = chunk * kCompactChunk + threadIdx.x * kCompactItems;
+    uint32_t bits = 0;
+    if (vec && base + kCompactItems <= n) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(mask + base));
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int b = 0; b < 4; b++)
+                if ((w[q] >> (8 * b)) & 0xffu) bits |= 1u << (4 * q + b);
+    } else {
+        for (int k = 0; k < kCompactItems; k++)
+            if (base + k < n && mask[base + k]) bits |= 1u << k;
+    }
+    const uint32_t cnt = __popc(bits);
+    const uint32_t off = chunk_offset(cnt, chunk, status, err);
+    write_run(bits, base, off, out);
+    if (chunk == gridDim.x - 1 && threadIdx.x == 255) *count = off + cnt;  // the last chunk knows the total
 }
 
 __global__ void gather_kernel(const int64_t* __restrict__ index, long long N, const float* __restrict__ xyz,
@@ -144,8 +173,9 @@ __global__ void gather_activate_kernel(const int64_t* __restrict__ index, const 
 
 // One LoG traversal level.  frontier[0..*fsize) are expanded nodes; their
 // children (frontier-major, child-slot-minor) are either kept (appended to
-// out at *out_count) or expanded (written to next[] in order).  Chunk order
-// comes from an atomic counter; two look-backs give ordered positions.
+// out at *out_count) or expanded (written to next[] in order).  Chunks of 4096
+// items (16 consecutive per thread) come from an atomic counter; two look-backs
+// give ordered positions.
 __global__ void __launch_bounds__(256)
     log_level_kernel(const int32_t* __restrict__ frontier, const uint32_t* __restrict__ fsize,
                      const int32_t* __restrict__ node_index, const int32_t* __restrict__ tree, int max_child,
@@ -159,7 +189,7 @@ __global__ void __launch_bounds__(256)
     __shared__ uint32_t s_chunk;
     __shared__ uint32_t s_base;
     const uint32_t items = min(*fsize * (uint32_t)max_child, max_items);
-    const uint32_t nchunks = (items + 255) / 256;
+    const uint32_t nchunks = (items + kCompactChunk - 1) / kCompactChunk;
     if (threadIdx.x == 0) s_base = *count_in;
     if (nchunks == 0) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -173,26 +203,37 @@ __global__ void __launch_bounds__(256)
         __syncthreads();
         const uint32_t chunk = s_chunk;
         if (chunk >= nchunks) break;
-        const uint32_t it = chunk * 256 + threadIdx.x;
-        int32_t ch = -1;
-        if (it < items) {
-            const int32_t node = frontier[it / max_child];
-            const int32_t ni = node_index[node];
-            if (ni >= 0) ch = tree[(size_t)ni * max_child + it % max_child];
+        const uint32_t base = chunk * kCompactChunk + threadIdx.x * kCompactItems;
+        int32_t ch[kCompactItems];
+#pragma unroll
+        for (int k = 0; k < kCompactItems; k++) {
+            const uint32_t it = base + k;
+            ch[k] = -1;
+            if (it < items) {
+                const int32_t ni = __ldg(node_index + __ldg(frontier + it / max_child));
+                if (ni >= 0) ch[k] = __ldg(tree + (size_t)ni * max_child + it % max_child);
+            }
         }
-        uint32_t k = 0, x = 0;
-        if (ch >= 0) {
-            const bool keep = radius[ch] < min_res || node_index[ch] == -1;
-            k = keep ? 1u : 0u;
-            x = keep ? 0u : 1u;
+        uint32_t kbits = 0, xbits = 0;
+#pragma unroll
+        for (int k = 0; k < kCompactItems; k++) {
+            if (ch[k] < 0) continue;
+            const bool keep = __ldg(radius + ch[k]) < min_res || __ldg(node_index + ch[k]) == -1;
+            if (keep) kbits |= 1u << k;
+            else xbits |= 1u << k;
         }
-        const uint32_t ok = chunk_offset(k, chunk, status_keep, err);
-        const uint32_t ox = chunk_offset(x, chunk, status_next, err);
-        if (k) out[s_base + ok] = ch;
-        if (x) next[ox] = ch;
+        const uint32_t kc = __popc(kbits), xc = __popc(xbits);
+        const uint32_t ok = chunk_offset(kc, chunk, status_keep, err);
+        const uint32_t ox = chunk_offset(xc, chunk, status_next, err);
+        uint32_t o = s_base + ok, q = ox;
+#pragma unroll
+        for (int k = 0; k < kCompactItems; k++) {
+            if ((kbits >> k) & 1u) out[o++] = ch[k];
+            if ((xbits >> k) & 1u) next[q++] = ch[k];
+        }
         if (chunk == nchunks - 1 && threadIdx.x == 255) {
-            *next_size = ox + x;
-            *count_out = s_base + ok + k;
+            *next_size = ox + xc;
+            *count_out = s_base + ok + kc;
         }
         __syncthreads();
     }
@@ -229,6 +270,7 @@ __global__ void __launch_bounds__(256)
 }
 
 // Order-preserving filter of a node list: keep radius >= min_px and sigmoid(opacity) >= 1/255.
+// Chunks of 4096 ids; CTAs past the live count leave at once.
 __global__ void __launch_bounds__(256)
     cull_kernel(const int32_t* __restrict__ in, const uint32_t* __restrict__ n_in, uint32_t cap,
                 const float* __restrict__ radius, const float* __restrict__ opac_raw, float min_px,
@@ -237,26 +279,34 @@ __global__ void __launch_bounds__(256)
 {
     __shared__ uint32_t s_chunk;
     const uint32_t n = min(*n_in, cap);
-    const uint32_t nchunks = (n + 255) / 256;
-    for (;;) {
-        if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1u);
-        __syncthreads();
-        const uint32_t chunk = s_chunk;
-        if (chunk >= nchunks) break;
-        const uint32_t i = chunk * 256 + threadIdx.x;
-        uint32_t k = 0;
-        int32_t id = -1;
-        if (i < n) {
-            id = in[i];
-            const float o = 1.0f / (1.0f + expf(-opac_raw[id]));
-            k = (radius[id] >= min_px && o >= 1.0f / 255.0f) ? 1u : 0u;
-        }
-        const uint32_t off = chunk_offset(k, chunk, status, err);
-        if (k) out[off] = id;
-        if (chunk == nchunks - 1 && threadIdx.x == 255) *n_out = off + k;
-        __syncthreads();
+    const uint32_t nchunks = (n + kCompactChunk - 1) / kCompactChunk;
+    if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t chunk = s_chunk;
+    if (chunk >= nchunks) {
+        if (chunk == 0 && threadIdx.x == 0) *n_out = 0;  // n == 0
+        return;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && n == 0) *n_out = 0;
+    const uint32_t base = chunk * kCompactChunk + threadIdx.x * kCompactItems;
+    int32_t id[kCompactItems];
+    uint32_t bits = 0;
+#pragma unroll
+    for (int k = 0; k < kCompactItems; k++) id[k] = base + k < n ? __ldg(in + base + k) : -1;
+#pragma unroll
+    for (int k = 0; k < kCompactItems; k++) {
+        if (id[k] < 0) continue;
+        const float o = 1.0f / (1.0f + expf(-__ldg(opac_raw + id[k])));
+        if (__ldg(radius + id[k]) >= min_px && o >= 1.0f / 255.0f) bits |= 1u << k;
+    }
+    const uint32_t cnt = __popc(bits);
+    const uint32_t off = chunk_offset(cnt, chunk, status, err);
+    uint32_t o = off;
+    while (bits) {
+        const int k = __ffs(bits) - 1;
+        bits &= bits - 1;
+        out[o++] = (int64_t)id[k];
+    }
+    if (chunk == nchunks - 1 && threadIdx.x == 255) *n_out = off + cnt;
 }
 
 // v2 3-sigma radius on raw parameters: exp(log scale) and normalised quaternion in-kernel
@@ -331,14 +381,15 @@ __global__ void __launch_bounds__(256) ancestor_path_kernel(int P, const int32_t
 void launch_compact(const uint8_t* mask, uint32_t n, int64_t* out, unsigned long long* count, uint32_t* scratch,
                     unsigned* err, cudaStream_t s)
 {
-    // scratch: [1 counter][ceil(n/256) status], zeroed here
-    const uint32_t nch = (n + 255) / 256;
+    // scratch: [1 counter][one status word per chunk], zeroed here
+    const uint32_t nch = (n + kCompactChunk - 1) / kCompactChunk;
     cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * (1 + nch), s);
     if (n == 0) {
         cudaMemsetAsync(count, 0, sizeof(unsigned long long), s);
         return;
     }
-    compact_kernel<<<nch, 256, 0, s>>>(mask, n, out, count, scratch + 1, scratch, err);
+    const int vec = (reinterpret_cast<uintptr_t>(mask) & 15u) == 0;
+    compact_kernel<<<nch, 256, 0, s>>>(mask, n, vec, out, count, scratch + 1, scratch, err);
     note_launches(1);
 }
 
@@ -382,9 +433,16 @@ void launch_radius_raw(int P, const float* means, const float* lscales, const fl
 // workspace layout (uint32 words): [0,1] output-count slots, [2,3] frontier-size slots,
 // [8 .. 8+levels+2) chunk counters, then 2 status arrays per level, then frontiers A and B.
 // After `levels` levels the output count is in slot (levels & 1).
+// look-back status words per level: 4096-item chunks of the children, 256-root chunks of the roots
+size_t log_cut_chunks(int P, int nroots, int max_child)
+{
+    return ((size_t)P * (size_t)max(1, max_child) + kCompactChunk - 1) / kCompactChunk + ((size_t)nroots + 255) / 256 +
+           1;
+}
+
 size_t log_cut_scratch_words(int P, int nroots, int max_child, int levels)
 {
-    const size_t chunks = ((size_t)P * (size_t)max(1, max_child) + 255) / 256 + ((size_t)nroots + 255) / 256 + 1;
+    const size_t chunks = log_cut_chunks(P, nroots, max_child);
     return 8 + (size_t)levels + 2 + (size_t)(levels + 2) * 2 * chunks + 2 * (size_t)P;
 }
 
@@ -395,7 +453,7 @@ void launch_log_cut(int P, const int32_t* roots, int nroots, const int32_t* node
     const size_t words = log_cut_scratch_words(P, nroots, max_child, levels);
     cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * (words - 2 * (size_t)P), s);
     if (nroots <= 0) return;
-    const size_t chunks = ((size_t)P * (size_t)max(1, max_child) + 255) / 256 + ((size_t)nroots + 255) / 256 + 1;
+    const size_t chunks = log_cut_chunks(P, nroots, max_child);
     uint32_t* count = scratch;       // [2]
     uint32_t* fsize = scratch + 2;   // [2]
     uint32_t* counters = scratch + 8;
@@ -414,7 +472,7 @@ void launch_log_cut(int P, const int32_t* roots, int nroots, const int32_t* node
         uint32_t* st = status + (size_t)(l + 1) * 2 * chunks;
         log_level_kernel<<<sms * 4, 256, 0, s>>>(fr[a], fsize + a, node_index, tree, max_child, radius, min_res, out,
                                                 count + a, count + b, fr[b], fsize + b, st, st + chunks,
-                                                counters + 1 + l, (uint32_t)(chunks * 256), err);
+                                                counters + 1 + l, (uint32_t)(chunks * kCompactChunk), err);
     }
     note_launches(1 + levels);
 }
@@ -423,14 +481,11 @@ void launch_cull(const int32_t* in, const uint32_t* n_in, uint32_t cap, const fl
                  float min_px, int64_t* out, unsigned long long* n_out, uint32_t* scratch, unsigned* err,
                  cudaStream_t s)
 {
-    const uint32_t nch = (cap + 255) / 256 + 1;
+    // one CTA per possible chunk of the capacity; those past the live count leave at once
+    const uint32_t nch = (cap + kCompactChunk - 1) / kCompactChunk + 1;
     cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * (1 + nch), s);
     cudaMemsetAsync(n_out, 0, sizeof(unsigned long long), s);
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cull_kernel<<<sms * 4, 256, 0, s>>>(in, n_in, cap, radius, opac_raw, min_px, out, n_out, scratch + 1, scratch,
-                                       err);
+    cull_kernel<<<nch, 256, 0, s>>>(in, n_in, cap, radius, opac_raw, min_px, out, n_out, scratch + 1, scratch, err);
     note_launches(1);
 }
 
