@@ -71,6 +71,8 @@ def parse(argv=None):
     ap.add_argument("--train-gaussians", type=int, default=4_000_000)
     ap.add_argument("--lod-nodes", type=int, default=8_000_000)
     ap.add_argument("--no-autotune", action="store_true", help="keep the default render kernel shape")
+    ap.add_argument("--only", choices=["lod", "train"], default=None,
+                    help="run only this workload on one GPU and print its result (profiling entry point)")
     ap.add_argument("--render-config", default=None,
                     help="fwd_ppt,fwd_batch,bwd_ppt,bwd_batch (skips the autotuner)")
     return ap.parse_args(argv)
@@ -553,6 +555,12 @@ def measure_train(args, dev):
     del pert
     out = {"gaussians": P, "views_per_step": 4, "width": 1600, "height": 900, "unit": "ms/iteration",
            "loss": "0.8 L1 + 0.2 (1 - SSIM 11x11, sigma 1.5)", "optimizer": "FP32 Adam on visible Gaussians"}
+    # the compositing launch shape for these views, tuned on a throwaway copy of the state (eager steps)
+    st = TR.TrainState(*state_args)
+    tune = TR.BatchedTrainer(st, cams, targets, bg=bg, graph=False)
+    out["render_config"] = autotune(args, lambda i: tune.step(), ("train", P), 0)
+    del tune, st
+    torch.cuda.empty_cache()
     for name in ("batched", "plain"):
         st = TR.TrainState(*state_args)
         tr = TR.BatchedTrainer(st, cams, targets, bg=bg) if name == "batched" else TR.PlainTrainer(st, cams, targets,
@@ -595,6 +603,12 @@ def fp64_image_error(mod, dev):
 
 def main():
     args = parse()
+    if args.only:
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        res = measure_lod(args, dev, args.impl) if args.only == "lod" else measure_train(args, dev)
+        print(json.dumps({"workload": args.only, "impl": args.impl, **res}))
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
