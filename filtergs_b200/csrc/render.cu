@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas<PPT>())
         const uint32_t item = s_item;
         if (item >= total) break;
         const int v = view_of(begin, nviews, item);
-        const TileArgs a = views[v];
+        const TileArgs& a = views[v];  // fields read where used, not held in registers
         render_fwd_tile<PPT, kBatch>(sm, a, (int)(item - begin[v]), gb, split_min, err);
         __syncthreads();
     }
@@ -903,6 +903,13 @@ __device__ __forceinline__ void bwd_smem_init(BwdSmem<kBatch, kSlots>& sm, int N
 template <int PPT, int kBatch>
 using BwdSmemT = BwdSmem<kBatch, bwd_slots<PPT>()>;
 
+// Resident CTAs per SM the multi-view backward is compiled for at 2 pixels per
+// thread (24 warps; left alone it takes 86 registers, 20 warps).  The other shapes
+// and the single-view kernel keep the compiler's allocation (capping 4 pixels per
+// thread below its 122 registers spills).
+template <int PPT>
+constexpr int bwd_multi_min_ctas() { return PPT == 2 ? 6 : 1; }
+
 template <int PPT, int kBatch>
 __global__ void __launch_bounds__(256 / PPT) render_bwd_kernel(TileArgs a, int consistent, unsigned* err)
 {
@@ -914,7 +921,7 @@ __global__ void __launch_bounds__(256 / PPT) render_bwd_kernel(TileArgs a, int c
 }
 
 template <int PPT, int kBatch>
-__global__ void __launch_bounds__(256 / PPT)
+__global__ void __launch_bounds__(256 / PPT, bwd_multi_min_ctas<PPT>())
     render_bwd_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin, int nviews,
                             uint32_t total, uint32_t* queue, int consistent, unsigned* err)
 {
@@ -930,7 +937,7 @@ __global__ void __launch_bounds__(256 / PPT)
         if (item >= total) break;
         int v = 0;
         while (v + 1 < nviews && begin[v + 1] <= item) v++;
-        const TileArgs a = views[v];
+        const TileArgs& a = views[v];  // fields read where used, not held in registers
         render_bwd_tile<PPT, kBatch>(sm, a, (int)(item - begin[v]), gb, consistent, err);
         __syncthreads();
     }
