@@ -150,24 +150,39 @@ __device__ __forceinline__ float3 sh_backward(int deg, const float* __restrict__
 
 // Screen-space gradients of the visible Gaussians: the sum of each Gaussian's
 // per-pair gradients (pgrad rows at its emission indices, its tiles row-major).
-// One warp per Gaussian: lane l takes rows l, l+32, ... (coalesced 36-byte rows,
-// 128 rows in flight per round trip, so a splat over thousands of tiles does not
-// stall the kernel) and a fixed shuffle tree adds them, 32 rows at a time in
-// emission order -- the same sum on every run.  Row layout: dcolor r,g,b |
-// dmean2D x,y | dconic x,y,w | dopacity.
+// Gaussians are taken in depth rank j, whose pairs are the contiguous rows
+// [pair_off[j], pair_off[j + 1]) (the last ends at K), so a warp reads its next
+// Gaussian's row range while it sums the current one.  One warp per Gaussian:
+// lane l takes rows l, l+32, ... (coalesced 36-byte rows, 128 rows in flight per
+// round trip, so a splat over thousands of tiles does not stall the kernel) and a
+// fixed shuffle tree adds them, 32 rows at a time in emission order -- the same
+// sum on every run.  Row layout: dcolor r,g,b | dmean2D x,y | dconic x,y,w |
+// dopacity.
 __global__ void __launch_bounds__(256)
-    pair_grad_gather_kernel(const uint32_t* __restrict__ visible_ids, const unsigned long long* __restrict__ visible_count,
-                            const uint32_t* __restrict__ tiles, const uint32_t* __restrict__ pair_off,
-                            const float* __restrict__ pgrad, float* __restrict__ dmean2D, float* __restrict__ dconic,
-                            float* __restrict__ dcolor, float* __restrict__ dopac, float* __restrict__ dens_grad,
-                            int* __restrict__ dens_count, uint8_t* __restrict__ dens_flag)
+    pair_grad_gather_kernel(const uint32_t* __restrict__ visible_ids, const unsigned long long* __restrict__ totals,
+                            const uint32_t* __restrict__ pair_off, const float* __restrict__ pgrad,
+                            float* __restrict__ dmean2D, float* __restrict__ dconic, float* __restrict__ dcolor,
+                            float* __restrict__ dopac, float* __restrict__ dens_grad, int* __restrict__ dens_count,
+                            uint8_t* __restrict__ dens_flag)
 {
-    const uint32_t V = (uint32_t)*visible_count;
+    const uint32_t K = (uint32_t)totals[0], V = (uint32_t)totals[1];
     const int lane = threadIdx.x & 31;
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < V; j += nwarps) {
-        const int idx = (int)visible_ids[j];
-        const uint32_t e0 = __ldg(pair_off + idx), ne = __ldg(tiles + idx);
+    uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    auto range = [&](uint32_t jj, uint32_t& e0, uint32_t& e1, int& idx) {
+        e0 = __ldg(pair_off + jj);
+        e1 = jj + 1 < V ? __ldg(pair_off + jj + 1) : K;
+        idx = (int)__ldg(visible_ids + jj);
+    };
+    uint32_t e0 = 0, e1 = 0;
+    int idx = 0;
+    if (j < V) range(j, e0, e1, idx);
+    while (j < V) {
+        const uint32_t jn = j + nwarps;
+        uint32_t n0 = 0, n1 = 0;
+        int nidx = 0;
+        if (jn < V) range(jn, n0, n1, nidx);  // the next Gaussian's rows, in flight meanwhile
+        const uint32_t ne = e1 - e0;
         float acc = 0.f;  // lanes 2q and 2q+1: component q
         for (uint32_t k = 0; k < ne; k += 128) {
             float v[4][9];
@@ -200,6 +215,10 @@ __global__ void __launch_bounds__(256)
                                : dopac + idx;
             *dst = acc;
         }
+        j = jn;
+        e0 = n0;
+        e1 = n1;
+        idx = nidx;
     }
 }
 
@@ -463,8 +482,8 @@ void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* 
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int blocks = (int)std::min<size_t>((P + 255) / 256, (size_t)sms * 8);
     const bool sh = p.shs && dsh;
-    pair_grad_gather_kernel<<<blocks, 256, 0, s>>>(g.sort_ids_b, g.total + 1, g.tiles, g.pair_off, pgrad, dmean2D,
-                                                   dconic, dcolor, dopac, dens ? dens->grad_sum : nullptr,
+    pair_grad_gather_kernel<<<blocks, 256, 0, s>>>(g.sort_ids_b, g.total, g.pair_off, pgrad, dmean2D, dconic,
+                                                   dcolor, dopac, dens ? dens->grad_sum : nullptr,
                                                    dens ? dens->count : nullptr, dens ? dens->flag : nullptr);
     if (accumulate) {
         preprocess_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, dmean2D, dconic, dopac,

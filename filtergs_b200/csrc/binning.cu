@@ -251,9 +251,10 @@ __global__ void __launch_bounds__(256)
         __syncthreads();
         const uint32_t off = s_prefix + local;
         if (cnt) {
-            // first emitted pair, and the emission index of tile (tx, ty) as
-            // erow.x + ty * erow.y + tx (unsigned wrap-around)
-            pair_off[id] = off;
+            // first emitted pair (by depth rank j: Gaussian j's pairs are
+            // [pair_off[j], pair_off[j + 1])), and the emission index of tile
+            // (tx, ty) as erow.x + ty * erow.y + tx (unsigned wrap-around)
+            pair_off[j] = off;
             erow[id] = make_int2((int)(off - (uint32_t)y0 * (uint32_t)w - (uint32_t)x0), w);
         }
         // warp-local exclusive prefix of cnt

@@ -40,8 +40,8 @@ struct GeomState {
     uint32_t* sort_ids_a;      // [V] depth-sorted ids (ping)
     uint32_t* sort_ids_b;      // [V] visible ids in index order, then depth-sorted (pong)
     uint32_t* sort_keys_b;     // [P]
-    uint32_t* pair_off;        // [P] first emitted pair of each visible Gaussian (aliases sort_keys_b,
-                               //     dead once the depth sort is done)
+    uint32_t* pair_off;        // [V] first emitted pair of the visible Gaussian of depth rank j (aliases
+                               //     sort_keys_b, dead once the depth sort is done)
     int2* erow;                // [P] emission index of tile (tx, ty) = erow.x + ty * erow.y + tx
     uint32_t* hist;            // [8][256] radix histograms: 4 depth passes + up to 4 tile passes
     uint32_t* status;          // lookback status words, depth passes
