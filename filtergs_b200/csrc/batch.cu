@@ -7,7 +7,7 @@
 // memsets on the caller's stream -- no host synchronisation, no allocation --
 // so the pair can be captured into a CUDA graph and replayed.  Per view the
 // front end (preprocess, depth sort, pair emission, tile sort, ranges) runs
-// with the pair count kept on the device, the views spread over four streams
+// with the pair count kept on the device, the views spread over eight streams
 // forked from the caller's stream and joined before compositing (those kernels
 // are latency-bound, so views overlap); compositing, forward and backward,
 // is ONE persistent launch per direction over the tiles of all views, fed by a
@@ -42,7 +42,7 @@ struct ViewState {
     int* radii_out;
 };
 
-constexpr int kFrontStreams = 4;  // views whose front ends run concurrently
+constexpr int kFrontStreams = 8;  // views whose front ends run concurrently
 
 struct Batch {
     int P, V, consistent;
