@@ -152,9 +152,9 @@ def make_scene(P, device):
                     opacities=t(sc["opacities"]), shs=t(sc["shs"]))
 
 
-def make_views(n, device, rank, W=1920, H=1080, mixed=False):
+def rank_cameras(n, rank, W=1920, H=1080, mixed=False):
     """n cameras of the 1080p workload, or of the mixed-resolution one (same field of view at every
-    resolution: fx scales with the width).  Rank r draws its own cameras."""
+    resolution: fx scales with the width).  Rank r draws its own cameras (host only)."""
     from filtergs_b200 import synthetic as S
     rng = np.random.default_rng((4001 if mixed else 2001) + 97 * rank)
     cams = []
@@ -165,6 +165,19 @@ def make_views(n, device, rank, W=1920, H=1080, mixed=False):
                                         pitch_deg=float(rng.uniform(30, 75))))
         else:
             cams.append(S.aerial_camera(rng, W=W, H=H))
+    return cams
+
+
+def aggregate_views_per_s(n_ranks, views_per_rank, steps, ms_max):
+    """Whole-job views/s: every rank renders its own views_per_rank cameras per step; the step time
+    is the slowest rank's (max over ranks)."""
+    return n_ranks * views_per_rank * steps / (ms_max / 1000.0)
+
+
+def make_views(n, device, rank, W=1920, H=1080, mixed=False):
+    """rank_cameras(...) on `device`, with a seeded upstream gradient per view (device copy and a
+    pinned host copy for the end-to-end leg)."""
+    cams = rank_cameras(n, rank, W, H, mixed)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
     g = torch.Generator(device="cpu").manual_seed(3001 + 7 * rank + (1 if mixed else 0))
     views = []
@@ -657,7 +670,7 @@ def main():
     else:
         head = measure_plain(args, mod, scene, views, bg, dev, ref_dist, rank, clocks=clocks, profile=True)
         path = "plain"
-    value = n_ranks * nv * args.steps / (head["ms"] / 1000.0)
+    value = aggregate_views_per_s(n_ranks, nv, args.steps, head["ms"])
 
     e2e = None
     if not args.no_e2e:
