@@ -13,6 +13,8 @@
 // racy out_point_weight max, the KPC statistics, the backward's 9 gradient
 // atomics) are reduced across the warp first, then across the CTA in shared
 // memory, and leave the CTA once per (tile, pair).
+#include <cstddef>
+
 #include "fgs_common.cuh"
 #include "fgs_internal.h"
 
@@ -127,6 +129,9 @@ __device__ __forceinline__ bool may_touch(float mx, float my, float a, float b, 
 // Everything one tile needs, for the plain launch (one view, one tile per CTA)
 // and the persistent multi-view launch (CTAs pop (view, tile) work items).
 
+// The statistics sums come last: a launch without statistics allocates the
+// dynamic shared memory only up to ksum (fwd_smem_bytes), which leaves room for
+// one more CTA per SM at the batch sizes the autotuner picks.
 template <int kBatch>
 struct FwdSmem {
     PairRecord rec[kBufs][kBatch];
@@ -245,7 +250,7 @@ __device__ __forceinline__ void fwd_pixel_step(const float4 ra, const float4 rb,
 // once per CTA and keep their phase across tiles.
 template <int PPT, int kBatch>
 __device__ __forceinline__ void render_fwd_tile(FwdSmem<kBatch>& sm, const TileArgs& a, int tile, uint32_t& gb,
-                                                uint32_t split_min, unsigned* err)
+                                                uint32_t split_min, bool stats_smem, unsigned* err)
 {
     constexpr int NT = 256 / PPT;
     const int tid = threadIdx.x;
@@ -258,7 +263,7 @@ __device__ __forceinline__ void render_fwd_tile(FwdSmem<kBatch>& sm, const TileA
     const uint32_t n = range.y - range.x;
     if (split_min && n >= split_min) return;  // rendered in bands (render_fwd_band)
     const int nb = (int)((n + kBatch - 1) / kBatch);
-    const bool stats = a.kv_sum != nullptr;
+    const bool stats = stats_smem && a.kv_sum != nullptr;  // the sums exist only in a launch that has them
     const PairRecord* recs = a.recs;
 
     if (tid == 0) {
@@ -410,12 +415,14 @@ __device__ __forceinline__ void render_fwd_tile(FwdSmem<kBatch>& sm, const TileA
 }
 
 template <int kBatch>
-__device__ __forceinline__ void fwd_smem_init(FwdSmem<kBatch>& sm, int NT)
+__device__ __forceinline__ void fwd_smem_init(FwdSmem<kBatch>& sm, int NT, bool stats_smem)
 {
     for (int e = threadIdx.x; e < 2 * kBatch; e += NT) {
         (&sm.wmax[0][0])[e] = 0;
-        (&sm.ksum[0][0])[e] = 0.f;
-        (&sm.kcnt[0][0])[e] = 0;
+        if (stats_smem) {
+            (&sm.ksum[0][0])[e] = 0.f;
+            (&sm.kcnt[0][0])[e] = 0;
+        }
     }
     if (threadIdx.x == 0) {
         for (int i = 0; i < kBufs; i++) mbar_init(&sm.bar[i], 1);
@@ -433,10 +440,12 @@ template <int PPT, int kBatch>
 __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas<PPT>())
     render_fwd_kernel(TileArgs a, uint32_t split_min, unsigned* err)
 {
-    __shared__ __align__(128) FwdSmem<kBatch> sm;
-    fwd_smem_init(sm, 256 / PPT);
+    extern __shared__ __align__(128) unsigned char fwd_dyn[];
+    FwdSmem<kBatch>& sm = *reinterpret_cast<FwdSmem<kBatch>*>(fwd_dyn);
+    const bool stats_smem = a.kv_sum != nullptr;  // the launch sized the shared memory from the same test
+    fwd_smem_init(sm, 256 / PPT, stats_smem);
     uint32_t gb = 0;
-    render_fwd_tile<PPT, kBatch>(sm, a, blockIdx.x, gb, split_min, err);
+    render_fwd_tile<PPT, kBatch>(sm, a, blockIdx.x, gb, split_min, stats_smem, err);
 }
 
 // Persistent multi-view forward: CTAs pop work items from one queue; item i is
@@ -453,9 +462,11 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas<PPT>())
     render_fwd_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin, int nviews,
                             uint32_t total, uint32_t* queue, uint32_t split_min, unsigned* err)
 {
-    __shared__ __align__(128) FwdSmem<kBatch> sm;
+    // launched without the statistics sums (the batched path keeps no statistics)
+    extern __shared__ __align__(128) unsigned char fwd_dyn[];
+    FwdSmem<kBatch>& sm = *reinterpret_cast<FwdSmem<kBatch>*>(fwd_dyn);
     __shared__ uint32_t s_item;
-    fwd_smem_init(sm, 256 / PPT);
+    fwd_smem_init(sm, 256 / PPT, false);
     uint32_t gb = 0;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(queue, 1u);
@@ -464,7 +475,7 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas<PPT>())
         if (item >= total) break;
         const int v = view_of(begin, nviews, item);
         const TileArgs& a = views[v];  // fields read where used, not held in registers
-        render_fwd_tile<PPT, kBatch>(sm, a, (int)(item - begin[v]), gb, split_min, err);
+        render_fwd_tile<PPT, kBatch>(sm, a, (int)(item - begin[v]), gb, split_min, false, err);
         __syncthreads();
     }
 }
@@ -949,6 +960,14 @@ __global__ void __launch_bounds__(256 / PPT, bwd_multi_min_ctas<PPT>())
 namespace {
 RenderConfig g_cfg{2, 256, 2, 256, 0, 0};
 
+// Dynamic shared memory of a forward launch: the whole FwdSmem with statistics,
+// up to its statistics sums without.
+template <int kBatch>
+size_t fwd_smem_bytes(bool stats)
+{
+    return stats ? sizeof(FwdSmem<kBatch>) : offsetof(FwdSmem<kBatch>, ksum);
+}
+
 // Band shapes (fgs_set_render_split): 0 = 16x2, 1 = 8x4, 2 = 4x4, 3 = 4x2 pixels per warp.
 template <int BW, int BH>
 void band_launch(const TileArgs& a, const uint32_t* list, uint32_t* ctr, uint32_t cap, unsigned* err, cudaStream_t s)
@@ -1003,7 +1022,8 @@ void fwd_launch(int grid, const ImageState& im, const BinState& b, long long K, 
         launch_band_kernel(band_shape, a, im.long_list, im.long_ctr, (uint32_t)grid, err, s);
         note_launches(2);
     }
-    render_fwd_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(a, (uint32_t)(split > 0 ? split : 0), err);
+    render_fwd_kernel<PPT, B><<<grid, 256 / PPT, fwd_smem_bytes<B>(stats), s>>>(a, (uint32_t)(split > 0 ? split : 0),
+                                                                                err);
 }
 
 // Dynamic shared memory of a backward kernel instantiation (opted in once per process
@@ -1083,8 +1103,13 @@ void fwd_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, 
         launch_band_multi_kernel(band_shape, views, begin, nviews, long_list, long_ctr, total, err, s);
         note_launches(2);
     }
-    const int grid = (int)resident_ctas(render_fwd_multi_kernel<PPT, B>, 256 / PPT);
-    render_fwd_multi_kernel<PPT, B><<<grid, 256 / PPT, 0, s>>>(views, begin, nviews, total, queue,
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t smem = fwd_smem_bytes<B>(false);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_fwd_multi_kernel<PPT, B>, 256 / PPT, smem);
+    const int grid = sms * (per_sm > 0 ? per_sm : 1);
+    render_fwd_multi_kernel<PPT, B><<<grid, 256 / PPT, smem, s>>>(views, begin, nviews, total, queue,
                                                                (uint32_t)(split > 0 ? split : 0), err);
 }
 
