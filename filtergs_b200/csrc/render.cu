@@ -432,9 +432,10 @@ __device__ __forceinline__ void fwd_smem_init(FwdSmem<kBatch>& sm, int NT, bool 
 }
 
 // Resident CTAs per SM the forward kernels are compiled for (a register cap of
-// 65536 / (CTAs x threads)): 24 warps per SM at 2 pixels per thread, 20 at 4.
+// 65536 / (CTAs x threads)): 24 warps per SM at 2 and at 4 pixels per thread (at 4
+// the cap is 80 registers, which a 64-record batch's shared memory then lets fill).
 template <int PPT>
-constexpr int fwd_min_ctas() { return PPT == 1 ? 3 : (PPT == 2 ? 6 : 10); }
+constexpr int fwd_min_ctas() { return PPT == 1 ? 3 : (PPT == 2 ? 6 : 12); }
 
 template <int PPT, int kBatch>
 __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas<PPT>())
