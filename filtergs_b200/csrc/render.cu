@@ -746,7 +746,12 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
     const uint2 range = a.ranges[tile];
     const PairRecord* recs = a.recs;
 
-    float T[PPT], T_final[PPT], dpix[PPT][3], accum[PPT][3], last_color[PPT][3], last_alpha[PPT], pyf[PPT];
+    // Per pixel: the reference's accum_rec recurrence (the colour composited behind
+    // the current Gaussian, backward.cu:513-520) enters dL/dalpha only through its
+    // dot product with dL/dpixel, so the pixel carries that dot product (acc_dot)
+    // and the previous contributor's colour dotted the same way (last_dot): the
+    // same sums, regrouped, in 2 values instead of 6.
+    float T[PPT], T_final[PPT], dpix[PPT][3], acc_dot[PPT], last_dot[PPT], last_alpha[PPT], pyf[PPT];
     uint32_t last[PPT];
     float bg_dot[PPT];
     const float bg0 = a.bg[0], bg1 = a.bg[1], bg2 = a.bg[2];
@@ -761,11 +766,9 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
         last[k] = inside ? a.n_contrib[pix] : 0;
         my_max = max(my_max, last[k]);
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            dpix[k][c] = inside ? a.dL_dpix[c * H * W + pix] : 0.f;
-            accum[k][c] = 0.f;
-            last_color[k][c] = 0.f;
-        }
+        for (int c = 0; c < 3; c++) dpix[k][c] = inside ? a.dL_dpix[c * H * W + pix] : 0.f;
+        acc_dot[k] = 0.f;
+        last_dot[k] = 0.f;
         last_alpha[k] = 0.f;
         bg_dot[k] = bg0 * dpix[k][0] + bg1 * dpix[k][1] + bg2 * dpix[k][2];
         pyf[k] = (float)py;
@@ -775,6 +778,11 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
     const float ry0 = (float)(by * kTileY + (tid >> 5) * 2 * PPT), ry1 = ry0 + (2 * PPT - 1);
     const float ddelx_dx = 0.5 * W;
     const float ddely_dy = 0.5 * H;
+    // The per-pixel loop sums the mean and conic gradients without their constant
+    // factors (-W/2, -H/2 and -1/2, backward.cu:545-551); each warp total is scaled
+    // once, on the lanes that hold it (value q on lanes 2q and 2q+1).
+    const unsigned q_lane = (tid & 31) >> 1;
+    const float gscale = q_lane == 3 ? -ddelx_dx : (q_lane == 4 ? -ddely_dy : (q_lane >= 5 && q_lane <= 7 ? -0.5f : 1.f));
 
     if (tid == 0) sm.max_last = 0;
     __syncthreads();
@@ -824,46 +832,47 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
 #pragma unroll
                 for (int k = 0; k < PPT; k++) {
                     if (contributor >= last[k]) continue;
-                    const float2 d = {ra.x - pxf, ra.y - pyf[k]};
-                    const float power = -0.5f * (ra.z * d.x * d.x + rb.x * d.y * d.y) - ra.w * d.x * d.y;
+                    // G and alpha in the forward's arithmetic (fwd_alpha): the same
+                    // bits, so this pass skips exactly the pairs the forward skipped
+                    const float dx = ra.x - pxf, dy = ra.y - pyf[k];
+                    const float qf = __fmaf_rn(__fmul_rn(ra.z, dx), dx, __fmul_rn(__fmul_rn(rb.x, dy), dy));
+                    const float power = __fmaf_rn(-0.5f, qf, -__fmul_rn(__fmul_rn(ra.w, dx), dy));
                     if (power > 0.0f) continue;
-                    const float G = exp(power);
-                    const float alpha = min(0.99f, rb.y * G);
+                    const float G = expf(power);
+                    const float oG = __fmul_rn(rb.y, G);
+                    const float alpha = fminf(0.99f, oG);
                     if (alpha < 1.0f / 255.0f) continue;
                     // transmittance before this Gaussian (fast reciprocal: 1 - alpha >= 0.01)
                     const float inv_1ma = __fdividef(1.f, 1.f - alpha);
                     T[k] = T[k] * inv_1ma;
                     const float dchannel_dcolor = alpha * T[k];
-                    const float col[3] = {rb.z, rb.w, R[j].c.x};
-                    float dL_dalpha = 0.0f;
-#pragma unroll
-                    for (int ch = 0; ch < 3; ch++) {
-                        const float c = col[ch];
-                        accum[k][ch] = last_alpha[k] * last_color[k][ch] + (1.f - last_alpha[k]) * accum[k][ch];
-                        last_color[k][ch] = c;
-                        dL_dalpha += (c - accum[k][ch]) * dpix[k][ch];
-                        gr[ch] += dchannel_dcolor * dpix[k][ch];
-                    }
-                    dL_dalpha *= T[k];
+                    const float c2 = R[j].c.x;
+                    gr[0] += dchannel_dcolor * dpix[k][0];
+                    gr[1] += dchannel_dcolor * dpix[k][1];
+                    gr[2] += dchannel_dcolor * dpix[k][2];
+                    const float cdot = rb.z * dpix[k][0] + rb.w * dpix[k][1] + c2 * dpix[k][2];
+                    acc_dot[k] += last_alpha[k] * (last_dot[k] - acc_dot[k]);
+                    last_dot[k] = cdot;
                     last_alpha[k] = alpha;
+                    float dL_dalpha = (cdot - acc_dot[k]) * T[k];
                     // background term; exactly zero (and skipped) for a black background
                     if (bg_dot[k] != 0.f) dL_dalpha += (-T_final[k] * inv_1ma) * bg_dot[k];
-                    if (consistent && rb.y * G > 0.99f) dL_dalpha = 0.f;
-                    const float dL_dG = rb.y * dL_dalpha;
-                    const float gdx = G * d.x;
-                    const float gdy = G * d.y;
-                    const float dG_ddelx = -gdx * ra.z - gdy * ra.w;
-                    const float dG_ddely = -gdy * rb.x - gdx * ra.w;
-                    gr[3] += dL_dG * dG_ddelx * ddelx_dx;
-                    gr[4] += dL_dG * dG_ddely * ddely_dy;
-                    gr[5] += -0.5f * gdx * d.x * dL_dG;
-                    gr[6] += -0.5f * gdx * d.y * dL_dG;
-                    gr[7] += -0.5f * gdy * d.y * dL_dG;
+                    if (consistent && oG > 0.99f) dL_dalpha = 0.f;
+                    // s = G dL/dG; the sums below, times gscale, are dL/dmean2D
+                    // (G (a dx + b dy), G (b dx + c dy)) and dL/dconic (G dx dx, G dx dy,
+                    // G dy dy) of the reference's atomics
+                    const float s = G * (rb.y * dL_dalpha);
+                    const float u = s * dx, v = s * dy;
+                    gr[3] += u * ra.z + v * ra.w;
+                    gr[4] += v * rb.x + u * ra.w;
+                    gr[5] += u * dx;
+                    gr[6] += u * dy;
+                    gr[7] += v * dy;
                     gr[8] += G * dL_dalpha;
                     any = true;
                 }
                 if (__any_sync(0xffffffffu, any)) {
-                    const float tot = warp_transpose_sum9(gr);
+                    const float tot = warp_transpose_sum9(gr) * gscale;
                     const unsigned lane = tid & 31;
                     if (!(lane & 1) && (lane >> 1) < NG) atomicAdd(&sm.acc[(tid >> 5) >> 1][lane >> 1][j], tot);
                 }
@@ -916,12 +925,13 @@ __device__ __forceinline__ void bwd_smem_init(BwdSmem<kBatch, kSlots>& sm, int N
 template <int PPT, int kBatch>
 using BwdSmemT = BwdSmem<kBatch, bwd_slots<PPT>()>;
 
-// Resident CTAs per SM the multi-view backward is compiled for at 2 pixels per
-// thread (24 warps; left alone it takes 86 registers, 20 warps).  The other shapes
-// and the single-view kernel keep the compiler's allocation (capping 4 pixels per
-// thread below its 122 registers spills).
+// Resident CTAs per SM the multi-view backward is compiled for: 24 warps at 2 pixels
+// per thread (77 registers), 20 at 4 (96 registers instead of the 110 the compiler
+// takes when left alone; with 64-record batches the shared memory then lets all 10
+// CTAs in).  Neither spills; one more CTA at either shape does.  The single-view
+// kernel keeps the compiler's allocation.
 template <int PPT>
-constexpr int bwd_multi_min_ctas() { return PPT == 2 ? 6 : 1; }
+constexpr int bwd_multi_min_ctas() { return PPT == 2 ? 6 : (PPT == 4 ? 10 : 1); }
 
 template <int PPT, int kBatch>
 __global__ void __launch_bounds__(256 / PPT) render_bwd_kernel(TileArgs a, int consistent, unsigned* err)
