@@ -730,9 +730,11 @@ __global__ void __launch_bounds__(32 * kBandWarps)
 }
 
 // ---------------------------------------------------------------- backward
-template <int PPT, int kBatch>
+// kConsistent: the exact-gradient backward mode (FGS_BACKWARD_CONSISTENT), a
+// compile-time switch so that the reference mode pays nothing for it per pixel.
+template <int PPT, int kBatch, bool kConsistent>
 __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()>& sm, const TileArgs& a, int tile,
-                                                uint32_t& gb, int consistent, unsigned* err)
+                                                uint32_t& gb, unsigned* err)
 {
     constexpr int kSlots = bwd_slots<PPT>();
     constexpr int NT = 256 / PPT;
@@ -857,7 +859,7 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
                     float dL_dalpha = (cdot - acc_dot[k]) * T[k];
                     // background term; exactly zero (and skipped) for a black background
                     if (bg_dot[k] != 0.f) dL_dalpha += (-T_final[k] * inv_1ma) * bg_dot[k];
-                    if (consistent && oG > 0.99f) dL_dalpha = 0.f;
+                    if (kConsistent && oG > 0.99f) dL_dalpha = 0.f;
                     // s = G dL/dG; the sums below, times gscale, are dL/dmean2D
                     // (G (a dx + b dy), G (b dx + c dy)) and dL/dconic (G dx dx, G dx dy,
                     // G dy dy) of the reference's atomics
@@ -933,20 +935,20 @@ using BwdSmemT = BwdSmem<kBatch, bwd_slots<PPT>()>;
 template <int PPT>
 constexpr int bwd_multi_min_ctas() { return PPT == 2 ? 6 : (PPT == 4 ? 10 : 1); }
 
-template <int PPT, int kBatch>
-__global__ void __launch_bounds__(256 / PPT) render_bwd_kernel(TileArgs a, int consistent, unsigned* err)
+template <int PPT, int kBatch, bool kConsistent>
+__global__ void __launch_bounds__(256 / PPT) render_bwd_kernel(TileArgs a, unsigned* err)
 {
     extern __shared__ __align__(128) unsigned char bwd_dyn[];
     BwdSmemT<PPT, kBatch>& sm = *reinterpret_cast<BwdSmemT<PPT, kBatch>*>(bwd_dyn);
     bwd_smem_init(sm, 256 / PPT);
     uint32_t gb = 0;
-    render_bwd_tile<PPT, kBatch>(sm, a, blockIdx.x, gb, consistent, err);
+    render_bwd_tile<PPT, kBatch, kConsistent>(sm, a, blockIdx.x, gb, err);
 }
 
-template <int PPT, int kBatch>
+template <int PPT, int kBatch, bool kConsistent>
 __global__ void __launch_bounds__(256 / PPT, bwd_multi_min_ctas<PPT>())
     render_bwd_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin, int nviews,
-                            uint32_t total, uint32_t* queue, int consistent, unsigned* err)
+                            uint32_t total, uint32_t* queue, unsigned* err)
 {
     extern __shared__ __align__(128) unsigned char bwd_dyn[];
     BwdSmemT<PPT, kBatch>& sm = *reinterpret_cast<BwdSmemT<PPT, kBatch>*>(bwd_dyn);
@@ -961,7 +963,7 @@ __global__ void __launch_bounds__(256 / PPT, bwd_multi_min_ctas<PPT>())
         int v = 0;
         while (v + 1 < nviews && begin[v + 1] <= item) v++;
         const TileArgs& a = views[v];  // fields read where used, not held in registers
-        render_bwd_tile<PPT, kBatch>(sm, a, (int)(item - begin[v]), gb, consistent, err);
+        render_bwd_tile<PPT, kBatch, kConsistent>(sm, a, (int)(item - begin[v]), gb, err);
         __syncthreads();
     }
 }
@@ -1038,7 +1040,8 @@ void fwd_launch(int grid, const ImageState& im, const BinState& b, long long K, 
 }
 
 // Dynamic shared memory of a backward kernel instantiation (opted in once per process
-// and device ordinal; Tag tells the single-view and multi-view kernels apart).
+// and device ordinal; Tag tells the kernels apart: single-view 0, multi-view 1, +2 in the
+// consistent mode).
 template <int PPT, int B, int Tag, typename Kern>
 size_t bwd_smem_bytes(Kern k)
 {
@@ -1061,8 +1064,13 @@ void bwd_launch(int grid, const ImageState& im, const BinState& b, int W, int H,
     a.ranges = im.ranges; a.recs = b.rec; a.W = W; a.H = H; a.bg = bg;
     a.final_T = im.final_T; a.n_contrib = im.n_contrib;
     a.dL_dpix = dL; a.pgrad = b.pgrad;
-    const size_t smem = bwd_smem_bytes<PPT, B, 0>(render_bwd_kernel<PPT, B>);
-    render_bwd_kernel<PPT, B><<<grid, 256 / PPT, smem, s>>>(a, consistent, err);
+    if (consistent) {
+        const size_t smem = bwd_smem_bytes<PPT, B, 2>(render_bwd_kernel<PPT, B, true>);
+        render_bwd_kernel<PPT, B, true><<<grid, 256 / PPT, smem, s>>>(a, err);
+    } else {
+        const size_t smem = bwd_smem_bytes<PPT, B, 0>(render_bwd_kernel<PPT, B, false>);
+        render_bwd_kernel<PPT, B, false><<<grid, 256 / PPT, smem, s>>>(a, err);
+    }
 }
 
 #define FGS_RENDER_DISPATCH(FN, PPT_, B_, ...)                                            \
@@ -1124,18 +1132,27 @@ void fwd_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, 
                                                                (uint32_t)(split > 0 ? split : 0), err);
 }
 
-template <int PPT, int B>
-void bwd_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total, uint32_t* queue,
-                      int consistent, unsigned* err, cudaStream_t s)
+template <int PPT, int B, bool kConsistent>
+void bwd_multi_launch_mode(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total, uint32_t* queue,
+                           unsigned* err, cudaStream_t s)
 {
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t smem = bwd_smem_bytes<PPT, B, 1>(render_bwd_multi_kernel<PPT, B>);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_bwd_multi_kernel<PPT, B>, 256 / PPT, smem);
+    const size_t smem = bwd_smem_bytes<PPT, B, kConsistent ? 3 : 1>(render_bwd_multi_kernel<PPT, B, kConsistent>);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, render_bwd_multi_kernel<PPT, B, kConsistent>, 256 / PPT,
+                                                  smem);
     const int grid = sms * (per_sm > 0 ? per_sm : 1);
-    render_bwd_multi_kernel<PPT, B><<<grid, 256 / PPT, smem, s>>>(views, begin, nviews, total, queue, consistent,
-                                                                  err);
+    render_bwd_multi_kernel<PPT, B, kConsistent><<<grid, 256 / PPT, smem, s>>>(views, begin, nviews, total, queue,
+                                                                               err);
+}
+
+template <int PPT, int B>
+void bwd_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, uint32_t total, uint32_t* queue,
+                      int consistent, unsigned* err, cudaStream_t s)
+{
+    if (consistent) bwd_multi_launch_mode<PPT, B, true>(views, begin, nviews, total, queue, err, s);
+    else bwd_multi_launch_mode<PPT, B, false>(views, begin, nviews, total, queue, err, s);
 }
 }  // namespace
 
