@@ -27,29 +27,25 @@ __device__ __forceinline__ float3 dnormvdv(float3 v, float3 dv)
     const float sum2 = v.x * v.x + v.y * v.y + v.z * v.z;
     const float invsum32 = 1.0f / sqrtf(sum2 * sum2 * sum2);
     float3 r;
-    r.x = ((+sum2 - v.x * v.x) * dv.x - v.y * v.x * dv.y - v.z * v.x * dv.z) * invsum32;
-    r.y = (-v.x * v.y * dv.x + (sum2 - v.y * v.y) * dv.y - v.z * v.y * dv.z) * invsum32;
-    r.z = (-v.x * v.z * dv.x - v.y * v.z * dv.y + (sum2 - v.z * v.z) * dv.z) * invsum32;
+    // the last product rounded on its own: callers add the result to other terms, and an
+    // add fused into it would round differently in different kernels
+    r.x = __fmul_rn((+sum2 - v.x * v.x) * dv.x - v.y * v.x * dv.y - v.z * v.x * dv.z, invsum32);
+    r.y = __fmul_rn(-v.x * v.y * dv.x + (sum2 - v.y * v.y) * dv.y - v.z * v.y * dv.z, invsum32);
+    r.z = __fmul_rn(-v.x * v.z * dv.x - v.y * v.z * dv.y + (sum2 - v.z * v.z) * dv.z, invsum32);
     return r;
 }
 
-// backward.cu:20-139 for one Gaussian; shrow / dsh are its [M][3] rows (added to
-// dsh instead of stored when kAccum; vec: both rows 16-byte aligned, M*3 % 4 == 0).
-// dL/dsh depends only on the direction, so it is written before the SH row is
-// read: the two 48-float sets are never live at the same time.
-template <bool kAccum>
-__device__ __forceinline__ float3 sh_backward(int deg, const float* __restrict__ shrow, float3 pos, float3 campos,
-                                              uint8_t clamp_bits, float3 dcol, float* __restrict__ dsh, int M,
-                                              bool vec)
+// SH basis at the unit view direction of a Gaussian at pos seen from campos
+// (backward.cu:20-57): dL/dsh[i][c] = B[i] * dL/dcolor[c].
+__device__ __forceinline__ void sh_basis(float3 pos, float3 campos, float3& dir_orig, float& x, float& y, float& z,
+                                         float (&B)[16])
 {
-    const float3 dir_orig = {pos.x - campos.x, pos.y - campos.y, pos.z - campos.z};
+    dir_orig = {pos.x - campos.x, pos.y - campos.y, pos.z - campos.z};
     const float len = sqrtf(dir_orig.x * dir_orig.x + dir_orig.y * dir_orig.y + dir_orig.z * dir_orig.z);
-    const float x = dir_orig.x / len, y = dir_orig.y / len, z = dir_orig.z / len;
-    const float d[3] = {(clamp_bits & 1) ? 0.f : dcol.x, (clamp_bits & 2) ? 0.f : dcol.y,
-                        (clamp_bits & 4) ? 0.f : dcol.z};
+    x = dir_orig.x / len;
+    y = dir_orig.y / len;
+    z = dir_orig.z / len;
     const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
-    // basis values (dL/dsh[i][c] = B[i] * d[c])
-    float B[16];
     B[0] = kSH_C0;
     B[1] = -kSH_C1 * y;
     B[2] = kSH_C1 * z;
@@ -66,50 +62,15 @@ __device__ __forceinline__ float3 sh_backward(int deg, const float* __restrict__
     B[13] = kSH_C3_4 * x * (4.f * zz - xx - yy);
     B[14] = kSH_C3_5 * z * (xx - yy);
     B[15] = kSH_C3_6 * x * (xx - 3.f * yy);
-    const int ncoef = (deg + 1) * (deg + 1);
-    const int nfl = M * 3;
-#define FGS_DSH(f) (((f) / 3 < ncoef) ? B[(f) / 3] * d[(f) % 3] : 0.f)
-    if (vec) {
-        float4* d4 = reinterpret_cast<float4*>(dsh);
-#pragma unroll
-        for (int v = 0; v < 12; v++)
-            if (4 * v < nfl) {
-                float4 o = make_float4(FGS_DSH(4 * v), FGS_DSH(4 * v + 1), FGS_DSH(4 * v + 2), FGS_DSH(4 * v + 3));
-                if (kAccum) {
-                    const float4 a = d4[v];
-                    o.x += a.x; o.y += a.y; o.z += a.z; o.w += a.w;
-                }
-                d4[v] = o;
-            }
-    } else {
-#pragma unroll
-        for (int f = 0; f < 48; f++)
-            if (f < nfl) {
-                if (kAccum) dsh[f] += FGS_DSH(f);
-                else dsh[f] = FGS_DSH(f);
-            }
-    }
-#undef FGS_DSH
-    if (!kAccum)
-        for (int f = 48; f < nfl; f++) dsh[f] = 0.f;
-    if (deg == 0) return make_float3(0.f, 0.f, 0.f);
+}
 
-    // dRGB/ddir (backward.cu:59-124 expression order) from the SH row
-    float sh[48];
-    const int nf = min(48, nfl);
-    if (vec) {
-        const float4* r4 = reinterpret_cast<const float4*>(shrow);
-#pragma unroll
-        for (int v = 0; v < 12; v++)
-            if (4 * v < nf) {
-                const float4 q = __ldg(r4 + v);
-                sh[4 * v] = q.x; sh[4 * v + 1] = q.y; sh[4 * v + 2] = q.z; sh[4 * v + 3] = q.w;
-            }
-    } else {
-#pragma unroll
-        for (int f = 0; f < 48; f++)
-            if (f < nf) sh[f] = __ldg(shrow + f);
-    }
+// dL/dmean3D through the view direction (backward.cu:59-139, the expression
+// order of the reference): dRGB/ddir from the SH coefficients sh (deg > 0), dotted
+// with the clamp-masked dL/dcolor d, through the normalisation.
+__device__ __forceinline__ float3 sh_ddir(int deg, const float (&sh)[48], float x, float y, float z,
+                                          const float (&d)[3], float3 dir_orig)
+{
+    const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
     float dx[3], dy[3], dz[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -148,6 +109,30 @@ __device__ __forceinline__ float3 sh_backward(int deg, const float* __restrict__
     return dnormvdv(dir_orig, ddir);
 }
 
+// dL/dsh of float f of an [M][3] row: basis value times masked colour gradient.
+__device__ __forceinline__ float sh_dsh(int f, int ncoef, const float (&B)[16], const float (&d)[3])
+{
+    return (f / 3 < ncoef) ? __fmul_rn(B[f / 3], d[f % 3]) : 0.f;
+}
+
+// The SH coefficients of one Gaussian (nf <= 48 floats; vec: 16-byte aligned row).
+__device__ __forceinline__ void load_sh_row(const float* __restrict__ shrow, int nf, bool vec, float (&sh)[48])
+{
+    if (vec) {
+        const float4* r4 = reinterpret_cast<const float4*>(shrow);
+#pragma unroll
+        for (int v = 0; v < 12; v++)
+            if (4 * v < nf) {
+                const float4 q = __ldg(r4 + v);
+                sh[4 * v] = q.x; sh[4 * v + 1] = q.y; sh[4 * v + 2] = q.z; sh[4 * v + 3] = q.w;
+            }
+    } else {
+#pragma unroll
+        for (int f = 0; f < 48; f++)
+            if (f < nf) sh[f] = __ldg(shrow + f);
+    }
+}
+
 // Screen-space gradients of the visible Gaussians: the sum of each Gaussian's
 // per-pair gradients (pgrad rows at its emission indices, its tiles row-major).
 // Gaussians are taken in depth rank j, whose pairs are the contiguous rows
@@ -162,8 +147,7 @@ __global__ void __launch_bounds__(256)
     pair_grad_gather_kernel(const uint32_t* __restrict__ visible_ids, const unsigned long long* __restrict__ totals,
                             const uint32_t* __restrict__ pair_off, const float* __restrict__ pgrad,
                             float* __restrict__ dmean2D, float* __restrict__ dconic, float* __restrict__ dcolor,
-                            float* __restrict__ dopac, float* __restrict__ dens_grad, int* __restrict__ dens_count,
-                            uint8_t* __restrict__ dens_flag)
+                            float* __restrict__ dopac, uint32_t* __restrict__ vis, uint32_t vis_bit)
 {
     const uint32_t K = (uint32_t)totals[0], V = (uint32_t)totals[1];
     const int lane = threadIdx.x & 31;
@@ -197,15 +181,7 @@ __global__ void __launch_bounds__(256)
             for (int u = 0; u < 4; u++)
                 if (k + 32 * u < ne) acc += warp_transpose_sum9(v[u]);
         }
-        if (dens_grad) {
-            // densification statistics (LoG/model/counter.py): |dL/dmean2D[:2]| and visibility
-            const float gx = __shfl_sync(0xffffffffu, acc, 6), gy = __shfl_sync(0xffffffffu, acc, 8);
-            if (lane == 0) {
-                dens_grad[idx] += sqrtf(gx * gx + gy * gy);
-                dens_count[idx] += 1;
-                dens_flag[idx] = 1;
-            }
-        }
+        if (vis && lane == 0) atomicOr(vis + idx, vis_bit);  // this view sees Gaussian idx
         if (lane < 18 && !(lane & 1)) {
             const int q = lane >> 1;
             float* dst = q < 3 ? dcolor + 3 * idx + q
@@ -222,283 +198,387 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// kAccum: add this view's gradients into dense buffers shared by several views
-// (views run one after another on a stream, so each row has one writer at a
-// time) and fold the view's opacity gradient into shared_dopac.
-template <bool kAccum>
-__global__ void __launch_bounds__(256)
-    preprocess_bwd_kernel(PreParams p, const uint32_t* __restrict__ visible_ids,
-                          const unsigned long long* __restrict__ visible_count, float* __restrict__ dmean2D,
-                          const float* __restrict__ dconic, float* __restrict__ dopac, float* __restrict__ dmean3D,
-                          float* __restrict__ dcov3D,
-                          float* __restrict__ dscale, float* __restrict__ drot, int consistent,
-                          float* __restrict__ shared_dopac, bool sh_follows)
+// One view's geometric backward of Gaussian idx (backward.cu:144-396 without the
+// SH part): from its screen-space gradients (g2x, g2y of dL/dmean2D, dL/dconic) to
+// the geometric dL/dmean3D, dL/dcov3D and, with want_sr, dL/dscale and
+// dL/drotation.  floor_mask: the consistent mode gives no opacity gradient to an
+// opacity under the 1e-6 floor.
+struct GeoGrad {
+    float3 dm;
+    float dc[6];
+    float ds[3];
+    float4 dq;
+    bool floor_mask;
+};
+
+__device__ __forceinline__ void geo_backward(const PreParams& p, int idx, float g2x, float g2y, float3 dL_dconic,
+                                             int consistent, bool want_sr, GeoGrad& o)
 {
-    // The forward's depth ordering put the V visible Gaussians first; culled
-    // rows were zero-filled by the launcher.
-    const uint32_t V = (uint32_t)*visible_count;
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < V; j += gridDim.x * blockDim.x) {
-    const int idx = (int)visible_ids[j];
-    float3 dm = {0.f, 0.f, 0.f};
-    float dc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    {
-        const float3 mean = {p.means[3 * idx], p.means[3 * idx + 1], p.means[3 * idx + 2]};
-        float cov3D[6];
-        if (p.cov3D) {
+    o.dm = {0.f, 0.f, 0.f};
 #pragma unroll
-            for (int k = 0; k < 6; k++) cov3D[k] = p.cov3D[6 * (size_t)idx + k];
-        } else {
-            const float4 q = {p.rots[4 * idx], p.rots[4 * idx + 1], p.rots[4 * idx + 2], p.rots[4 * idx + 3]};
-            cov3d_from_scale_rot(p.scales[3 * idx], p.scales[3 * idx + 1], p.scales[3 * idx + 2], p.scale_mod, q,
-                                 cov3D);
-        }
-        if (p.filter3d > 0.f) {
-            const float3 pv = xform_point4x3(mean, p.view);
-            const float sf = p.filter3d * pv.z / p.fx;
-            const float v = sf * sf;
-            cov3D[0] += v; cov3D[3] += v; cov3D[5] += v;
-        }
-        const float3 dL_dconic = {dconic[4 * idx], dconic[4 * idx + 1], dconic[4 * idx + 3]};
-        Ewa e;
-        const float3 c2 = ewa_cov2d(mean, p.fx, p.fy, p.tanx, p.tany, cov3D, p.view, &e);
-        float a, b = c2.y, c;
-        float mask_a = 1.f, mask_c = 1.f;
-        if (consistent) {
-            if (p.use_filter) {
-                a = dilate_max(c2.x);
-                c = dilate_max(c2.z);
-                if (!((double)c2.x > 0.3)) mask_a = 0.f;
-                if (!((double)c2.z > 0.3)) mask_c = 0.f;
-            } else {
-                a = c2.x;
-                c = c2.z;
-            }
-        } else {
-            a = dilate_add(c2.x);
-            c = dilate_add(c2.z);
-        }
-        const float denom = a * c - b * b;
-        float dL_da = 0, dL_db = 0, dL_dc = 0;
-        const float denom2inv = consistent ? 1.0f / (denom * denom) : 1.0f / ((denom * denom) + 0.0000001f);
-        const M3& T = e.T;
-        if (denom2inv != 0) {
-            dL_da = denom2inv * (-c * c * dL_dconic.x + 2 * b * c * dL_dconic.y + (denom - a * c) * dL_dconic.z);
-            dL_dc = denom2inv * (-a * a * dL_dconic.z + 2 * a * b * dL_dconic.y + (denom - a * c) * dL_dconic.x);
-            dL_db = denom2inv * 2 * (b * c * dL_dconic.x - (denom + 2 * b * b) * dL_dconic.y + a * b * dL_dconic.z);
-            dL_da *= mask_a;
-            dL_dc *= mask_c;
-            dc[0] = (T.m[0][0] * T.m[0][0] * dL_da + T.m[0][0] * T.m[1][0] * dL_db + T.m[1][0] * T.m[1][0] * dL_dc);
-            dc[3] = (T.m[0][1] * T.m[0][1] * dL_da + T.m[0][1] * T.m[1][1] * dL_db + T.m[1][1] * T.m[1][1] * dL_dc);
-            dc[5] = (T.m[0][2] * T.m[0][2] * dL_da + T.m[0][2] * T.m[1][2] * dL_db + T.m[1][2] * T.m[1][2] * dL_dc);
-            dc[1] = 2 * T.m[0][0] * T.m[0][1] * dL_da + (T.m[0][0] * T.m[1][1] + T.m[0][1] * T.m[1][0]) * dL_db +
-                    2 * T.m[1][0] * T.m[1][1] * dL_dc;
-            dc[2] = 2 * T.m[0][0] * T.m[0][2] * dL_da + (T.m[0][0] * T.m[1][2] + T.m[0][2] * T.m[1][0]) * dL_db +
-                    2 * T.m[1][0] * T.m[1][2] * dL_dc;
-            dc[4] = 2 * T.m[0][2] * T.m[0][1] * dL_da + (T.m[0][1] * T.m[1][2] + T.m[0][2] * T.m[1][1]) * dL_db +
-                    2 * T.m[1][1] * T.m[1][2] * dL_dc;
-        }
-        // Vrk[c][r]
-        const float V00 = cov3D[0], V01 = cov3D[1], V02 = cov3D[2], V11 = cov3D[3], V12 = cov3D[4], V22 = cov3D[5];
-        const float V10 = V01, V20 = V02, V21 = V12;
-        const float dL_dT00 = 2 * (T.m[0][0] * V00 + T.m[0][1] * V01 + T.m[0][2] * V02) * dL_da +
-                              (T.m[1][0] * V00 + T.m[1][1] * V01 + T.m[1][2] * V02) * dL_db;
-        const float dL_dT01 = 2 * (T.m[0][0] * V10 + T.m[0][1] * V11 + T.m[0][2] * V12) * dL_da +
-                              (T.m[1][0] * V10 + T.m[1][1] * V11 + T.m[1][2] * V12) * dL_db;
-        const float dL_dT02 = 2 * (T.m[0][0] * V20 + T.m[0][1] * V21 + T.m[0][2] * V22) * dL_da +
-                              (T.m[1][0] * V20 + T.m[1][1] * V21 + T.m[1][2] * V22) * dL_db;
-        const float dL_dT10 = 2 * (T.m[1][0] * V00 + T.m[1][1] * V01 + T.m[1][2] * V02) * dL_dc +
-                              (T.m[0][0] * V00 + T.m[0][1] * V01 + T.m[0][2] * V02) * dL_db;
-        const float dL_dT11 = 2 * (T.m[1][0] * V10 + T.m[1][1] * V11 + T.m[1][2] * V12) * dL_dc +
-                              (T.m[0][0] * V10 + T.m[0][1] * V11 + T.m[0][2] * V12) * dL_db;
-        const float dL_dT12 = 2 * (T.m[1][0] * V20 + T.m[1][1] * V21 + T.m[1][2] * V22) * dL_dc +
-                              (T.m[0][0] * V20 + T.m[0][1] * V21 + T.m[0][2] * V22) * dL_db;
-        // W[c][r] = view[c + 4r]
-        const float* v = p.view;
-        const float dL_dJ00 = v[0] * dL_dT00 + v[4] * dL_dT01 + v[8] * dL_dT02;
-        const float dL_dJ02 = v[2] * dL_dT00 + v[6] * dL_dT01 + v[10] * dL_dT02;
-        const float dL_dJ11 = v[1] * dL_dT10 + v[5] * dL_dT11 + v[9] * dL_dT12;
-        const float dL_dJ12 = v[2] * dL_dT10 + v[6] * dL_dT11 + v[10] * dL_dT12;
-        const float tz = 1.f / e.tz;
-        const float tz2 = tz * tz;
-        const float tz3 = tz2 * tz;
-        const float x_grad_mul = e.xclamp ? 0 : 1;
-        const float y_grad_mul = e.yclamp ? 0 : 1;
-        const float dL_dtx = x_grad_mul * -p.fx * tz2 * dL_dJ02;
-        const float dL_dty = y_grad_mul * -p.fy * tz2 * dL_dJ12;
-        float dL_dtz = -p.fx * tz2 * dL_dJ00 - p.fy * tz2 * dL_dJ11 + (2 * p.fx * e.tx) * tz3 * dL_dJ02 +
-                       (2 * p.fy * e.ty) * tz3 * dL_dJ12;
-        if (consistent) {
-            const float limx = 1.3f * p.tanx, limy = 1.3f * p.tany;
-            if (e.xclamp) dL_dtz += (-p.fx * tz2 * dL_dJ02) * (e.txtz < 0 ? -limx : limx);
-            if (e.yclamp) dL_dtz += (-p.fy * tz2 * dL_dJ12) * (e.tytz < 0 ? -limy : limy);
-        }
-        // transformVec4x3Transpose
-        dm.x = v[0] * dL_dtx + v[1] * dL_dty + v[2] * dL_dtz;
-        dm.y = v[4] * dL_dtx + v[5] * dL_dty + v[6] * dL_dtz;
-        dm.z = v[8] * dL_dtx + v[9] * dL_dty + v[10] * dL_dtz;
-
-        // backward.cu:370-387: screen-space mean gradient through the projection
-        const float* pr = p.proj;
-        const float4 m_hom = xform_point4x4(mean, pr);
-        const float m_w = 1.0f / (m_hom.w + 0.0000001f);
-        const float mul1 = (pr[0] * mean.x + pr[4] * mean.y + pr[8] * mean.z + pr[12]) * m_w * m_w;
-        const float mul2 = (pr[1] * mean.x + pr[5] * mean.y + pr[9] * mean.z + pr[13]) * m_w * m_w;
-        const float g2x = dmean2D[3 * idx], g2y = dmean2D[3 * idx + 1];
-        dm.x += (pr[0] * m_w - pr[3] * mul1) * g2x + (pr[1] * m_w - pr[3] * mul2) * g2y;
-        dm.y += (pr[4] * m_w - pr[7] * mul1) * g2x + (pr[5] * m_w - pr[7] * mul2) * g2y;
-        dm.z += (pr[8] * m_w - pr[11] * mul1) * g2x + (pr[9] * m_w - pr[11] * mul2) * g2y;
-
-        if (p.scales && dscale) {
-            // backward.cu:278-341 (gradient w.r.t. the quaternion as given)
-            const float r = p.rots[4 * idx], x = p.rots[4 * idx + 1], y = p.rots[4 * idx + 2], z = p.rots[4 * idx + 3];
-            const M3 R = m3_cols(1.f - 2.f * (y * y + z * z), 2.f * (x * y - r * z), 2.f * (x * z + r * y),
-                                 2.f * (x * y + r * z), 1.f - 2.f * (x * x + z * z), 2.f * (y * z - r * x),
-                                 2.f * (x * z - r * y), 2.f * (y * z + r * x), 1.f - 2.f * (x * x + y * y));
-            const float s[3] = {p.scale_mod * p.scales[3 * idx], p.scale_mod * p.scales[3 * idx + 1],
-                                p.scale_mod * p.scales[3 * idx + 2]};
-            M3 S = m3_cols(1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f);
-            S.m[0][0] = s[0]; S.m[1][1] = s[1]; S.m[2][2] = s[2];
-            const M3 M = m3_mul(S, R);
-            const M3 dSig = m3_cols(dc[0], 0.5f * dc[1], 0.5f * dc[2], 0.5f * dc[1], dc[3], 0.5f * dc[4], 0.5f * dc[2],
-                                    0.5f * dc[4], dc[5]);
-            M3 M2;
+    for (int k = 0; k < 6; k++) o.dc[k] = 0.f;
+    const float3 mean = {p.means[3 * idx], p.means[3 * idx + 1], p.means[3 * idx + 2]};
+    float cov3D[6];
+    if (p.cov3D) {
 #pragma unroll
-            for (int cc = 0; cc < 3; cc++)
-#pragma unroll
-                for (int rr = 0; rr < 3; rr++) M2.m[cc][rr] = 2.0f * M.m[cc][rr];
-            const M3 dM = m3_mul(M2, dSig);
-            const M3 Rt = m3_t(R);
-            M3 dMt = m3_t(dM);
-            float* ds = dscale + 3 * (size_t)idx;
-#pragma unroll
-            for (int cc = 0; cc < 3; cc++)
-            {
-                const float v = Rt.m[cc][0] * dMt.m[cc][0] + Rt.m[cc][1] * dMt.m[cc][1] + Rt.m[cc][2] * dMt.m[cc][2];
-                if (kAccum) ds[cc] += v;
-                else ds[cc] = v;
-            }
-#pragma unroll
-            for (int cc = 0; cc < 3; cc++)
-#pragma unroll
-                for (int rr = 0; rr < 3; rr++) dMt.m[cc][rr] *= s[cc];
-            float4 dq;
-            dq.x = 2 * z * (dMt.m[0][1] - dMt.m[1][0]) + 2 * y * (dMt.m[2][0] - dMt.m[0][2]) +
-                   2 * x * (dMt.m[1][2] - dMt.m[2][1]);
-            dq.y = 2 * y * (dMt.m[1][0] + dMt.m[0][1]) + 2 * z * (dMt.m[2][0] + dMt.m[0][2]) +
-                   2 * r * (dMt.m[1][2] - dMt.m[2][1]) - 4 * x * (dMt.m[2][2] + dMt.m[1][1]);
-            dq.z = 2 * x * (dMt.m[1][0] + dMt.m[0][1]) + 2 * r * (dMt.m[2][0] - dMt.m[0][2]) +
-                   2 * z * (dMt.m[1][2] + dMt.m[2][1]) - 4 * y * (dMt.m[2][2] + dMt.m[0][0]);
-            dq.w = 2 * r * (dMt.m[0][1] - dMt.m[1][0]) + 2 * x * (dMt.m[2][0] + dMt.m[0][2]) +
-                   2 * y * (dMt.m[1][2] + dMt.m[2][1]) - 4 * z * (dMt.m[1][1] + dMt.m[0][0]);
-            float* dr = drot + 4 * (size_t)idx;
-            if (kAccum) {
-                dr[0] += dq.x; dr[1] += dq.y; dr[2] += dq.z; dr[3] += dq.w;
-            } else {
-                dr[0] = dq.x; dr[1] = dq.y; dr[2] = dq.z; dr[3] = dq.w;
-            }
-        }
-        const bool floor_mask = consistent && p.opac && p.opac[idx] < 1e-6f;
-        if (kAccum) {
-            if (!floor_mask) shared_dopac[idx] += dopac[idx];
-        } else if (floor_mask) {
-            dopac[idx] = 0.f;
-        }
-    }
-    if (kAccum && sh_follows) {
-        // the SH pass adds its term and then accumulates the view's total (the same
-        // sum, in the same order, as the plain backward of this view)
-        dmean2D[3 * idx] = dm.x;
-        dmean2D[3 * idx + 1] = dm.y;
-        dmean2D[3 * idx + 2] = dm.z;
-#pragma unroll
-        for (int k = 0; k < 6; k++) dcov3D[6 * (size_t)idx + k] += dc[k];
-    } else if (kAccum) {
-        dmean3D[3 * idx] += dm.x;
-        dmean3D[3 * idx + 1] += dm.y;
-        dmean3D[3 * idx + 2] += dm.z;
-#pragma unroll
-        for (int k = 0; k < 6; k++) dcov3D[6 * (size_t)idx + k] += dc[k];
+        for (int k = 0; k < 6; k++) cov3D[k] = p.cov3D[6 * (size_t)idx + k];
     } else {
-        dmean3D[3 * idx] = dm.x;
-        dmean3D[3 * idx + 1] = dm.y;
-        dmean3D[3 * idx + 2] = dm.z;
-#pragma unroll
-        for (int k = 0; k < 6; k++) dcov3D[6 * (size_t)idx + k] = dc[k];
+        const float4 q = {p.rots[4 * idx], p.rots[4 * idx + 1], p.rots[4 * idx + 2], p.rots[4 * idx + 3]};
+        cov3d_from_scale_rot(p.scales[3 * idx], p.scales[3 * idx + 1], p.scales[3 * idx + 2], p.scale_mod, q,
+                             cov3D);
     }
+    if (p.filter3d > 0.f) {
+        const float3 pv = xform_point4x3(mean, p.view);
+        const float sf = p.filter3d * pv.z / p.fx;
+        const float v = sf * sf;
+        cov3D[0] += v; cov3D[3] += v; cov3D[5] += v;
+    }
+    Ewa e;
+    const float3 c2 = ewa_cov2d(mean, p.fx, p.fy, p.tanx, p.tany, cov3D, p.view, &e);
+    float a, b = c2.y, c;
+    float mask_a = 1.f, mask_c = 1.f;
+    if (consistent) {
+        if (p.use_filter) {
+            a = dilate_max(c2.x);
+            c = dilate_max(c2.z);
+            if (!((double)c2.x > 0.3)) mask_a = 0.f;
+            if (!((double)c2.z > 0.3)) mask_c = 0.f;
+        } else {
+            a = c2.x;
+            c = c2.z;
+        }
+    } else {
+        a = dilate_add(c2.x);
+        c = dilate_add(c2.z);
+    }
+    const float denom = a * c - b * b;
+    float dL_da = 0, dL_db = 0, dL_dc = 0;
+    const float denom2inv = consistent ? 1.0f / (denom * denom) : 1.0f / ((denom * denom) + 0.0000001f);
+    const M3& T = e.T;
+    if (denom2inv != 0) {
+        dL_da = denom2inv * (-c * c * dL_dconic.x + 2 * b * c * dL_dconic.y + (denom - a * c) * dL_dconic.z);
+        dL_dc = denom2inv * (-a * a * dL_dconic.z + 2 * a * b * dL_dconic.y + (denom - a * c) * dL_dconic.x);
+        dL_db = denom2inv * 2 * (b * c * dL_dconic.x - (denom + 2 * b * b) * dL_dconic.y + a * b * dL_dconic.z);
+        dL_da *= mask_a;
+        dL_dc *= mask_c;
+        o.dc[0] = (T.m[0][0] * T.m[0][0] * dL_da + T.m[0][0] * T.m[1][0] * dL_db + T.m[1][0] * T.m[1][0] * dL_dc);
+        o.dc[3] = (T.m[0][1] * T.m[0][1] * dL_da + T.m[0][1] * T.m[1][1] * dL_db + T.m[1][1] * T.m[1][1] * dL_dc);
+        o.dc[5] = (T.m[0][2] * T.m[0][2] * dL_da + T.m[0][2] * T.m[1][2] * dL_db + T.m[1][2] * T.m[1][2] * dL_dc);
+        o.dc[1] = 2 * T.m[0][0] * T.m[0][1] * dL_da + (T.m[0][0] * T.m[1][1] + T.m[0][1] * T.m[1][0]) * dL_db +
+                  2 * T.m[1][0] * T.m[1][1] * dL_dc;
+        o.dc[2] = 2 * T.m[0][0] * T.m[0][2] * dL_da + (T.m[0][0] * T.m[1][2] + T.m[0][2] * T.m[1][0]) * dL_db +
+                  2 * T.m[1][0] * T.m[1][2] * dL_dc;
+        o.dc[4] = 2 * T.m[0][2] * T.m[0][1] * dL_da + (T.m[0][1] * T.m[1][2] + T.m[0][2] * T.m[1][1]) * dL_db +
+                  2 * T.m[1][1] * T.m[1][2] * dL_dc;
+    }
+    // Vrk[c][r]
+    const float V00 = cov3D[0], V01 = cov3D[1], V02 = cov3D[2], V11 = cov3D[3], V12 = cov3D[4], V22 = cov3D[5];
+    const float V10 = V01, V20 = V02, V21 = V12;
+    const float dL_dT00 = 2 * (T.m[0][0] * V00 + T.m[0][1] * V01 + T.m[0][2] * V02) * dL_da +
+                          (T.m[1][0] * V00 + T.m[1][1] * V01 + T.m[1][2] * V02) * dL_db;
+    const float dL_dT01 = 2 * (T.m[0][0] * V10 + T.m[0][1] * V11 + T.m[0][2] * V12) * dL_da +
+                          (T.m[1][0] * V10 + T.m[1][1] * V11 + T.m[1][2] * V12) * dL_db;
+    const float dL_dT02 = 2 * (T.m[0][0] * V20 + T.m[0][1] * V21 + T.m[0][2] * V22) * dL_da +
+                          (T.m[1][0] * V20 + T.m[1][1] * V21 + T.m[1][2] * V22) * dL_db;
+    const float dL_dT10 = 2 * (T.m[1][0] * V00 + T.m[1][1] * V01 + T.m[1][2] * V02) * dL_dc +
+                          (T.m[0][0] * V00 + T.m[0][1] * V01 + T.m[0][2] * V02) * dL_db;
+    const float dL_dT11 = 2 * (T.m[1][0] * V10 + T.m[1][1] * V11 + T.m[1][2] * V12) * dL_dc +
+                          (T.m[0][0] * V10 + T.m[0][1] * V11 + T.m[0][2] * V12) * dL_db;
+    const float dL_dT12 = 2 * (T.m[1][0] * V20 + T.m[1][1] * V21 + T.m[1][2] * V22) * dL_dc +
+                          (T.m[0][0] * V20 + T.m[0][1] * V21 + T.m[0][2] * V22) * dL_db;
+    // W[c][r] = view[c + 4r]
+    const float* v = p.view;
+    const float dL_dJ00 = v[0] * dL_dT00 + v[4] * dL_dT01 + v[8] * dL_dT02;
+    const float dL_dJ02 = v[2] * dL_dT00 + v[6] * dL_dT01 + v[10] * dL_dT02;
+    const float dL_dJ11 = v[1] * dL_dT10 + v[5] * dL_dT11 + v[9] * dL_dT12;
+    const float dL_dJ12 = v[2] * dL_dT10 + v[6] * dL_dT11 + v[10] * dL_dT12;
+    const float tz = 1.f / e.tz;
+    const float tz2 = tz * tz;
+    const float tz3 = tz2 * tz;
+    const float x_grad_mul = e.xclamp ? 0 : 1;
+    const float y_grad_mul = e.yclamp ? 0 : 1;
+    const float dL_dtx = x_grad_mul * -p.fx * tz2 * dL_dJ02;
+    const float dL_dty = y_grad_mul * -p.fy * tz2 * dL_dJ12;
+    float dL_dtz = -p.fx * tz2 * dL_dJ00 - p.fy * tz2 * dL_dJ11 + (2 * p.fx * e.tx) * tz3 * dL_dJ02 +
+                   (2 * p.fy * e.ty) * tz3 * dL_dJ12;
+    if (consistent) {
+        const float limx = 1.3f * p.tanx, limy = 1.3f * p.tany;
+        if (e.xclamp) dL_dtz += (-p.fx * tz2 * dL_dJ02) * (e.txtz < 0 ? -limx : limx);
+        if (e.yclamp) dL_dtz += (-p.fy * tz2 * dL_dJ12) * (e.tytz < 0 ? -limy : limy);
+    }
+    // transformVec4x3Transpose
+    o.dm.x = v[0] * dL_dtx + v[1] * dL_dty + v[2] * dL_dtz;
+    o.dm.y = v[4] * dL_dtx + v[5] * dL_dty + v[6] * dL_dtz;
+    o.dm.z = v[8] * dL_dtx + v[9] * dL_dty + v[10] * dL_dtz;
+
+    // backward.cu:370-387: screen-space mean gradient through the projection
+    const float* pr = p.proj;
+    const float4 m_hom = xform_point4x4(mean, pr);
+    const float m_w = 1.0f / (m_hom.w + 0.0000001f);
+    const float mul1 = (pr[0] * mean.x + pr[4] * mean.y + pr[8] * mean.z + pr[12]) * m_w * m_w;
+    const float mul2 = (pr[1] * mean.x + pr[5] * mean.y + pr[9] * mean.z + pr[13]) * m_w * m_w;
+    o.dm.x += (pr[0] * m_w - pr[3] * mul1) * g2x + (pr[1] * m_w - pr[3] * mul2) * g2y;
+    o.dm.y += (pr[4] * m_w - pr[7] * mul1) * g2x + (pr[5] * m_w - pr[7] * mul2) * g2y;
+    o.dm.z += (pr[8] * m_w - pr[11] * mul1) * g2x + (pr[9] * m_w - pr[11] * mul2) * g2y;
+
+    if (want_sr) {
+        // backward.cu:278-341 (gradient w.r.t. the quaternion as given)
+        const float r = p.rots[4 * idx], x = p.rots[4 * idx + 1], y = p.rots[4 * idx + 2], z = p.rots[4 * idx + 3];
+        const M3 R = m3_cols(1.f - 2.f * (y * y + z * z), 2.f * (x * y - r * z), 2.f * (x * z + r * y),
+                             2.f * (x * y + r * z), 1.f - 2.f * (x * x + z * z), 2.f * (y * z - r * x),
+                             2.f * (x * z - r * y), 2.f * (y * z + r * x), 1.f - 2.f * (x * x + y * y));
+        const float s[3] = {p.scale_mod * p.scales[3 * idx], p.scale_mod * p.scales[3 * idx + 1],
+                            p.scale_mod * p.scales[3 * idx + 2]};
+        M3 S = m3_cols(1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f);
+        S.m[0][0] = s[0]; S.m[1][1] = s[1]; S.m[2][2] = s[2];
+        const M3 M = m3_mul(S, R);
+        const M3 dSig = m3_cols(o.dc[0], 0.5f * o.dc[1], 0.5f * o.dc[2], 0.5f * o.dc[1], o.dc[3], 0.5f * o.dc[4],
+                                0.5f * o.dc[2], 0.5f * o.dc[4], o.dc[5]);
+        M3 M2;
+#pragma unroll
+        for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+            for (int rr = 0; rr < 3; rr++) M2.m[cc][rr] = 2.0f * M.m[cc][rr];
+        const M3 dM = m3_mul(M2, dSig);
+        const M3 Rt = m3_t(R);
+        M3 dMt = m3_t(dM);
+#pragma unroll
+        for (int cc = 0; cc < 3; cc++)
+            o.ds[cc] = Rt.m[cc][0] * dMt.m[cc][0] + Rt.m[cc][1] * dMt.m[cc][1] + Rt.m[cc][2] * dMt.m[cc][2];
+#pragma unroll
+        for (int cc = 0; cc < 3; cc++)
+#pragma unroll
+            for (int rr = 0; rr < 3; rr++) dMt.m[cc][rr] *= s[cc];
+        float4 dq;
+        dq.x = 2 * z * (dMt.m[0][1] - dMt.m[1][0]) + 2 * y * (dMt.m[2][0] - dMt.m[0][2]) +
+               2 * x * (dMt.m[1][2] - dMt.m[2][1]);
+        dq.y = 2 * y * (dMt.m[1][0] + dMt.m[0][1]) + 2 * z * (dMt.m[2][0] + dMt.m[0][2]) +
+               2 * r * (dMt.m[1][2] - dMt.m[2][1]) - 4 * x * (dMt.m[2][2] + dMt.m[1][1]);
+        dq.z = 2 * x * (dMt.m[1][0] + dMt.m[0][1]) + 2 * r * (dMt.m[2][0] - dMt.m[0][2]) +
+               2 * z * (dMt.m[1][2] + dMt.m[2][1]) - 4 * y * (dMt.m[2][2] + dMt.m[0][0]);
+        dq.w = 2 * r * (dMt.m[0][1] - dMt.m[1][0]) + 2 * x * (dMt.m[2][0] + dMt.m[0][2]) +
+               2 * y * (dMt.m[1][2] + dMt.m[2][1]) - 4 * z * (dMt.m[1][1] + dMt.m[0][0]);
+        o.dq = dq;
+    }
+    o.floor_mask = consistent && p.opac && p.opac[idx] < 1e-6f;
+}
+
+// ---------------------------------------------------------------- one pass per Gaussian over its views
+// The per-Gaussian part of the backward, for one view (the plain path) or many
+// (the batched path) with the same code, so that a batch's sums are the plain
+// per-view results added in view order, bit for bit.  A thread takes one
+// Gaussian, walks the views that saw it in view order, adds each view's whole
+// contribution into registers with explicit round-to-nearest adds (no multiply
+// of a per-view term is fused into them), then writes every output row once,
+// zeros for Gaussians no view saw: no zeroing passes, no launch per view, no
+// re-reading of shared rows per view.
+//
+// Which views saw Gaussian i: vis[(w * P) + i] bit b for view 32 w + b (the
+// batched path; set by the views' gathers), or, for one view, radii[i] > 0 (the
+// reference's backward gates every per-Gaussian gradient on it, backward.cu:156,367).
+__device__ __forceinline__ uint32_t views_of(const uint32_t* __restrict__ vis, const int* __restrict__ radii, int w,
+                                             int P, int i)
+{
+    return vis ? vis[(size_t)w * P + i] : (radii[i] > 0 ? 1u : 0u);
+}
+
+// Geometric part: dL/dopacity, dL/dscale, dL/drotation, dL/dcov3D (optional) and
+// each view's geometric dL/dmean3D in its dm_geo row for fold_sh_kernel (with
+// SH), else the dL/dmean3D sum itself.  Densification statistics (optional) as
+// densify passes run per view would add them.
+__global__ void __launch_bounds__(256)
+    fold_geo_kernel(const FoldView* __restrict__ views, FoldView single, int nviews, int P,
+                    const uint32_t* __restrict__ vis, const int* __restrict__ radii, int consistent, bool sh_follows,
+                    float* __restrict__ dmean3D, float* __restrict__ dopac_out, float* __restrict__ dcov3D,
+                    float* __restrict__ dscale, float* __restrict__ drot, DensifyStats dens)
+{
+    const int words = (nviews + 31) >> 5;
+    const bool want_sr = single.p.scales && dscale;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+        float3 am = {0.f, 0.f, 0.f};
+        float adc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float ads[3] = {0.f, 0.f, 0.f};
+        float4 adq = {0.f, 0.f, 0.f, 0.f};
+        float ado = 0.f;
+        float dg = 0.f;
+        int seen = 0;
+        for (int w = 0; w < words; w++) {
+            uint32_t m = views_of(vis, radii, w, P, i);
+            while (m) {
+                const int v = 32 * w + __ffs(m) - 1;
+                m &= m - 1;
+                const FoldView& fv = views ? views[v] : single;
+                const float g2x = fv.dmean2D[3 * i], g2y = fv.dmean2D[3 * i + 1];
+                if (dens.grad_sum) {
+                    if (seen == 0) dg = dens.grad_sum[i];
+                    dg = __fadd_rn(dg, sqrtf(g2x * g2x + g2y * g2y));
+                }
+                seen++;
+                GeoGrad o;
+                geo_backward(fv.p, i, g2x, g2y, {fv.dconic[4 * i], fv.dconic[4 * i + 1], fv.dconic[4 * i + 3]},
+                             consistent, want_sr, o);
+#pragma unroll
+                for (int k = 0; k < 6; k++) adc[k] = __fadd_rn(adc[k], o.dc[k]);
+                if (want_sr) {
+                    ads[0] = __fadd_rn(ads[0], o.ds[0]);
+                    ads[1] = __fadd_rn(ads[1], o.ds[1]);
+                    ads[2] = __fadd_rn(ads[2], o.ds[2]);
+                    adq.x = __fadd_rn(adq.x, o.dq.x);
+                    adq.y = __fadd_rn(adq.y, o.dq.y);
+                    adq.z = __fadd_rn(adq.z, o.dq.z);
+                    adq.w = __fadd_rn(adq.w, o.dq.w);
+                }
+                if (!o.floor_mask) ado = __fadd_rn(ado, fv.dopac[i]);
+                if (sh_follows) {
+                    fv.dm_geo[3 * i] = o.dm.x;
+                    fv.dm_geo[3 * i + 1] = o.dm.y;
+                    fv.dm_geo[3 * i + 2] = o.dm.z;
+                } else {
+                    am.x = __fadd_rn(am.x, o.dm.x);
+                    am.y = __fadd_rn(am.y, o.dm.y);
+                    am.z = __fadd_rn(am.z, o.dm.z);
+                }
+            }
+        }
+        dopac_out[i] = ado;
+        if (dcov3D)
+#pragma unroll
+            for (int k = 0; k < 6; k++) dcov3D[6 * (size_t)i + k] = adc[k];
+        if (want_sr) {
+            dscale[3 * (size_t)i] = ads[0]; dscale[3 * (size_t)i + 1] = ads[1]; dscale[3 * (size_t)i + 2] = ads[2];
+            drot[4 * (size_t)i] = adq.x; drot[4 * (size_t)i + 1] = adq.y;
+            drot[4 * (size_t)i + 2] = adq.z; drot[4 * (size_t)i + 3] = adq.w;
+        }
+        if (!sh_follows) {
+            dmean3D[3 * (size_t)i] = am.x; dmean3D[3 * (size_t)i + 1] = am.y; dmean3D[3 * (size_t)i + 2] = am.z;
+        }
+        if (dens.grad_sum && seen) {
+            dens.grad_sum[i] = dg;
+            dens.count[i] += seen;
+            dens.flag[i] = 1;
+        }
     }
 }
 
-// SH part of the per-Gaussian backward as its own pass over the visible ids
-// (after preprocess_bwd_kernel on the same stream): dL/dsh and the SH term of
-// dL/dmean, added to the row preprocess_bwd_kernel wrote.  Kept apart so that
-// neither kernel holds the 48-float SH rows next to the covariance chain.
-template <bool kAccum>
-__global__ void __launch_bounds__(256, 3)
-    sh_bwd_kernel(PreParams p, const uint32_t* __restrict__ visible_ids,
-                  const unsigned long long* __restrict__ visible_count, const uint8_t* __restrict__ clamped,
-                  const float* __restrict__ dcolor, const float* __restrict__ dm_geo, float* __restrict__ dmean3D,
-                  float* __restrict__ dsh)
+// SH part (backward.cu:20-139 per view): dL/dsh and dL/dmean3D = the sum over views
+// of (geometric term + SH direction term); the SH row is read once for all views.
+// dL/dsh depends only on the direction and the clamp-masked colour gradient.
+__global__ void __launch_bounds__(256)
+    fold_sh_kernel(const FoldView* __restrict__ views, FoldView single, int nviews, int P,
+                   const uint32_t* __restrict__ vis, const int* __restrict__ radii, float* __restrict__ dmean3D,
+                   float* __restrict__ dsh)
 {
-    const uint32_t V = (uint32_t)*visible_count;
-    const bool vec = p.aligned && ((p.M * 3) & 3) == 0;
-    const float3 cam = {p.campos[0], p.campos[1], p.campos[2]};
-    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < V; j += gridDim.x * blockDim.x) {
-        const int idx = (int)visible_ids[j];
-        const float3 mean = {p.means[3 * idx], p.means[3 * idx + 1], p.means[3 * idx + 2]};
-        const float3 dcol = {dcolor[3 * idx], dcolor[3 * idx + 1], dcolor[3 * idx + 2]};
-        const float3 dmd = sh_backward<kAccum>(p.D, p.shs + (size_t)idx * p.M * 3, mean, cam, clamped[idx], dcol,
-                                               dsh + (size_t)idx * p.M * 3, p.M, vec);
-        if (kAccum) {  // this view's total, then into the shared sum
-            dmean3D[3 * idx] += dm_geo[3 * idx] + dmd.x;
-            dmean3D[3 * idx + 1] += dm_geo[3 * idx + 1] + dmd.y;
-            dmean3D[3 * idx + 2] += dm_geo[3 * idx + 2] + dmd.z;
-        } else {
-            dmean3D[3 * idx] += dmd.x;
-            dmean3D[3 * idx + 1] += dmd.y;
-            dmean3D[3 * idx + 2] += dmd.z;
+    const int words = (nviews + 31) >> 5;
+    const PreParams& p = single.p;
+    const int deg = p.D, M = p.M, nfl = M * 3;
+    const int ncoef = (deg + 1) * (deg + 1);
+    const bool vec = p.aligned && (nfl & 3) == 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+        float* drow = dsh + (size_t)i * nfl;
+        float acc[48];
+#pragma unroll
+        for (int f = 0; f < 48; f++) acc[f] = 0.f;
+        float3 am = {0.f, 0.f, 0.f};
+        bool any = false;
+        for (int w = 0; w < words && !any; w++) any = views_of(vis, radii, w, P, i) != 0;
+        if (any) {
+            float sh[48];
+            if (deg > 0) load_sh_row(p.shs + (size_t)i * nfl, min(48, nfl), vec, sh);
+            const float3 mean = {p.means[3 * i], p.means[3 * i + 1], p.means[3 * i + 2]};
+            for (int w = 0; w < words; w++) {
+                uint32_t m = views_of(vis, radii, w, P, i);
+                while (m) {
+                    const int v = 32 * w + __ffs(m) - 1;
+                    m &= m - 1;
+                    const FoldView& fv = views ? views[v] : single;
+                    const float3 cam = {fv.p.campos[0], fv.p.campos[1], fv.p.campos[2]};
+                    float3 dir_orig;
+                    float x, y, z, B[16];
+                    sh_basis(mean, cam, dir_orig, x, y, z, B);
+                    const uint8_t cb = fv.clamped[i];
+                    const float d[3] = {(cb & 1) ? 0.f : fv.dcolor[3 * i], (cb & 2) ? 0.f : fv.dcolor[3 * i + 1],
+                                        (cb & 4) ? 0.f : fv.dcolor[3 * i + 2]};
+#pragma unroll
+                    for (int f = 0; f < 48; f++)
+                        if (f < nfl) acc[f] = __fadd_rn(acc[f], sh_dsh(f, ncoef, B, d));
+                    const float3 dmd = deg == 0 ? make_float3(0.f, 0.f, 0.f) : sh_ddir(deg, sh, x, y, z, d, dir_orig);
+                    am.x = __fadd_rn(am.x, __fadd_rn(fv.dm_geo[3 * i], dmd.x));
+                    am.y = __fadd_rn(am.y, __fadd_rn(fv.dm_geo[3 * i + 1], dmd.y));
+                    am.z = __fadd_rn(am.z, __fadd_rn(fv.dm_geo[3 * i + 2], dmd.z));
+                }
+            }
         }
+        if (vec) {
+            float4* d4 = reinterpret_cast<float4*>(drow);
+#pragma unroll
+            for (int v = 0; v < 12; v++)
+                if (4 * v < nfl) d4[v] = make_float4(acc[4 * v], acc[4 * v + 1], acc[4 * v + 2], acc[4 * v + 3]);
+        } else {
+#pragma unroll
+            for (int f = 0; f < 48; f++)
+                if (f < nfl) drow[f] = acc[f];
+        }
+        for (int f = 48; f < nfl; f++) drow[f] = 0.f;
+        dmean3D[3 * (size_t)i] = am.x; dmean3D[3 * (size_t)i + 1] = am.y; dmean3D[3 * (size_t)i + 2] = am.z;
     }
+}
+
+int gather_blocks(size_t n)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (int)std::min<size_t>((n + 255) / 256, (size_t)sms * 8);
+}
+
+void fold_launch(const FoldView* views, const FoldView& single, int nviews, int P, const uint32_t* vis,
+                 const int* radii, int consistent, bool sh, float* dmean3D, float* dopac, float* dcov3D, float* dsh,
+                 float* dscale, float* drot, const DensifyStats* dens, cudaStream_t s)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = (int)std::min<size_t>(((size_t)P + 255) / 256, (size_t)sms * 16);
+    const DensifyStats d = dens ? *dens : DensifyStats{nullptr, nullptr, nullptr};
+    fold_geo_kernel<<<blocks, 256, 0, s>>>(views, single, nviews, P, vis, radii, consistent, sh, dmean3D, dopac,
+                                           dcov3D, dscale, drot, d);
+    if (sh) fold_sh_kernel<<<blocks, 256, 0, s>>>(views, single, nviews, P, vis, radii, dmean3D, dsh);
+    note_launches(sh ? 2 : 1);
 }
 
 }  // namespace
 
-void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* pgrad, float* dmean2D, float* dconic,
-                           float* dcolor, float* dopac, float* dmean3D, float* dcov3D, float* dsh, float* dscale,
-                           float* drot, int consistent, cudaStream_t s, bool accumulate, float* shared_dopac,
-                           const DensifyStats* dens)
+void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const int* radii, const float* pgrad,
+                           float* dmean2D, float* dconic, float* dcolor, float* dopac, float* dmean3D, float* dcov3D,
+                           float* dsh, float* dscale, float* drot, int consistent, cudaStream_t s)
 {
     if (p.P <= 0) return;
-    const size_t P = (size_t)p.P;
-    if (!accumulate) {
-        // Dense outputs: culled rows are zero, written here at copy-engine speed.
-        cudaMemsetAsync(dmean3D, 0, sizeof(float) * 3 * P, s);
-        cudaMemsetAsync(dcov3D, 0, sizeof(float) * 6 * P, s);
-        if (dsh) cudaMemsetAsync(dsh, 0, sizeof(float) * 3 * (size_t)p.M * P, s);
-        if (dscale) cudaMemsetAsync(dscale, 0, sizeof(float) * 3 * P, s);
-        if (drot) cudaMemsetAsync(drot, 0, sizeof(float) * 4 * P, s);
-    }
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int blocks = (int)std::min<size_t>((P + 255) / 256, (size_t)sms * 8);
     const bool sh = p.shs && dsh;
-    pair_grad_gather_kernel<<<blocks, 256, 0, s>>>(g.sort_ids_b, g.total, g.pair_off, pgrad, dmean2D, dconic,
-                                                   dcolor, dopac, dens ? dens->grad_sum : nullptr,
-                                                   dens ? dens->count : nullptr, dens ? dens->flag : nullptr);
-    if (accumulate) {
-        preprocess_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, dmean2D, dconic, dopac,
-                                                           dmean3D, dcov3D, dscale, drot, consistent, shared_dopac, sh);
-        if (sh)
-            sh_bwd_kernel<true><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dcolor, dmean2D,
-                                                       dmean3D, dsh);
-    } else {
-        preprocess_bwd_kernel<false><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, dmean2D, dconic, dopac,
-                                                            dmean3D, dcov3D, dscale, drot, consistent, nullptr, sh);
-        if (sh)
-            sh_bwd_kernel<false><<<blocks, 256, 0, s>>>(p, g.sort_ids_b, g.total + 1, g.clamped, dcolor, nullptr,
-                                                        dmean3D, dsh);
-    }
-    note_launches(sh ? 3 : 2);
+    pair_grad_gather_kernel<<<gather_blocks((size_t)p.P), 256, 0, s>>>(g.sort_ids_b, g.total, g.pair_off, pgrad,
+                                                                       dmean2D, dconic, dcolor, dopac, nullptr, 0u);
+    note_launches(1);
+    // the view's geometric dL/dmean3D waits in the dL/dmean3D rows for the SH pass
+    const FoldView one{p, dmean3D, dmean2D, dconic, dopac, dcolor, g.clamped};
+    fold_launch(nullptr, one, 1, p.P, nullptr, radii ? radii : g.radii, consistent, sh, dmean3D, dopac, dcov3D, dsh,
+                dscale, drot, nullptr, s);
+}
+
+void launch_pair_grad_gather(const GeomState& g, const float* pgrad, float* dmean2D, float* dconic, float* dcolor,
+                             float* dopac, uint32_t* vis, uint32_t vis_bit, int P, cudaStream_t s)
+{
+    if (P <= 0) return;
+    pair_grad_gather_kernel<<<gather_blocks((size_t)P), 256, 0, s>>>(g.sort_ids_b, g.total, g.pair_off, pgrad,
+                                                                     dmean2D, dconic, dcolor, dopac, vis, vis_bit);
+    note_launches(1);
+}
+
+void launch_fold_bwd(const FoldView* views, int nviews, int P, const uint32_t* vis, int consistent, bool sh,
+                     float* dmean3D, float* dopac, float* dsh, float* dscale, float* drot, const DensifyStats* dens,
+                     const FoldView& shared, cudaStream_t s)
+{
+    if (P <= 0 || nviews <= 0) return;
+    fold_launch(views, shared, nviews, P, vis, nullptr, consistent, sh, dmean3D, dopac, nullptr, dsh, dscale, drot,
+                dens, s);
 }
 
 }  // namespace fgs

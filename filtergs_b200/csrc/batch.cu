@@ -11,8 +11,9 @@
 // forked from the caller's stream and joined before compositing (those kernels
 // are latency-bound, so views overlap); compositing, forward and backward,
 // is ONE persistent launch per direction over the tiles of all views, fed by a
-// global work queue.  Backward sums every view's gradients into shared dense
-// buffers (views in stream order, so each row has a single writer at a time).
+// global work queue.  Backward then gathers each view's screen-space gradients
+// (views on the same streams) and sums every view's gradients per Gaussian in
+// view order in one pass, writing each shared gradient row once.
 // A view whose pairs exceed its capacity is truncated and FGS_ERR_OVERFLOW is
 // recorded; fgs_batch_check reports it (the caller re-plans with a larger
 // capacity, outside any captured graph).
@@ -66,7 +67,11 @@ struct Batch {
     unsigned* d_err;
     uint32_t total_tiles;
     const float* background;
-    float *g_means3D, *g_opacity, *g_sh, *g_scales, *g_rot, *g_cov3D;
+    float *g_means3D, *g_opacity, *g_sh, *g_scales, *g_rot;
+    FoldView* d_fold;  // [V] per-view backward descriptors
+    FoldView h_fold0;  // host copy of view 0's (the inputs all views share)
+    uint32_t* d_vis;   // [(V + 31) / 32][P] views that saw each Gaussian (set by the gathers)
+    int vis_words;
     DensifyStats dens{nullptr, nullptr, nullptr};  // optional (fgs_batch_set_densify)
     int M;
     bool has_sr;
@@ -75,7 +80,7 @@ struct Batch {
 struct Layout {
     size_t total;
     std::vector<size_t> geom_off, img_off, bin_off, grad_off;
-    size_t args_off, begin_off, misc_off, cov_off, long_off;
+    size_t args_off, begin_off, misc_off, vis_off, fold_off, long_off;
 };
 
 Layout plan(int P, int V, const fgs_view_args* views)
@@ -98,8 +103,10 @@ Layout plan(int P, int V, const fgs_view_args* views)
     off = align_up(off + sizeof(uint32_t) * (size_t)(V + 1));
     L.misc_off = off;
     off = align_up(off + 64);
-    L.cov_off = off;
-    off = align_up(off + sizeof(float) * 6 * (size_t)P);
+    L.vis_off = off;
+    off = align_up(off + sizeof(uint32_t) * (size_t)((V + 31) / 32) * P);
+    L.fold_off = off;
+    off = align_up(off + sizeof(FoldView) * (size_t)V);
     size_t tiles = 0;
     for (int v = 0; v < V; v++)
         tiles += (size_t)((views[v].width + kTileX - 1) / kTileX) * ((views[v].height + kTileY - 1) / kTileY);
@@ -174,7 +181,9 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
     B->g_scales = dL_dscales;
     B->g_rot = dL_drotations;
     char* base = static_cast<char*>(workspace);
-    B->g_cov3D = reinterpret_cast<float*>(base + L.cov_off);
+    B->d_vis = reinterpret_cast<uint32_t*>(base + L.vis_off);
+    B->vis_words = (nviews + 31) / 32;
+    B->d_fold = reinterpret_cast<FoldView*>(base + L.fold_off);
     std::vector<TileArgs> fa(nviews), ba(nviews);
     std::vector<uint32_t> begin(nviews + 1, 0);
     for (int v = 0; v < nviews; v++) {
@@ -224,6 +233,12 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
         B->views.push_back(s);
     }
     B->total_tiles = begin[nviews];
+    std::vector<FoldView> fold(nviews);
+    for (int v = 0; v < nviews; v++) {
+        const ViewState& s = B->views[v];
+        fold[v] = FoldView{s.pre, s.dmean2D, s.dmean2D, s.dconic, s.dopac, s.dcolor, s.g.clamped};
+    }
+    B->h_fold0 = fold[0];
     B->h_args = fa;
     B->h_args.insert(B->h_args.end(), ba.begin(), ba.end());
     B->d_args_fwd = reinterpret_cast<TileArgs*>(base + L.args_off);
@@ -236,6 +251,8 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
     if (cudaMemcpyAsync(B->d_args_fwd, fa.data(), sizeof(TileArgs) * nviews, cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(B->d_args_bwd, ba.data(), sizeof(TileArgs) * nviews, cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(B->d_begin, begin.data(), sizeof(uint32_t) * (nviews + 1), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(B->d_fold, fold.data(), sizeof(FoldView) * nviews, cudaMemcpyHostToDevice, s) !=
             cudaSuccess ||
         cudaMemsetAsync(B->d_queue, 0, 64, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
         delete B;
@@ -321,27 +338,31 @@ int fgs_batch_backward(void* handle, void* stream)
     const size_t P = (size_t)B->P;
     if (!B->g_means3D || !B->g_opacity) return FGS_ERR_ARG;
     {
-        // dense zeroing of the shared outputs
-        StageTimer t(FGS_STAGE_PREPROCESS_BWD, s);
-        cudaMemsetAsync(B->g_means3D, 0, sizeof(float) * 3 * P, s);
-        cudaMemsetAsync(B->g_opacity, 0, sizeof(float) * P, s);
-        cudaMemsetAsync(B->g_cov3D, 0, sizeof(float) * 6 * P, s);
-        if (B->g_sh && B->M > 0) cudaMemsetAsync(B->g_sh, 0, sizeof(float) * 3 * (size_t)B->M * P, s);
-        if (B->g_scales) cudaMemsetAsync(B->g_scales, 0, sizeof(float) * 3 * P, s);
-        if (B->g_rot) cudaMemsetAsync(B->g_rot, 0, sizeof(float) * 4 * P, s);
-    }
-    {
         StageTimer t(FGS_STAGE_RENDER_BWD, s);
         launch_render_bwd_multi(B->d_args_bwd, B->d_begin, B->V, B->total_tiles, B->d_queue + 1, B->consistent,
                                 B->d_err, s);
     }
     StageTimer t(FGS_STAGE_PREPROCESS_BWD, s);
-    for (ViewState& v : B->views) {
-        launch_preprocess_bwd(v.pre, v.g, v.b.pgrad, v.dmean2D, v.dconic, v.dcolor, v.dopac, B->g_means3D,
-                              B->g_cov3D, (v.pre.shs && B->g_sh) ? B->g_sh : nullptr,
-                              B->has_sr ? B->g_scales : nullptr, B->has_sr ? B->g_rot : nullptr, B->consistent, s,
-                              true, B->g_opacity, B->dens.grad_sum ? &B->dens : nullptr);
+    // Each view's screen-space gradients (the sums of its per-pair rows) and the
+    // views that saw each Gaussian, the views spread over the front-end streams;
+    // then one pass per Gaussian over all views writes every gradient row once.
+    cudaMemsetAsync(B->d_vis, 0, sizeof(uint32_t) * (size_t)B->vis_words * P, s);
+    const int ns = (int)B->aux.size();
+    if (cudaEventRecord(B->forked, s) != cudaSuccess) return FGS_ERR_CUDA;
+    for (int i = 0; i < ns; i++) cudaStreamWaitEvent(B->aux[i], B->forked, 0);
+    for (int vi = 0; vi < B->V; vi++) {
+        ViewState& v = B->views[vi];
+        launch_pair_grad_gather(v.g, v.b.pgrad, v.dmean2D, v.dconic, v.dcolor, v.dopac,
+                                B->d_vis + (size_t)(vi >> 5) * P, 1u << (vi & 31), B->P, B->aux[vi % ns]);
     }
+    for (int i = 0; i < ns; i++) {
+        cudaEventRecord(B->joined[i], B->aux[i]);
+        cudaStreamWaitEvent(s, B->joined[i], 0);
+    }
+    const bool sh = B->views[0].pre.shs && B->g_sh;
+    launch_fold_bwd(B->d_fold, B->V, B->P, B->d_vis, B->consistent, sh, B->g_means3D, B->g_opacity,
+                    sh ? B->g_sh : nullptr, B->has_sr ? B->g_scales : nullptr, B->has_sr ? B->g_rot : nullptr,
+                    B->dens.grad_sum ? &B->dens : nullptr, B->h_fold0, s);
     return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
 }
 

@@ -109,23 +109,39 @@ void launch_render_fwd(int W, int H, const ImageState& im, const BinState& b, lo
                        unsigned* err, cudaStream_t s);
 void launch_render_bwd(int W, int H, const ImageState& im, const BinState& b, const float* bg,
                        const float* dL_dpix, int consistent, unsigned* err, cudaStream_t s);
-// Per-Gaussian backward over the visible Gaussians.  Screen-space gradients come from
-// the per-pair gradients (pgrad, at the emission index), summed per Gaussian in
-// emission order.  Plain: dmean2D / dconic / dcolor / dopac are the dense
-// screen-space outputs (visible rows written; the caller zeroes them), the rest are
-// written densely.  accumulate: adds into shared dense buffers (views run one after
-// another on a stream); dcolor and dmean2D ([P,3]) are then this view's scratch and
-// dopac is not used (the opacity gradient goes to shared_dopac).
 // Densification statistics a training step keeps per Gaussian (null pointers: off).
 struct DensifyStats {
     float* grad_sum;   // += |dL/dmean2D[:2]| per view that sees the Gaussian
     int* count;        // += 1 per such view
     uint8_t* flag;     // = 1 (visible in this step)
 };
-void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* pgrad, float* dmean2D, float* dconic,
-                           float* dcolor, float* dopac, float* dmean3D, float* dcov3D, float* dsh, float* dscale,
-                           float* drot, int consistent, cudaStream_t s, bool accumulate = false,
-                           float* shared_dopac = nullptr, const DensifyStats* dens = nullptr);
+// Per-Gaussian backward of one view.  Screen-space gradients come from the
+// per-pair gradients (pgrad, at the emission index), summed per Gaussian in
+// emission order: dmean2D / dconic / dcolor / dopac are the dense screen-space
+// outputs (rows of visible Gaussians written; the caller zeroes them), the rest are
+// written densely.  radii: the forward's (radii > 0 receive gradients); null: the
+// forward's internal radii (a forward given no radii output).
+void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const int* radii, const float* pgrad,
+                           float* dmean2D, float* dconic, float* dcolor, float* dopac, float* dmean3D, float* dcov3D,
+                           float* dsh, float* dscale, float* drot, int consistent, cudaStream_t s);
+// Batched backward (backward.cu): per-view screen-space gradient gathers, each
+// also setting the view's bit (vis_bit) in vis[idx] for every Gaussian it sees, then
+// one pass per Gaussian over all views.
+struct FoldView {
+    PreParams p;              // the view's preprocess parameters (camera, shared inputs)
+    float* dm_geo;            // [P,3] the view's geometric dL/dmean3D between the two passes (with SH)
+    const float* dmean2D;     // [P,3] the view's screen-space gradients (gather outputs)
+    const float* dconic;      // [P,4]
+    const float* dopac;       // [P]
+    const float* dcolor;      // [P,3]
+    const uint8_t* clamped;   // [P] SH clamp bits of the view's forward
+};
+void launch_pair_grad_gather(const GeomState& g, const float* pgrad, float* dmean2D, float* dconic, float* dcolor,
+                             float* dopac, uint32_t* vis, uint32_t vis_bit, int P, cudaStream_t s);
+// views: device table of nviews descriptors; shared: any one of them (its inputs shared by all views).
+void launch_fold_bwd(const FoldView* views, int nviews, int P, const uint32_t* vis, int consistent, bool sh,
+                     float* dmean3D, float* dopac, float* dsh, float* dscale, float* drot, const DensifyStats* dens,
+                     const FoldView& shared, cudaStream_t s);
 void launch_kpc_stats(const BinState& b, const ImageState& im, int num_tiles, float used_thresh, double* dev_out,
                       cudaStream_t s);
 
