@@ -37,14 +37,19 @@ __device__ __forceinline__ float3 dnormvdv(float3 v, float3 dv)
 
 // SH basis at the unit view direction of a Gaussian at pos seen from campos
 // (backward.cu:20-57): dL/dsh[i][c] = B[i] * dL/dcolor[c].
-__device__ __forceinline__ void sh_basis(float3 pos, float3 campos, float3& dir_orig, float& x, float& y, float& z,
-                                         float (&B)[16])
+__device__ __forceinline__ void sh_dir(float3 pos, float3 campos, float3& dir_orig, float& x, float& y, float& z)
 {
     dir_orig = {pos.x - campos.x, pos.y - campos.y, pos.z - campos.z};
     const float len = sqrtf(dir_orig.x * dir_orig.x + dir_orig.y * dir_orig.y + dir_orig.z * dir_orig.z);
     x = dir_orig.x / len;
     y = dir_orig.y / len;
     z = dir_orig.z / len;
+}
+
+__device__ __forceinline__ void sh_basis(float3 pos, float3 campos, float3& dir_orig, float& x, float& y, float& z,
+                                         float (&B)[16])
+{
+    sh_dir(pos, campos, dir_orig, x, y, z);
     const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
     B[0] = kSH_C0;
     B[1] = -kSH_C1 * y;
@@ -142,8 +147,10 @@ __device__ __forceinline__ void load_sh_row(const float* __restrict__ shrow, int
 // round trip, so a splat over thousands of tiles does not stall the kernel) and a
 // fixed shuffle tree adds them, 32 rows at a time in emission order -- the same
 // sum on every run.  Row layout: dcolor r,g,b | dmean2D x,y | dconic x,y,w |
-// dopacity.
-__global__ void __launch_bounds__(256)
+// dopacity.  vis (optional): the view sets vis_bit in vis[idx] for every Gaussian
+// it sees.  Compiled for 4 blocks per SM (64 registers; measured faster than the
+// compiler's 76 with fewer warps).
+__global__ void __launch_bounds__(256, 4)
     pair_grad_gather_kernel(const uint32_t* __restrict__ visible_ids, const unsigned long long* __restrict__ totals,
                             const uint32_t* __restrict__ pair_off, const float* __restrict__ pgrad,
                             float* __restrict__ dmean2D, float* __restrict__ dconic, float* __restrict__ dcolor,
@@ -172,6 +179,7 @@ __global__ void __launch_bounds__(256)
             float v[4][9];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
+                if (k + 32 * u >= ne) continue;  // (warp-uniform) no rows in this group
                 const uint32_t r = k + 32 * u + lane;
                 const float* src = pgrad + (size_t)(e0 + r) * 9;
 #pragma unroll
@@ -367,34 +375,39 @@ __device__ __forceinline__ void geo_backward(const PreParams& p, int idx, float 
 // The per-Gaussian part of the backward, for one view (the plain path) or many
 // (the batched path) with the same code, so that a batch's sums are the plain
 // per-view results added in view order, bit for bit.  A thread takes one
-// Gaussian, walks the views that saw it in view order, adds each view's whole
-// contribution into registers with explicit round-to-nearest adds (no multiply
-// of a per-view term is fused into them), then writes every output row once,
-// zeros for Gaussians no view saw: no zeroing passes, no launch per view, no
-// re-reading of shared rows per view.
+// Gaussian of a list of the Gaussians some view saw, walks those views in view
+// order, adds each view's whole contribution into registers with explicit
+// round-to-nearest adds (no multiply of a per-view term is fused into them) and
+// writes the Gaussian's output rows once; the rows of Gaussians no view saw are
+// zeroed by the launcher.  No launch per view, no re-reading of shared rows per
+// view, and every thread of a warp does a seen Gaussian's work.
 //
-// Which views saw Gaussian i: vis[(w * P) + i] bit b for view 32 w + b (the
-// batched path; set by the views' gathers), or, for one view, radii[i] > 0 (the
-// reference's backward gates every per-Gaussian gradient on it, backward.cu:156,367).
-__device__ __forceinline__ uint32_t views_of(const uint32_t* __restrict__ vis, const int* __restrict__ radii, int w,
-                                             int P, int i)
+// list / count: the Gaussians (count[0] of them, any order).  Which views saw
+// Gaussian i: vis[(w * P) + i] bit b for view 32 w + b (the batched path, set by
+// the views' gathers); with vis null, the one view (the plain path, whose list is
+// the view's visible Gaussians: radii > 0, which the reference's backward gates
+// every per-Gaussian gradient on, backward.cu:156,367).
+__device__ __forceinline__ uint32_t views_of(const uint32_t* __restrict__ vis, int w, int P, int i)
 {
-    return vis ? vis[(size_t)w * P + i] : (radii[i] > 0 ? 1u : 0u);
+    return vis ? vis[(size_t)w * P + i] : 1u;
 }
 
 // Geometric part: dL/dopacity, dL/dscale, dL/drotation, dL/dcov3D (optional) and
-// each view's geometric dL/dmean3D in its dm_geo row for fold_sh_kernel (with
+// each view's geometric dL/dmean3D in its dm_geo row for fold_shdir_kernel (with
 // SH), else the dL/dmean3D sum itself.  Densification statistics (optional) as
 // densify passes run per view would add them.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128, 4)
     fold_geo_kernel(const FoldView* __restrict__ views, FoldView single, int nviews, int P,
-                    const uint32_t* __restrict__ vis, const int* __restrict__ radii, int consistent, bool sh_follows,
-                    float* __restrict__ dmean3D, float* __restrict__ dopac_out, float* __restrict__ dcov3D,
-                    float* __restrict__ dscale, float* __restrict__ drot, DensifyStats dens)
+                    const uint32_t* __restrict__ list, const unsigned long long* __restrict__ count,
+                    const uint32_t* __restrict__ vis, int consistent, bool sh_follows, float* __restrict__ dmean3D,
+                    float* __restrict__ dopac_out, float* __restrict__ dcov3D, float* __restrict__ dscale,
+                    float* __restrict__ drot, DensifyStats dens)
 {
     const int words = (nviews + 31) >> 5;
     const bool want_sr = single.p.scales && dscale;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+    const uint32_t n = (uint32_t)*count;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int i = (int)list[j];
         float3 am = {0.f, 0.f, 0.f};
         float adc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         float ads[3] = {0.f, 0.f, 0.f};
@@ -403,7 +416,7 @@ __global__ void __launch_bounds__(256)
         float dg = 0.f;
         int seen = 0;
         for (int w = 0; w < words; w++) {
-            uint32_t m = views_of(vis, radii, w, P, i);
+            uint32_t m = views_of(vis, w, P, i);
             while (m) {
                 const int v = 32 * w + __ffs(m) - 1;
                 m &= m - 1;
@@ -460,54 +473,46 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// SH part (backward.cu:20-139 per view): dL/dsh and dL/dmean3D = the sum over views
-// of (geometric term + SH direction term); the SH row is read once for all views.
-// dL/dsh depends only on the direction and the clamp-masked colour gradient.
-__global__ void __launch_bounds__(256)
-    fold_sh_kernel(const FoldView* __restrict__ views, FoldView single, int nviews, int P,
-                   const uint32_t* __restrict__ vis, const int* __restrict__ radii, float* __restrict__ dmean3D,
-                   float* __restrict__ dsh)
+// SH part (backward.cu:20-139 per view), two passes over the list that each hold
+// one 48-float set (the coefficient sums or the SH row), not both.
+// fold_shcoef_kernel: dL/dsh = the sum over views of basis x clamp-masked colour
+// gradient (it depends only on the view direction).
+__global__ void __launch_bounds__(128, 5)
+    fold_shcoef_kernel(const FoldView* __restrict__ views, FoldView single, int nviews, int P,
+                       const uint32_t* __restrict__ list, const unsigned long long* __restrict__ count,
+                       const uint32_t* __restrict__ vis, float* __restrict__ dsh)
 {
     const int words = (nviews + 31) >> 5;
     const PreParams& p = single.p;
     const int deg = p.D, M = p.M, nfl = M * 3;
     const int ncoef = (deg + 1) * (deg + 1);
     const bool vec = p.aligned && (nfl & 3) == 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
-        float* drow = dsh + (size_t)i * nfl;
+    const uint32_t n = (uint32_t)*count;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int i = (int)list[j];
         float acc[48];
 #pragma unroll
         for (int f = 0; f < 48; f++) acc[f] = 0.f;
-        float3 am = {0.f, 0.f, 0.f};
-        bool any = false;
-        for (int w = 0; w < words && !any; w++) any = views_of(vis, radii, w, P, i) != 0;
-        if (any) {
-            float sh[48];
-            if (deg > 0) load_sh_row(p.shs + (size_t)i * nfl, min(48, nfl), vec, sh);
-            const float3 mean = {p.means[3 * i], p.means[3 * i + 1], p.means[3 * i + 2]};
-            for (int w = 0; w < words; w++) {
-                uint32_t m = views_of(vis, radii, w, P, i);
-                while (m) {
-                    const int v = 32 * w + __ffs(m) - 1;
-                    m &= m - 1;
-                    const FoldView& fv = views ? views[v] : single;
-                    const float3 cam = {fv.p.campos[0], fv.p.campos[1], fv.p.campos[2]};
-                    float3 dir_orig;
-                    float x, y, z, B[16];
-                    sh_basis(mean, cam, dir_orig, x, y, z, B);
-                    const uint8_t cb = fv.clamped[i];
-                    const float d[3] = {(cb & 1) ? 0.f : fv.dcolor[3 * i], (cb & 2) ? 0.f : fv.dcolor[3 * i + 1],
-                                        (cb & 4) ? 0.f : fv.dcolor[3 * i + 2]};
+        const float3 mean = {p.means[3 * i], p.means[3 * i + 1], p.means[3 * i + 2]};
+        for (int w = 0; w < words; w++) {
+            uint32_t m = views_of(vis, w, P, i);
+            while (m) {
+                const int v = 32 * w + __ffs(m) - 1;
+                m &= m - 1;
+                const FoldView& fv = views ? views[v] : single;
+                const float3 cam = {fv.p.campos[0], fv.p.campos[1], fv.p.campos[2]};
+                float3 dir_orig;
+                float x, y, z, B[16];
+                sh_basis(mean, cam, dir_orig, x, y, z, B);
+                const uint8_t cb = fv.clamped[i];
+                const float d[3] = {(cb & 1) ? 0.f : fv.dcolor[3 * i], (cb & 2) ? 0.f : fv.dcolor[3 * i + 1],
+                                    (cb & 4) ? 0.f : fv.dcolor[3 * i + 2]};
 #pragma unroll
-                    for (int f = 0; f < 48; f++)
-                        if (f < nfl) acc[f] = __fadd_rn(acc[f], sh_dsh(f, ncoef, B, d));
-                    const float3 dmd = deg == 0 ? make_float3(0.f, 0.f, 0.f) : sh_ddir(deg, sh, x, y, z, d, dir_orig);
-                    am.x = __fadd_rn(am.x, __fadd_rn(fv.dm_geo[3 * i], dmd.x));
-                    am.y = __fadd_rn(am.y, __fadd_rn(fv.dm_geo[3 * i + 1], dmd.y));
-                    am.z = __fadd_rn(am.z, __fadd_rn(fv.dm_geo[3 * i + 2], dmd.z));
-                }
+                for (int f = 0; f < 48; f++)
+                    if (f < nfl) acc[f] = __fadd_rn(acc[f], sh_dsh(f, ncoef, B, d));
             }
         }
+        float* drow = dsh + (size_t)i * nfl;
         if (vec) {
             float4* d4 = reinterpret_cast<float4*>(drow);
 #pragma unroll
@@ -518,67 +523,146 @@ __global__ void __launch_bounds__(256)
             for (int f = 0; f < 48; f++)
                 if (f < nfl) drow[f] = acc[f];
         }
-        for (int f = 48; f < nfl; f++) drow[f] = 0.f;
+    }
+}
+
+// fold_shdir_kernel: dL/dmean3D = the sum over views of (geometric term + the SH
+// colour's dependence on the view direction); the SH row is read once.
+__global__ void __launch_bounds__(128, 4)
+    fold_shdir_kernel(const FoldView* __restrict__ views, FoldView single, int nviews, int P,
+                      const uint32_t* __restrict__ list, const unsigned long long* __restrict__ count,
+                      const uint32_t* __restrict__ vis, float* __restrict__ dmean3D)
+{
+    const int words = (nviews + 31) >> 5;
+    const PreParams& p = single.p;
+    const int deg = p.D, nfl = p.M * 3;
+    const bool vec = p.aligned && (nfl & 3) == 0;
+    const uint32_t n = (uint32_t)*count;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const int i = (int)list[j];
+        float3 am = {0.f, 0.f, 0.f};
+        float sh[48];
+        if (deg > 0) load_sh_row(p.shs + (size_t)i * nfl, min(48, nfl), vec, sh);
+        const float3 mean = {p.means[3 * i], p.means[3 * i + 1], p.means[3 * i + 2]};
+        for (int w = 0; w < words; w++) {
+            uint32_t m = views_of(vis, w, P, i);
+            while (m) {
+                const int v = 32 * w + __ffs(m) - 1;
+                m &= m - 1;
+                const FoldView& fv = views ? views[v] : single;
+                float3 dmd = make_float3(0.f, 0.f, 0.f);
+                if (deg > 0) {
+                    const float3 cam = {fv.p.campos[0], fv.p.campos[1], fv.p.campos[2]};
+                    float3 dir_orig;
+                    float x, y, z;
+                    sh_dir(mean, cam, dir_orig, x, y, z);
+                    const uint8_t cb = fv.clamped[i];
+                    const float d[3] = {(cb & 1) ? 0.f : fv.dcolor[3 * i], (cb & 2) ? 0.f : fv.dcolor[3 * i + 1],
+                                        (cb & 4) ? 0.f : fv.dcolor[3 * i + 2]};
+                    dmd = sh_ddir(deg, sh, x, y, z, d, dir_orig);
+                }
+                am.x = __fadd_rn(am.x, __fadd_rn(fv.dm_geo[3 * i], dmd.x));
+                am.y = __fadd_rn(am.y, __fadd_rn(fv.dm_geo[3 * i + 1], dmd.y));
+                am.z = __fadd_rn(am.z, __fadd_rn(fv.dm_geo[3 * i + 2], dmd.z));
+            }
+        }
         dmean3D[3 * (size_t)i] = am.x; dmean3D[3 * (size_t)i + 1] = am.y; dmean3D[3 * (size_t)i + 2] = am.z;
     }
 }
 
-int gather_blocks(size_t n)
+// The Gaussians some view saw (any vis bit set), appended in any order to list
+// (count[0] entries; the caller zeroes count).
+__global__ void __launch_bounds__(256)
+    seen_list_kernel(const uint32_t* __restrict__ vis, int words, int P, uint32_t* __restrict__ list,
+                     unsigned long long* __restrict__ count)
 {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return (int)std::min<size_t>((n + 255) / 256, (size_t)sms * 8);
+    const int lane = threadIdx.x & 31;
+    for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < P; base += gridDim.x * blockDim.x) {
+        const int i = base + lane;
+        bool any = false;
+        if (i < P)
+            for (int w = 0; w < words && !any; w++) any = vis[(size_t)w * P + i] != 0;
+        const uint32_t b = __ballot_sync(0xffffffffu, any);
+        if (!b) continue;
+        unsigned long long at = 0;
+        if (lane == 0) at = atomicAdd(count, (unsigned long long)__popc(b));
+        at = __shfl_sync(0xffffffffu, at, 0);
+        if (any) list[at + __popc(b & ((1u << lane) - 1))] = (uint32_t)i;
+    }
 }
 
-void fold_launch(const FoldView* views, const FoldView& single, int nviews, int P, const uint32_t* vis,
-                 const int* radii, int consistent, bool sh, float* dmean3D, float* dopac, float* dcov3D, float* dsh,
-                 float* dscale, float* drot, const DensifyStats* dens, cudaStream_t s)
+int grid_for(size_t n, int per_sm)
 {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int blocks = (int)std::min<size_t>(((size_t)P + 255) / 256, (size_t)sms * 16);
+    return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)sms * per_sm));
+}
+
+// The two passes over the list (the caller has zeroed the output rows, which the
+// passes overwrite for the listed Gaussians only).  list_bound sizes the grids.
+void fold_launch(const FoldView* views, const FoldView& single, int nviews, int P, const uint32_t* list,
+                 const unsigned long long* count, size_t list_bound, const uint32_t* vis, int consistent, bool sh,
+                 float* dmean3D, float* dopac, float* dcov3D, float* dsh, float* dscale, float* drot,
+                 const DensifyStats* dens, cudaStream_t s)
+{
+    // 128-thread blocks: these kernels hold 95-128 registers a thread
+    const int blocks = 2 * grid_for(list_bound, 16);
     const DensifyStats d = dens ? *dens : DensifyStats{nullptr, nullptr, nullptr};
-    fold_geo_kernel<<<blocks, 256, 0, s>>>(views, single, nviews, P, vis, radii, consistent, sh, dmean3D, dopac,
+    fold_geo_kernel<<<blocks, 128, 0, s>>>(views, single, nviews, P, list, count, vis, consistent, sh, dmean3D, dopac,
                                            dcov3D, dscale, drot, d);
-    if (sh) fold_sh_kernel<<<blocks, 256, 0, s>>>(views, single, nviews, P, vis, radii, dmean3D, dsh);
-    note_launches(sh ? 2 : 1);
+    if (sh) {
+        fold_shcoef_kernel<<<blocks, 128, 0, s>>>(views, single, nviews, P, list, count, vis, dsh);
+        fold_shdir_kernel<<<blocks, 128, 0, s>>>(views, single, nviews, P, list, count, vis, dmean3D);
+    }
+    note_launches(sh ? 3 : 1);
 }
 
 }  // namespace
 
-void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const int* radii, const float* pgrad,
-                           float* dmean2D, float* dconic, float* dcolor, float* dopac, float* dmean3D, float* dcov3D,
-                           float* dsh, float* dscale, float* drot, int consistent, cudaStream_t s)
+void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* pgrad, float* dmean2D,
+                           float* dconic, float* dcolor, float* dopac, float* dmean3D, float* dcov3D, float* dsh,
+                           float* dscale, float* drot, int consistent, cudaStream_t s)
 {
     if (p.P <= 0) return;
     const bool sh = p.shs && dsh;
-    pair_grad_gather_kernel<<<gather_blocks((size_t)p.P), 256, 0, s>>>(g.sort_ids_b, g.total, g.pair_off, pgrad,
-                                                                       dmean2D, dconic, dcolor, dopac, nullptr, 0u);
+    pair_grad_gather_kernel<<<grid_for((size_t)p.P, 8), 256, 0, s>>>(g.sort_ids_b, g.total, g.pair_off, pgrad,
+                                                                     dmean2D, dconic, dcolor, dopac, nullptr, 0u);
     note_launches(1);
-    // the view's geometric dL/dmean3D waits in the dL/dmean3D rows for the SH pass
+    // the list: the view's visible Gaussians (depth order); the view's geometric
+    // dL/dmean3D waits in the dL/dmean3D rows for the SH pass.  dL/dopacity is the
+    // gather's output, read and rewritten in place (rows outside the list were
+    // zeroed by the caller).
+    const size_t P = (size_t)p.P;
+    cudaMemsetAsync(dmean3D, 0, sizeof(float) * 3 * P, s);
+    cudaMemsetAsync(dcov3D, 0, sizeof(float) * 6 * P, s);
+    if (sh) cudaMemsetAsync(dsh, 0, sizeof(float) * 3 * (size_t)p.M * P, s);
+    if (dscale) cudaMemsetAsync(dscale, 0, sizeof(float) * 3 * P, s);
+    if (drot) cudaMemsetAsync(drot, 0, sizeof(float) * 4 * P, s);
     const FoldView one{p, dmean3D, dmean2D, dconic, dopac, dcolor, g.clamped};
-    fold_launch(nullptr, one, 1, p.P, nullptr, radii ? radii : g.radii, consistent, sh, dmean3D, dopac, dcov3D, dsh,
-                dscale, drot, nullptr, s);
+    fold_launch(nullptr, one, 1, p.P, g.sort_ids_b, g.total + 1, P, nullptr, consistent, sh, dmean3D, dopac, dcov3D,
+                dsh, dscale, drot, nullptr, s);
 }
 
 void launch_pair_grad_gather(const GeomState& g, const float* pgrad, float* dmean2D, float* dconic, float* dcolor,
                              float* dopac, uint32_t* vis, uint32_t vis_bit, int P, cudaStream_t s)
 {
     if (P <= 0) return;
-    pair_grad_gather_kernel<<<gather_blocks((size_t)P), 256, 0, s>>>(g.sort_ids_b, g.total, g.pair_off, pgrad,
-                                                                     dmean2D, dconic, dcolor, dopac, vis, vis_bit);
+    pair_grad_gather_kernel<<<grid_for((size_t)P, 8), 256, 0, s>>>(g.sort_ids_b, g.total, g.pair_off, pgrad,
+                                                                   dmean2D, dconic, dcolor, dopac, vis, vis_bit);
     note_launches(1);
 }
 
-void launch_fold_bwd(const FoldView* views, int nviews, int P, const uint32_t* vis, int consistent, bool sh,
-                     float* dmean3D, float* dopac, float* dsh, float* dscale, float* drot, const DensifyStats* dens,
-                     const FoldView& shared, cudaStream_t s)
+void launch_fold_bwd(const FoldView* views, int nviews, int P, const uint32_t* vis, uint32_t* list,
+                     unsigned long long* count, int consistent, bool sh, float* dmean3D, float* dopac, float* dsh,
+                     float* dscale, float* drot, const DensifyStats* dens, const FoldView& shared, cudaStream_t s)
 {
     if (P <= 0 || nviews <= 0) return;
-    fold_launch(views, shared, nviews, P, vis, nullptr, consistent, sh, dmean3D, dopac, nullptr, dsh, dscale, drot,
-                dens, s);
+    cudaMemsetAsync(count, 0, sizeof(unsigned long long), s);
+    seen_list_kernel<<<grid_for((size_t)P, 8), 256, 0, s>>>(vis, (nviews + 31) >> 5, P, list, count);
+    note_launches(1);
+    fold_launch(views, shared, nviews, P, list, count, (size_t)P, vis, consistent, sh, dmean3D, dopac, nullptr, dsh,
+                dscale, drot, dens, s);
 }
 
 }  // namespace fgs

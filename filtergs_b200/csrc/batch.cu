@@ -71,6 +71,8 @@ struct Batch {
     FoldView* d_fold;  // [V] per-view backward descriptors
     FoldView h_fold0;  // host copy of view 0's (the inputs all views share)
     uint32_t* d_vis;   // [(V + 31) / 32][P] views that saw each Gaussian (set by the gathers)
+    unsigned long long* d_seen_count;
+    uint32_t* d_seen;  // [P] the Gaussians some view saw (count in d_seen_count)
     int vis_words;
     DensifyStats dens{nullptr, nullptr, nullptr};  // optional (fgs_batch_set_densify)
     int M;
@@ -80,7 +82,7 @@ struct Batch {
 struct Layout {
     size_t total;
     std::vector<size_t> geom_off, img_off, bin_off, grad_off;
-    size_t args_off, begin_off, misc_off, vis_off, fold_off, long_off;
+    size_t args_off, begin_off, misc_off, vis_off, list_off, fold_off, long_off;
 };
 
 Layout plan(int P, int V, const fgs_view_args* views)
@@ -105,6 +107,8 @@ Layout plan(int P, int V, const fgs_view_args* views)
     off = align_up(off + 64);
     L.vis_off = off;
     off = align_up(off + sizeof(uint32_t) * (size_t)((V + 31) / 32) * P);
+    L.list_off = off;  // count (8 bytes, padded to 16), then [P] ids
+    off = align_up(off + 16 + sizeof(uint32_t) * (size_t)P);
     L.fold_off = off;
     off = align_up(off + sizeof(FoldView) * (size_t)V);
     size_t tiles = 0;
@@ -182,6 +186,8 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
     B->g_rot = dL_drotations;
     char* base = static_cast<char*>(workspace);
     B->d_vis = reinterpret_cast<uint32_t*>(base + L.vis_off);
+    B->d_seen_count = reinterpret_cast<unsigned long long*>(base + L.list_off);
+    B->d_seen = reinterpret_cast<uint32_t*>(base + L.list_off + 16);
     B->vis_words = (nviews + 31) / 32;
     B->d_fold = reinterpret_cast<FoldView*>(base + L.fold_off);
     std::vector<TileArgs> fa(nviews), ba(nviews);
@@ -350,6 +356,14 @@ int fgs_batch_backward(void* handle, void* stream)
     const int ns = (int)B->aux.size();
     if (cudaEventRecord(B->forked, s) != cudaSuccess) return FGS_ERR_CUDA;
     for (int i = 0; i < ns; i++) cudaStreamWaitEvent(B->aux[i], B->forked, 0);
+    // the shared outputs are zeroed while the gathers run (the fold writes the rows of
+    // the Gaussians some view saw)
+    const bool sh = B->views[0].pre.shs && B->g_sh;
+    cudaMemsetAsync(B->g_means3D, 0, sizeof(float) * 3 * P, s);
+    cudaMemsetAsync(B->g_opacity, 0, sizeof(float) * P, s);
+    if (sh) cudaMemsetAsync(B->g_sh, 0, sizeof(float) * 3 * (size_t)B->M * P, s);
+    if (B->has_sr && B->g_scales) cudaMemsetAsync(B->g_scales, 0, sizeof(float) * 3 * P, s);
+    if (B->has_sr && B->g_rot) cudaMemsetAsync(B->g_rot, 0, sizeof(float) * 4 * P, s);
     for (int vi = 0; vi < B->V; vi++) {
         ViewState& v = B->views[vi];
         launch_pair_grad_gather(v.g, v.b.pgrad, v.dmean2D, v.dconic, v.dcolor, v.dopac,
@@ -359,10 +373,9 @@ int fgs_batch_backward(void* handle, void* stream)
         cudaEventRecord(B->joined[i], B->aux[i]);
         cudaStreamWaitEvent(s, B->joined[i], 0);
     }
-    const bool sh = B->views[0].pre.shs && B->g_sh;
-    launch_fold_bwd(B->d_fold, B->V, B->P, B->d_vis, B->consistent, sh, B->g_means3D, B->g_opacity,
-                    sh ? B->g_sh : nullptr, B->has_sr ? B->g_scales : nullptr, B->has_sr ? B->g_rot : nullptr,
-                    B->dens.grad_sum ? &B->dens : nullptr, B->h_fold0, s);
+    launch_fold_bwd(B->d_fold, B->V, B->P, B->d_vis, B->d_seen, B->d_seen_count, B->consistent, sh, B->g_means3D,
+                    B->g_opacity, sh ? B->g_sh : nullptr, B->has_sr ? B->g_scales : nullptr,
+                    B->has_sr ? B->g_rot : nullptr, B->dens.grad_sum ? &B->dens : nullptr, B->h_fold0, s);
     return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
 }
 

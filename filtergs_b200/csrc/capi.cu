@@ -519,6 +519,7 @@ int fgs_backward(const fgs_raster_args* a, const void* geom, const void* image, 
     GeomState g = geom_views(const_cast<void*>(geom), p.P);
     ImageState im = image_views(const_cast<void*>(image), p.W, p.H);
     BinState b = bin_views(const_cast<void*>(binning), num_rendered, p.P);
+    (void)radii;  // the forward's visible list (radii > 0) is in geom
     cudaMemsetAsync(dL_dmeans2D, 0, sizeof(float) * 3 * (size_t)p.P, s);
     cudaMemsetAsync(dL_dconic, 0, sizeof(float) * 4 * (size_t)p.P, s);
     cudaMemsetAsync(dL_dopacity, 0, sizeof(float) * (size_t)p.P, s);
@@ -535,7 +536,7 @@ int fgs_backward(const fgs_raster_args* a, const void* geom, const void* image, 
     }
     {
         StageTimer t_pb(FGS_STAGE_PREPROCESS_BWD, s);
-        launch_preprocess_bwd(p, g, radii, b.pgrad, dL_dmeans2D, dL_dconic, dL_dcolors, dL_dopacity, dL_dmeans3D,
+        launch_preprocess_bwd(p, g, b.pgrad, dL_dmeans2D, dL_dconic, dL_dcolors, dL_dopacity, dL_dmeans3D,
                               dL_dcov3D, p.shs ? dL_dsh : nullptr, p.scales ? dL_dscales : nullptr,
                               p.scales ? dL_drotations : nullptr, consistent, s);
     }

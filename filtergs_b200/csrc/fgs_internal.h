@@ -119,11 +119,11 @@ struct DensifyStats {
 // per-pair gradients (pgrad, at the emission index), summed per Gaussian in
 // emission order: dmean2D / dconic / dcolor / dopac are the dense screen-space
 // outputs (rows of visible Gaussians written; the caller zeroes them), the rest are
-// written densely.  radii: the forward's (radii > 0 receive gradients); null: the
-// forward's internal radii (a forward given no radii output).
-void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const int* radii, const float* pgrad,
-                           float* dmean2D, float* dconic, float* dcolor, float* dopac, float* dmean3D, float* dcov3D,
-                           float* dsh, float* dscale, float* drot, int consistent, cudaStream_t s);
+// written densely.  The Gaussians the forward found visible (radii > 0) receive
+// gradients.
+void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* pgrad, float* dmean2D,
+                           float* dconic, float* dcolor, float* dopac, float* dmean3D, float* dcov3D, float* dsh,
+                           float* dscale, float* drot, int consistent, cudaStream_t s);
 // Batched backward (backward.cu): per-view screen-space gradient gathers, each
 // also setting the view's bit (vis_bit) in vis[idx] for every Gaussian it sees, then
 // one pass per Gaussian over all views.
@@ -138,10 +138,12 @@ struct FoldView {
 };
 void launch_pair_grad_gather(const GeomState& g, const float* pgrad, float* dmean2D, float* dconic, float* dcolor,
                              float* dopac, uint32_t* vis, uint32_t vis_bit, int P, cudaStream_t s);
-// views: device table of nviews descriptors; shared: any one of them (its inputs shared by all views).
-void launch_fold_bwd(const FoldView* views, int nviews, int P, const uint32_t* vis, int consistent, bool sh,
-                     float* dmean3D, float* dopac, float* dsh, float* dscale, float* drot, const DensifyStats* dens,
-                     const FoldView& shared, cudaStream_t s);
+// views: device table of nviews descriptors; shared: any one of them (its inputs shared by all views);
+// list [P] and count: scratch for the Gaussians some view saw.  The caller zeroes dmean3D, dopac,
+// dsh, dscale and drot first (rows no view saw stay zero).
+void launch_fold_bwd(const FoldView* views, int nviews, int P, const uint32_t* vis, uint32_t* list,
+                     unsigned long long* count, int consistent, bool sh, float* dmean3D, float* dopac, float* dsh,
+                     float* dscale, float* drot, const DensifyStats* dens, const FoldView& shared, cudaStream_t s);
 void launch_kpc_stats(const BinState& b, const ImageState& im, int num_tiles, float used_thresh, double* dev_out,
                       cudaStream_t s);
 
