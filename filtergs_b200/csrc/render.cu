@@ -432,11 +432,12 @@ __device__ __forceinline__ void fwd_smem_init(FwdSmem<kBatch>& sm, int NT, bool 
 }
 
 // Resident CTAs per SM the forward kernels are compiled for (a register cap of
-// 65536 / (CTAs x threads)): 24 warps per SM at 2 pixels per thread, 32 at 4 (64
-// registers and a few spilled bytes, which a 64-record batch's shared memory then
-// lets fill; measured faster than 24 and 28 warps without or with fewer spills).
+// 65536 / (CTAs x threads)): 32 warps per SM at 2 and at 4 pixels per thread (64
+// registers, at 4 with a few spilled bytes; a 64- or 128-record batch's shared
+// memory then lets them fill; measured faster than 24 and 28 warps without or with
+// fewer spills).
 template <int PPT>
-constexpr int fwd_min_ctas() { return PPT == 1 ? 3 : (PPT == 2 ? 6 : 16); }
+constexpr int fwd_min_ctas() { return PPT == 1 ? 3 : (PPT == 2 ? 8 : 16); }
 
 template <int PPT, int kBatch>
 __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas<PPT>())
@@ -928,14 +929,14 @@ __device__ __forceinline__ void bwd_smem_init(BwdSmem<kBatch, kSlots>& sm, int N
 template <int PPT, int kBatch>
 using BwdSmemT = BwdSmem<kBatch, bwd_slots<PPT>()>;
 
-// Resident CTAs per SM the multi-view backward is compiled for: 24 warps at 2 pixels
-// per thread (77 registers) and at 4 (80 registers and a few spilled bytes instead of
-// the 110 the compiler takes when left alone; with 64-record batches the shared
-// memory then lets all 12 CTAs in).  Measured: 4 pixels per thread at 12 CTAs beats
-// 10 (no spills) and 14 (more spills).  The single-view kernel keeps the compiler's
-// allocation.
+// Resident CTAs per SM the multi-view backward is compiled for: 32 warps at 2 pixels
+// per thread (64 registers, a few spilled bytes) and 24 at 4 (80 registers and a few
+// spilled bytes instead of the 110 the compiler takes when left alone; with 64-record
+// batches the shared memory then lets all 12 CTAs in).  Measured: 4 pixels per thread
+// at 12 CTAs beats 10 (no spills) and 14 (more spills); 2 at 8 beats 6.  The
+// single-view kernel keeps the compiler's allocation.
 template <int PPT>
-constexpr int bwd_multi_min_ctas() { return PPT == 2 ? 6 : (PPT == 4 ? 12 : 1); }
+constexpr int bwd_multi_min_ctas() { return PPT == 2 ? 8 : (PPT == 4 ? 12 : 1); }
 
 template <int PPT, int kBatch, bool kConsistent>
 __global__ void __launch_bounds__(256 / PPT) render_bwd_kernel(TileArgs a, unsigned* err)
