@@ -103,9 +103,9 @@ int fgs_forward_render(const fgs_raster_args *a, void *geom, void *image, void *
  *   dL_dmeans2D [P,3], dL_dconic [P,4], dL_dopacity [P], dL_dcolors [P,3],
  *   dL_dmeans3D [P,3], dL_dcov3D [P,6], dL_dsh [P,M,3] (may be null when M==0),
  *   dL_dscales [P,3], dL_drotations [P,4] (both may be null when scales is null).
- * radii: the forward's radii; the Gaussians with radii > 0 receive gradients, as in
- *   the reference (backward.cu:156,367).  Null: the forward's internal radii (valid when
- *   the forward was given no radii output).
+ * radii: the forward's radii (may be null; not read): the Gaussians with radii > 0
+ *   receive gradients, as in the reference (backward.cu:156,367), and geom holds
+ *   their list from the forward.
  * backward_mode: FGS_BACKWARD_REF_COMPAT or FGS_BACKWARD_CONSISTENT.        */
 int fgs_backward(const fgs_raster_args *a, const void *geom, const void *image, const void *binning,
                  long long num_rendered, const int *radii, const float *dL_dout_color, float *dL_dmeans2D,
