@@ -81,6 +81,34 @@ def test_batched_matches_plain(cuda, graph):
     assert all(0 < k <= c for k, c in zip(K, br.capacity))
 
 
+def test_batched_more_than_32_views(cuda):
+    """34 views: the per-Gaussian backward walks two words of view bits; the shared gradients still
+    equal the per-view sums (view order) bit for bit."""
+    sc = _scene(P=100_000, seed=5021)
+    cams = _cams(34, seed=5022)
+    bg = torch.zeros(3, device="cuda")
+    br = BatchedRasterizer(sc["means3D"], sc["opacities"], sc["scales"], sc["rotations"], cams, shs=sc["shs"],
+                           sh_degree=3, bg=bg, graph=False)
+    gen = torch.Generator(device="cuda").manual_seed(23)
+    for v in range(len(cams)):
+        br.dL[v].copy_(torch.randn(br.dL[v].shape, device="cuda", generator=gen))
+    br.step()
+    br.check()
+    torch.cuda.synchronize()
+    sums = {k: torch.zeros_like(v) for k, v in br.grad.items()}
+    for v, cam in enumerate(cams):
+        f, g = _plain(sc, cam, br.dL[v], bg)
+        assert torch.equal(br.images[v], f[1]), v
+        sums["means3D"] += g[3]
+        sums["opacity"] += g[2]
+        sums["sh"] += g[5]
+        sums["scales"] += g[6]
+        sums["rotations"] += g[7]
+    for k in sums:
+        assert torch.equal(br.grad[k], sums[k]), (k, norm_rel(br.grad[k], sums[k]))
+    assert bool((sums["opacity"] != 0).any())
+
+
 def test_batched_capacity_overflow_is_reported(cuda):
     sc = _scene(P=100_000, seed=5003)
     cams = _cams(2, seed=5004)
