@@ -154,15 +154,17 @@ __global__ void __launch_bounds__(256, 4)
     pair_grad_gather_kernel(const uint32_t* __restrict__ visible_ids, const unsigned long long* __restrict__ totals,
                             const uint32_t* __restrict__ pair_off, const float* __restrict__ pgrad,
                             float* __restrict__ dmean2D, float* __restrict__ dconic, float* __restrict__ dcolor,
-                            float* __restrict__ dopac, uint32_t* __restrict__ vis, uint32_t vis_bit)
+                            float* __restrict__ dopac, uint32_t* __restrict__ vis, uint32_t vis_bit, uint32_t rows)
 {
     const uint32_t K = (uint32_t)totals[0], V = (uint32_t)totals[1];
     const int lane = threadIdx.x & 31;
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
     uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    // rows past `rows` (a batched view truncated at its pair capacity) were never
+    // written: each range is clamped to the buffer
     auto range = [&](uint32_t jj, uint32_t& e0, uint32_t& e1, int& idx) {
-        e0 = __ldg(pair_off + jj);
-        e1 = jj + 1 < V ? __ldg(pair_off + jj + 1) : K;
+        e0 = min(__ldg(pair_off + jj), rows);
+        e1 = max(e0, min(jj + 1 < V ? __ldg(pair_off + jj + 1) : K, rows));
         idx = (int)__ldg(visible_ids + jj);
     };
     uint32_t e0 = 0, e1 = 0;
@@ -627,7 +629,8 @@ void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* 
     if (p.P <= 0) return;
     const bool sh = p.shs && dsh;
     pair_grad_gather_kernel<<<grid_for((size_t)p.P, 8), 256, 0, s>>>(g.sort_ids_b, g.total, g.pair_off, pgrad,
-                                                                     dmean2D, dconic, dcolor, dopac, nullptr, 0u);
+                                                                     dmean2D, dconic, dcolor, dopac, nullptr, 0u,
+                                                                     0xffffffffu);
     note_launches(1);
     // the list: the view's visible Gaussians (depth order); the view's geometric
     // dL/dmean3D waits in the dL/dmean3D rows for the SH pass.  dL/dopacity is the
@@ -644,12 +647,13 @@ void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* 
                 dsh, dscale, drot, nullptr, s);
 }
 
-void launch_pair_grad_gather(const GeomState& g, const float* pgrad, float* dmean2D, float* dconic, float* dcolor,
-                             float* dopac, uint32_t* vis, uint32_t vis_bit, int P, cudaStream_t s)
+void launch_pair_grad_gather(const GeomState& g, const float* pgrad, long long rows, float* dmean2D, float* dconic,
+                             float* dcolor, float* dopac, uint32_t* vis, uint32_t vis_bit, int P, cudaStream_t s)
 {
     if (P <= 0) return;
+    const uint32_t r = rows < 0 ? 0u : (rows > 0xffffffffll ? 0xffffffffu : (uint32_t)rows);
     pair_grad_gather_kernel<<<grid_for((size_t)P, 8), 256, 0, s>>>(g.sort_ids_b, g.total, g.pair_off, pgrad,
-                                                                   dmean2D, dconic, dcolor, dopac, vis, vis_bit);
+                                                                   dmean2D, dconic, dcolor, dopac, vis, vis_bit, r);
     note_launches(1);
 }
 

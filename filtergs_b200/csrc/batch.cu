@@ -366,7 +366,7 @@ int fgs_batch_backward(void* handle, void* stream)
     if (B->has_sr && B->g_rot) cudaMemsetAsync(B->g_rot, 0, sizeof(float) * 4 * P, s);
     for (int vi = 0; vi < B->V; vi++) {
         ViewState& v = B->views[vi];
-        launch_pair_grad_gather(v.g, v.b.pgrad, v.dmean2D, v.dconic, v.dcolor, v.dopac,
+        launch_pair_grad_gather(v.g, v.b.pgrad, v.cap, v.dmean2D, v.dconic, v.dcolor, v.dopac,
                                 B->d_vis + (size_t)(vi >> 5) * P, 1u << (vi & 31), B->P, B->aux[vi % ns]);
     }
     for (int i = 0; i < ns; i++) {

@@ -124,9 +124,10 @@ struct DensifyStats {
 void launch_preprocess_bwd(const PreParams& p, const GeomState& g, const float* pgrad, float* dmean2D,
                            float* dconic, float* dcolor, float* dopac, float* dmean3D, float* dcov3D, float* dsh,
                            float* dscale, float* drot, int consistent, cudaStream_t s);
-// Batched backward (backward.cu): per-view screen-space gradient gathers, each
-// also setting the view's bit (vis_bit) in vis[idx] for every Gaussian it sees, then
-// one pass per Gaussian over all views.
+// Batched backward (backward.cu): per-view screen-space gradient gathers (pgrad holds
+// `rows` pair rows: the view's pair capacity), each also setting the view's bit
+// (vis_bit) in vis[idx] for every Gaussian it sees, then one pass per Gaussian over
+// all views.
 struct FoldView {
     PreParams p;              // the view's preprocess parameters (camera, shared inputs)
     float* dm_geo;            // [P,3] the view's geometric dL/dmean3D between the two passes (with SH)
@@ -136,8 +137,8 @@ struct FoldView {
     const float* dcolor;      // [P,3]
     const uint8_t* clamped;   // [P] SH clamp bits of the view's forward
 };
-void launch_pair_grad_gather(const GeomState& g, const float* pgrad, float* dmean2D, float* dconic, float* dcolor,
-                             float* dopac, uint32_t* vis, uint32_t vis_bit, int P, cudaStream_t s);
+void launch_pair_grad_gather(const GeomState& g, const float* pgrad, long long rows, float* dmean2D, float* dconic,
+                             float* dcolor, float* dopac, uint32_t* vis, uint32_t vis_bit, int P, cudaStream_t s);
 // views: device table of nviews descriptors; shared: any one of them (its inputs shared by all views);
 // list [P] and count: scratch for the Gaussians some view saw.  The caller zeroes dmean3D, dopac,
 // dsh, dscale and drot first (rows no view saw stay zero).
