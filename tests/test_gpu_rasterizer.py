@@ -272,3 +272,34 @@ def test_forward_identical_across_launch_shapes(cuda):
     for o in outs[1:]:
         for i in (1, 2, 3, 4):
             assert torch.equal(o[i], outs[0][i]), i
+
+
+def test_backward_launch_shapes_agree(cuda, ref):
+    """The backward at every pixels-per-thread shape and batch: the same gradients up to the order
+    in which a thread adds its pixels' terms (each shape is deterministic), all within the
+    reference tolerance."""
+    from filtergs_b200 import _lib
+    case = small_case(P=20000, seed=1040, W=320, H=240)
+    g = torch.Generator().manual_seed(11)
+    dL = torch.randn(3, case.cam.H, case.cam.W, generator=g).cuda()
+    theirs = run_backward(ref, case, run_forward(ref, case), dL)
+    fwd = run_forward(ours, case)
+    cfg = _lib.get_render_config()
+    grads = []
+    try:
+        for ppt, batch in ((1, 256), (2, 128), (4, 64), (4, 256)):
+            _lib.set_render_config(cfg[0], cfg[1], ppt, batch)
+            a = run_backward(ours, case, fwd, dL)
+            b = run_backward(ours, case, fwd, dL)
+            for x, y in zip(a, b):
+                assert torch.equal(x, y), (ppt, batch)
+            grads.append(a)
+    finally:
+        _lib.set_render_config(*cfg)
+    names = ["means2D", "colors", "opacity", "means3D", "cov3D", "sh", "scales", "rotations"]
+    for gr in grads:
+        for n, x, y, t in zip(names, gr, grads[0], theirs):
+            if t.numel() == 0 or t.abs().max() == 0:
+                continue
+            assert norm_rel(x, y) <= 1e-5, (n, norm_rel(x, y))
+            assert norm_rel(x, t) <= GRAD_TOL, (n, norm_rel(x, t))
