@@ -82,3 +82,30 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "absent.so"))
     with pytest.raises(RuntimeError, match="not built"):
         _lib.lib()
+
+
+def test_batch_workspace_planning():
+    """fgs_batch_workspace_bytes (host only): per view one geom + image + binning at its pair
+    capacity and 11 floats of screen-space scratch per Gaussian; per batch one bit per view per
+    Gaussian in 32-view words and the list of Gaussians some view saw."""
+    from filtergs_b200.batched import _ViewArgs
+    L = _lib.lib()
+    P = 100_000
+
+    def size(n, W=64, H=48, cap=5000):
+        va = (_ViewArgs * n)()
+        for v in va:
+            v.width, v.height, v.pair_capacity = W, H, cap
+        return int(L.fgs_batch_workspace_bytes(P, n, C.cast(va, C.c_void_p)))
+
+    per_view = L.fgs_geom_bytes(P) + L.fgs_image_bytes(64, 48) + L.fgs_binning_bytes(5000, P) + 44 * P
+    s1, s32, s33 = size(1), size(32), size(33)
+    assert s1 >= per_view + 4 * P + 4 * P            # one view-bit word and the seen list
+    assert s32 - s1 >= 31 * per_view
+    # the 33rd view adds its own state and a second word of view bits
+    assert s33 - s32 >= per_view + 4 * P
+    assert size(2, cap=10_000) > size(2, cap=5000)
+    assert size(0) == 0
+    va = (_ViewArgs * 1)()
+    va[0].width, va[0].height, va[0].pair_capacity = 0, 48, 10
+    assert L.fgs_batch_workspace_bytes(P, 1, C.cast(va, C.c_void_p)) == 0
