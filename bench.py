@@ -264,6 +264,37 @@ def ncu_traffic(key, pairs):
     return None
 
 
+def torch_cpu_baseline(sc, cam, threads):
+    """The reference's splat math restated in PyTorch-CPU FP32 (oracle/torch_cpu.py, after its torch helpers
+    LoG/model/geometry.py and sh_utils.py) on the same view, all host threads: forward + autograd backward.
+
+    Sample: full preprocess and binning (and their backward); tile compositing forward + backward on 4 evenly
+    spaced slices of 1/64 of the tiles each, scaled to the full frame."""
+    from oracle import torch_cpu as TC
+    prev = torch.get_num_threads()
+    torch.set_num_threads(threads)
+    try:
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a))  # noqa: E731
+        args = (t(sc["means3D"]), t(sc["scales"]), t(sc["rotations"]), t(sc["opacities"]), t(sc["shs"]), 3, cam)
+        dL = torch.from_numpy(np.random.default_rng(0).standard_normal((3, cam.H, cam.W)).astype(np.float32))
+        T = ((cam.W + 15) // 16) * ((cam.H + 15) // 16)
+        chunk = max(1, T // 64)
+        tiles = [k for st in (int(T * f) for f in (0.1, 0.35, 0.6, 0.85)) for k in range(st, min(T, st + chunk))]
+        a = time.perf_counter()
+        TC.forward_backward(*args, dL, tiles=[])          # per-Gaussian forward + backward, binning
+        b = time.perf_counter()
+        TC.forward_backward(*args, dL, tiles=tiles)
+        c = time.perf_counter()
+    finally:
+        torch.set_num_threads(prev)
+    t_gauss, t_sample = b - a, c - b
+    total = t_gauss + max(0.0, t_sample - t_gauss) * (T / len(tiles))
+    return {"value": 1.0 / total, "unit": "views/s", "cores": threads, "kind": "port",
+            "impl": "PyTorch-CPU FP32 restatement of the reference's splat math (oracle/torch_cpu.py)",
+            "sample": f"1 view: full preprocess+binning fwd+bwd ({t_gauss:.1f}s), tile compositing fwd+bwd on "
+                      f"{len(tiles)}/{T} tiles ({t_sample - t_gauss:.1f}s) scaled x{T / len(tiles):.1f}"}
+
+
 def cpu_baseline(sc, cam, threads):
     """The C oracle (a CPU port of the reference splat math) on the same view, all host threads.
 
@@ -737,7 +768,8 @@ def main():
             if e2e:
                 res["e2e"] = e2e
             if not args.no_cpu_baseline:
-                res["cpu_baseline"] = cpu_baseline(sc, views[0]["cam"], os.cpu_count() or 1)
+                res["cpu_baseline"] = torch_cpu_baseline(sc, views[0]["cam"], os.cpu_count() or 1)
+                res["cpu_baseline"]["c_port"] = cpu_baseline(sc, views[0]["cam"], os.cpu_count() or 1)
                 res["cpu_baseline"]["fp64_image_error"] = fp64_image_error(mod, dev)
         if lod_res:
             res["lod_tree"] = lod_res

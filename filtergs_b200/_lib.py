@@ -74,6 +74,7 @@ SIGNATURES = {
     "fgs_profile_read": (i32, [vp, vp, i32]),
     "fgs_launch_count": (i64, []),
     "fgs_noalloc_capacity_bytes": (sz, []),
+    "fgs_debug_lookback_fault": (i32, [C.c_uint, C.c_ulonglong]),
     "fgs_set_render_config": (i32, [i32, i32, i32, i32]),
     "fgs_gather_attributes": (i32, [i64, vp, vp, vp, vp, vp, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, vp]),
     "fgs_compact_scratch_bytes": (sz, [i32]),

@@ -71,7 +71,8 @@ __global__ void __launch_bounds__(kSortThreads, 4)
                     const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ vals_out, uint32_t n, int shift,
                     int nbits, const uint32_t* __restrict__ pass_hist, uint32_t* status, uint32_t* chunk_counter,
                     unsigned* err, const PairRecord* __restrict__ grec, PairRecord* __restrict__ rec_out,
-                    const unsigned long long* __restrict__ n_dev, const int2* __restrict__ erow, int gx)
+                    const unsigned long long* __restrict__ n_dev, const int2* __restrict__ erow, int gx,
+                    unsigned long long wait_ns = kWaitLimitNs, uint32_t skip_chunk = 0xffffffffu)
 {
     __shared__ uint32_t s_hist[kSortWarps][kRadix];
     __shared__ uint32_t s_keys[kSortTile];
@@ -136,7 +137,9 @@ __global__ void __launch_bounds__(kSortThreads, 4)
             s_hist[w][tid] = tot;
             tot += c;
         }
-        lookback_publish(status + tid, chunk, kRadix, tot);
+        // skip_chunk (a test hook) never publishes: its successors wait until wait_ns runs out
+        const bool publish = chunk != skip_chunk;
+        if (publish) lookback_publish(status + tid, chunk, kRadix, tot);
         s_start[tid] = block_excl_scan(tot, s_warp, nullptr);
         __syncthreads();
         // local sort of the chunk by digit
@@ -152,7 +155,7 @@ __global__ void __launch_bounds__(kSortThreads, 4)
             }
         }
         // global offset of this chunk's digit run
-        s_gbase[tid] = gofs + thread_lookback_walk<32>(status + tid, chunk, kRadix, tot, err);
+        s_gbase[tid] = gofs + thread_lookback_walk<32>(status + tid, chunk, kRadix, tot, err, wait_ns, publish);
         __syncthreads();
         for (uint32_t p = tid; p < count; p += kSortThreads) {
             const uint32_t k = s_keys[p];
@@ -317,8 +320,18 @@ __global__ void ranges_kernel(const uint32_t* __restrict__ tile, uint32_t K, uin
 
 inline uint32_t chunks_of(long long n, int tile) { return (uint32_t)((n + tile - 1) / tile); }
 
+// Test hook of the first depth-sort pass (fgs_debug_lookback_fault): the chunk
+// that never publishes its counts and the wait limit of that pass.
+unsigned long long g_fault_wait_ns = kWaitLimitNs;
+uint32_t g_fault_skip_chunk = 0xffffffffu;
 
 }  // namespace
+
+void set_lookback_fault(uint32_t skip_chunk, unsigned long long wait_ns)
+{
+    g_fault_skip_chunk = skip_chunk;
+    g_fault_wait_ns = wait_ns ? wait_ns : kWaitLimitNs;
+}
 
 int sort_chunk_size() { return kSortTileMin; }  // the smallest chunk: sizes the status words
 
@@ -342,7 +355,9 @@ void launch_depth_sort(const GeomState& g, int P, cudaStream_t s)
     for (int pass = 0; pass < 4; pass++) {
         onesweep_kernel<<<grid, kSortThreads, 0, s>>>(kin[pass], kout[pass], vin[pass], vout[pass], n, 8 * pass, 8,
                                                      g.hist + pass * kRadix, g.status + (size_t)pass * nch * kRadix,
-                                                     g.counters + pass, g.err, nullptr, nullptr, V, nullptr, 1);
+                                                     g.counters + pass, g.err, nullptr, nullptr, V, nullptr, 1,
+                                                     pass ? kWaitLimitNs : g_fault_wait_ns,
+                                                     pass ? 0xffffffffu : g_fault_skip_chunk);
     }
 }
 

@@ -93,13 +93,6 @@ BinCarve carve_bin(void* base, long long K, int P, bool with_grad = true)
     return r;
 }
 
-int tile_bits_for(int num_tiles)
-{
-    int bits = 1;
-    while (bits < 31 && (1u << bits) < (unsigned)num_tiles) bits++;
-    return bits;
-}
-
 // Device errors recorded after a launch are read back lazily through this
 // pinned word (checked at the next synchronisation point on the host).
 unsigned int* pinned_words()
@@ -130,6 +123,13 @@ int check_launch()
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 }  // namespace
+
+int tile_bits_for(int num_tiles)
+{
+    int bits = 1;
+    while (bits < 31 && (1u << bits) < (unsigned)num_tiles) bits++;
+    return bits;
+}
 
 int make_params(const fgs_raster_args* a, PreParams& p, bool backward)
 {
@@ -691,6 +691,12 @@ int fgs_profile_read(double* ms, long long* calls, int reset)
 }
 
 long long fgs_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int fgs_debug_lookback_fault(unsigned int skip_chunk, unsigned long long wait_ns)
+{
+    set_lookback_fault(skip_chunk, wait_ns);
+    return FGS_OK;
+}
 
 int fgs_set_render_config(int fwd_ppt, int fwd_batch, int bwd_ppt, int bwd_batch)
 {

@@ -20,9 +20,34 @@ constexpr int kTileX = 16;
 constexpr int kTileY = 16;
 constexpr int kOgfsBlockArea = 256;
 
-// Bounded spin: every wait on another CTA gives up after this many polls and
-// records FGS_ERR_TIMEOUT instead of hanging the GPU.
-constexpr long long kSpinLimit = 1ll << 26;
+// Bounded waits: every wait on another CTA or on a bulk copy gives up after
+// kWaitLimitNs of the GPU's global timer and records FGS_ERR_TIMEOUT instead of
+// hanging the GPU (legitimate waits last microseconds).
+constexpr unsigned long long kWaitLimitNs = 1000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Deadline of one wait: expired() is called once per unsuccessful poll and
+// reads the timer every 256 polls (the first read starts the clock).
+struct WaitBound {
+    unsigned long long t0 = 0;
+    uint32_t polls = 0;
+    __device__ __forceinline__ bool expired(unsigned long long limit_ns)
+    {
+        if ((++polls & 255u) != 0) return false;
+        const unsigned long long t = global_ns();
+        if (t0 == 0) {
+            t0 = t;
+            return false;
+        }
+        return t - t0 > limit_ns;
+    }
+};
 
 __device__ __forceinline__ void set_error(unsigned int* err, unsigned int code)
 {

@@ -81,6 +81,8 @@ struct BinState {
 BinState bin_views(void* base, long long K, int P);
 size_t bin_bytes(long long K, int P);
 size_t bin_bytes_forward(long long K, int P);  // without the per-pair gradients
+// Key bits of the tile index (the reference's getHigherMsb, rasterizer_impl.cu:78-93).
+int tile_bits_for(int num_tiles);
 
 // ---------------------------------------------------------------- launchers
 // Resident CTAs of a kernel on this device (persistent grids never exceed it).
@@ -95,6 +97,9 @@ inline uint32_t resident_ctas(Kern k, int threads)
 
 void launch_preprocess(const PreParams& p, const GeomState& g, int* radii, cudaStream_t s);
 void launch_depth_sort(const GeomState& g, int P, cudaStream_t s);
+// Test hook: chunk skip_chunk of the first depth-sort pass never publishes its
+// look-back counts, and that pass waits at most wait_ns (0: the default limit).
+void set_lookback_fault(uint32_t skip_chunk, unsigned long long wait_ns);
 void launch_duplicate(const GeomState& g, const BinState& b, uint32_t V, uint32_t K, int W, int H, int tile_bits,
                       cudaStream_t s);
 int sort_chunk_size();

@@ -7,8 +7,9 @@
 // predecessors summing aggregates until it meets an inclusive prefix, then
 // publishes its own inclusive prefix.  Chunk ids come from an atomic
 // counter, so every predecessor of a running chunk is already running and
-// the walk always ends; each poll is still bounded (kSpinLimit) and a
-// timeout is recorded as FGS_ERR_TIMEOUT instead of spinning forever.
+// the walk always ends; each wait is still bounded (kWaitLimitNs, or a
+// caller's shorter limit) and a timeout is recorded as FGS_ERR_TIMEOUT
+// instead of spinning forever.
 //
 // The walk is the scan's critical path: with all chunks resident at once a
 // chunk may find dozens of predecessors that have only published their
@@ -59,7 +60,7 @@ __device__ __forceinline__ uint32_t warp_lookback(uint32_t* status, uint32_t chu
     if (lane == 0) st_relaxed(mine, kFlagAgg | agg);
     unsigned long long excl = 0;
     long long j = (long long)chunk - 1;
-    long long spins = 0;
+    WaitBound wb;
     while (true) {
         const long long q = j - lane;
         const uint32_t s = q >= 0 ? ld_relaxed(status + (size_t)q * stride) : kFlagPrefix;
@@ -75,7 +76,9 @@ __device__ __forceinline__ uint32_t warp_lookback(uint32_t* status, uint32_t chu
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         excl += v;
         if (take == fp + 1 && pref) break;                      // reached an inclusive prefix
-        if (take == 0 && ++spins > kSpinLimit) {
+        // take is warp-uniform; lane 0's clock decides for the whole warp, so every
+        // lane leaves the loop (and its ballots) on the same iteration
+        if (take == 0 && __shfl_sync(0xffffffffu, (int)wb.expired(kWaitLimitNs), 0)) {
             if (lane == 0) set_error(err, FGS_ERR_TIMEOUT);
             break;
         }
@@ -95,7 +98,8 @@ __device__ __forceinline__ uint32_t warp_lookback(uint32_t* status, uint32_t chu
 // publish its aggregate as early as possible and walk later:
 // lookback_publish() first, then thread_lookback_walk<W>(), which polls W
 // predecessors per round trip, returns the exclusive prefix and publishes
-// the inclusive one.
+// the inclusive one (unless `publish` is false: a test hook that leaves the
+// chunk's successors waiting until their limit runs out).
 __device__ __forceinline__ void lookback_publish(uint32_t* status, uint32_t chunk, int stride, uint32_t agg)
 {
     st_relaxed(status + (size_t)chunk * stride, (chunk == 0 ? kFlagPrefix : kFlagAgg) | agg);
@@ -103,12 +107,14 @@ __device__ __forceinline__ void lookback_publish(uint32_t* status, uint32_t chun
 
 template <int kWindow>
 __device__ __forceinline__ uint32_t thread_lookback_walk(uint32_t* status, uint32_t chunk, int stride, uint32_t agg,
-                                                         unsigned* err)
+                                                         unsigned* err,
+                                                         unsigned long long limit_ns = kWaitLimitNs,
+                                                         bool publish = true)
 {
     if (chunk == 0) return 0;
     unsigned long long excl = 0;
     long long j = (long long)chunk - 1;
-    long long spins = 0;
+    WaitBound wb;
     while (true) {
         uint32_t s[kWindow];
 #pragma unroll
@@ -126,14 +132,15 @@ __device__ __forceinline__ uint32_t thread_lookback_walk(uint32_t* status, uint3
             }
         }
         if (done) break;
-        if (take == 0 && ++spins > kSpinLimit) {
+        if (take == 0 && wb.expired(limit_ns)) {
             set_error(err, FGS_ERR_TIMEOUT);
             break;
         }
         j -= take;
     }
     bool sat = false;
-    st_relaxed(status + (size_t)chunk * stride, kFlagPrefix | sat_value(excl + agg, sat));
+    const uint32_t incl = sat_value(excl + agg, sat);
+    if (publish) st_relaxed(status + (size_t)chunk * stride, kFlagPrefix | incl);
     if (sat) set_error(err, FGS_ERR_OVERFLOW);
     return excl > kValMask ? kValMask : (uint32_t)excl;
 }

@@ -11,16 +11,16 @@
 // fgs_forward_noalloc keeps those workspaces in one file-scope device array of
 // kNoAllocScratchBytes (32 MiB), which every GPU that loads this library holds
 // until the process exits.  The array's host-side name is not a device
-// address; its device address is looked up once per device, with that device
-// current, by cudaGetSymbolAddress on the first call made on that device.
+// address; each call looks up its device address on the current device with
+// cudaGetSymbolAddress (a table lookup once the module is loaded), so a device
+// reset or a new primary context between calls leaves no stale address.  The
+// first call on a device loads the library's device code there, so it should
+// come before any stream capture.
 //
 // Every call shares the array and finds the previous call's contents in it;
 // all state that must start at zero is cleared on the stream at the start of
 // each call.  Two calls whose work overlaps on the GPU (different streams, or
 // different host threads) race on the array: callers must serialise them.
-#include <cstring>
-#include <mutex>
-
 #include "fgs_common.cuh"
 #include "fgs_internal.h"
 
@@ -29,25 +29,16 @@ namespace fgs {
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = 32ull << 20;
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device (looked up once per device).
+// Device address of the scratch array in the current device's context, looked
+// up on every call (never cached: a reset device reloads the module elsewhere).
 int noalloc_scratch(void** out)
 {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FGS_ERR_CUDA;
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return FGS_ERR_CUDA;
-        g_noalloc_ptr[dev] = p;
-    }
-    *out = g_noalloc_ptr[dev];
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return FGS_ERR_CUDA;
+    *out = p;
     return FGS_OK;
 }
 
@@ -75,6 +66,7 @@ int fgs_forward_noalloc(const fgs_raster_args* a, int* radii, float* out_color, 
     PreParams p;
     int st = make_params(a, p);
     if (st) return st;
+    if (a->ogfs_enable_stats) return FGS_ERR_ARG;  // the statistics need workspace this entry point does not have
     if (!radii || !out_color || !out_point_id || !out_point_weight_pixel || !out_point_weight || !num_rendered)
         return FGS_ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -113,8 +105,7 @@ int fgs_forward_noalloc(const fgs_raster_args* a, int* radii, float* out_color, 
     BinState b = bin_views(base + gb + ib, K, p.P);
     const int gx = (p.W + kTileX - 1) / kTileX, gy = (p.H + kTileY - 1) / kTileY;
     const int num_tiles = gx * gy;
-    int tbits = 1;
-    while (tbits < 31 && (1u << tbits) < (unsigned)num_tiles) tbits++;
+    const int tbits = tile_bits_for(num_tiles);
     cudaMemsetAsync(out_point_weight, 0, sizeof(float) * (size_t)p.P, s);
     if (K > 0) {
         cudaMemsetAsync(b.status, 0, sizeof(uint32_t) * (b.status_words + b.scan_words), s);

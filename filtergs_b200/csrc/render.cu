@@ -54,9 +54,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
 // Bounded wait: false (and an error bit) if the copy never lands.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned* err)
 {
-    long long spins = 0;
+    WaitBound wb;
     while (!mbar_try_wait(bar, parity)) {
-        if (++spins > kSpinLimit) {
+        if (wb.expired(kWaitLimitNs)) {
             set_error(err, FGS_ERR_TIMEOUT);
             return false;
         }

@@ -300,9 +300,13 @@ int fgs_image_outputs(const void *image, int width, int height, float *final_T, 
  * out_point_id [H,W], out_point_weight_pixel [H,W], out_point_weight [P];
  * num_rendered (host) receives the pair count.  Workspaces that do not fit
  * the array are rejected with FGS_ERR_CAPACITY (checked before any work for
- * the per-Gaussian and per-pixel state, after preprocessing for the pairs).
- * The first call on a device looks up the array's device address.  The call
- * synchronises `stream`.  Calls share the array: two calls that overlap on
+ * the per-Gaussian and per-pixel state, after preprocessing for the pairs: a
+ * call refused there has already written radii).  ogfs_enable_stats must be 0
+ * (FGS_ERR_ARG otherwise).  Each call looks up the array's device address on
+ * the current device; the first call on a device loads the library's device
+ * code, so it should come before any stream capture.  The call synchronises
+ * `stream`; a CUDA error left pending by earlier work on the device is
+ * reported as FGS_ERR_CUDA.  Calls share the array: two calls that overlap on
  * the GPU race and must be serialised by the caller.                       */
 size_t fgs_noalloc_capacity_bytes(void);
 int fgs_forward_noalloc(const fgs_raster_args *a, int *radii, float *out_color, int *out_point_id,
@@ -343,6 +347,16 @@ int fgs_set_render_split(int min_records, int band_shape);
 int fgs_get_render_split(int *cfg);
 int fgs_profile_read(double *ms, long long *calls, int reset);
 long long fgs_launch_count(void);
+
+/* Failure-path test hook (no reference counterpart; the reference has no bounded
+ * waits).  From the next forward on, chunk `skip_chunk` of the first depth-sort
+ * pass never publishes its look-back counts, so the chunks after it wait until
+ * `wait_ns` nanoseconds run out (0: the default one-second limit), record
+ * FGS_ERR_TIMEOUT and finish; fgs_forward_preprocess then returns
+ * FGS_ERR_TIMEOUT.  skip_chunk = 0xffffffff switches the hook off.  Only the
+ * depth sort's keys and ids move in that pass, so the wrong offsets of a timed-out
+ * pass stay inside its buffers.  Process-wide; for tests only.               */
+int fgs_debug_lookback_fault(unsigned int skip_chunk, unsigned long long wait_ns);
 
 #ifdef __cplusplus
 }

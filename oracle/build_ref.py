@@ -18,8 +18,10 @@ the FilterGS kernels get the -O2 their JIT loaders pass.
 import os
 import sys
 
-REF_ROOT = os.environ.get("FGS_REFERENCE_ROOT", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+# The reference checkout: FGS_REFERENCE_ROOT, else a `reference` directory beside this repository.
+REF_ROOT = os.environ.get("FGS_REFERENCE_ROOT",
+                          os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 OUT = os.path.join(HERE, "_ref")
 
 MODULES = {

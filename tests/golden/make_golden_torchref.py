@@ -1,7 +1,7 @@
 """Generate golden fixtures from the reference's own Python/torch code (CPU).
 
-Run where the reference tree is available (default /root/reference, override
-with FGS_REFERENCE_ROOT):
+Run where the reference tree is available (FGS_REFERENCE_ROOT, else a
+`reference` directory beside this repository):
 
     python tests/golden/make_golden_torchref.py
 
@@ -23,7 +23,7 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("FGS_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("FGS_REFERENCE_ROOT", os.path.join(os.path.dirname(ROOT), "reference"))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, REF)
 

@@ -81,7 +81,36 @@ def test_noalloc_rejects_work_beyond_its_array(cuda):
     st = _noalloc(big)[0]
     assert st == _lib.FGS_ERR_CAPACITY
     # a normal call still works afterwards
-    ok = small_case(P=2000, seed=1104, W=128, H=128)
+    _check_normal_call(small_case(P=2000, seed=1104, W=128, H=128))
+
+
+def test_noalloc_rejects_pairs_beyond_its_array(cuda):
+    # few but large Gaussians on a large image: the per-Gaussian and per-pixel state
+    # fit, the tile/Gaussian pairs found by the preprocess do not
+    case = small_case(P=20_000, seed=1105, W=1024, H=1024)
+    case.scene = dict(case.scene, scales=(case.scene["scales"] * 8.0).astype(np.float32))
+    st = _noalloc(case)[0]
+    assert st == _lib.FGS_ERR_CAPACITY
+    ref = _regular(case)
+    assert ref[0] * 48 > int(_lib.lib().fgs_noalloc_capacity_bytes())
+    _check_normal_call(small_case(P=2500, seed=1106, W=160, H=120))
+
+
+def test_noalloc_rejects_statistics(cuda):
+    case = small_case(P=500, seed=1107, W=64, H=64)
+    a, args = _inputs(case)
+    args.ogfs_enable_stats = 1
+    dev = torch.device("cuda")
+    outs = [torch.zeros(case.P, dtype=torch.int32, device=dev), torch.zeros(3, 64, 64, device=dev),
+            torch.zeros(64, 64, dtype=torch.int32, device=dev), torch.zeros(64, 64, device=dev),
+            torch.zeros(case.P, device=dev)]
+    K = C.c_longlong(-1)
+    st = _lib.lib().fgs_forward_noalloc(C.byref(args), *[_ptr(o) for o in outs], C.byref(K),
+                                        C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == _lib.FGS_ERR_ARG
+
+
+def _check_normal_call(ok):
     st, K, radii, color, pid, pwp, pw = _noalloc(ok)
     assert st == _lib.FGS_OK
     ref = _regular(ok)
