@@ -204,14 +204,16 @@ def step_c(mod, scene, v, bg, stats):
 
 def make_batched(scene, views, bg):
     """BatchedRasterizer over `views`; its cameras live in one packed device buffer br.cam_dev
-    [nv, 35] (view 16, proj 16, campos 3 per row)."""
+    [nv, 35] (view 16, proj 16, campos 3 per row).  Every forward output of the reference's call is
+    produced per view (image, radii, point_id, point_weight_pixel, point_weight); the gradients of all
+    views are summed into the shared parameter gradients."""
     from filtergs_b200.batched import BatchedRasterizer, Camera
     cam_dev = torch.stack([torch.cat([v["view"].reshape(-1), v["proj"].reshape(-1), v["campos"].reshape(-1)])
                            for v in views]).contiguous()
     cams = [Camera(v["cam"].W, v["cam"].H, v["cam"].tanfovx, v["cam"].tanfovy, cam_dev[i, :16], cam_dev[i, 16:32],
                    cam_dev[i, 32:35]) for i, v in enumerate(views)]
     br = BatchedRasterizer(scene["means3D"], scene["opacities"], scene["scales"], scene["rotations"], cams,
-                           shs=scene["shs"], sh_degree=3, bg=bg, graph=True)
+                           shs=scene["shs"], sh_degree=3, bg=bg, graph=True, full_outputs=True)
     br.cam_dev = cam_dev
     br.set_io_many(list(range(len(views))), list(br.images), [v["dL"] for v in views])
     return br
@@ -234,7 +236,11 @@ def algo_bytes(stage, P, V, K, N, T, M=16, tile_passes=2):
     if stage == "render_fwd":
         return 40 * K + 28 * N
     if stage == "render_bwd":
-        return 76 * K + 20 * N  # records 40 B + per-pair gradient row 36 B; dL/dpix, T, n_contrib
+        # the survey's algorithmic bytes: records 40 B per pair; dL/dpix, T, n_contrib per pixel; the 44-byte
+        # screen-space gradient accumulators written once per visible Gaussian
+        return 40 * K + 20 * N + 44 * V
+    if stage == "render_bwd_design":
+        return 76 * K + 20 * N  # this design's traffic: records 40 B + the per-pair gradient row 36 B per pair
     if stage == "preprocess_bwd":
         return 36 * K + V * (12 + 24 + 16 + 12 + 12 + 16 + 12 + 3 + 192) + P * 284
     return 0
@@ -250,18 +256,36 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def kernel_source_digest():
+    """Short digest of the render kernels' source, stamped into the ncu summaries they were captured from."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in ("render.cu", "fgs_common.cuh"):
+        with open(os.path.join(ROOT, "filtergs_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:12]
+
+
 def ncu_traffic(key, pairs):
-    """DRAM bytes of one launch of `key` from the committed ncu summary: per-pair traffic x pairs
-    (None if the summary has no figure for it)."""
-    p = os.path.join(ROOT, "profiles", "traffic_urban1080.md")
+    """DRAM bytes of one launch of `key` from the committed ncu summary of the CURRENT render kernels:
+    per-pair traffic x pairs.  (None, reason) when the summary has no figure for this key or was captured
+    from other kernel sources than the ones built now."""
+    p = os.path.join(ROOT, "profiles", "render_traffic_urban1080.md")
+    digest, per_pair = None, None
     try:
         with open(p) as f:
             for ln in f:
+                if ln.startswith("source_digest ="):
+                    digest = ln.split("=")[1].strip()
                 if ln.startswith("traffic_per_pair[") and ln.split("[")[1].split("]")[0] == key:
-                    return float(ln.split("=")[1].strip().split()[0]) * pairs
+                    per_pair = float(ln.split("=")[1].strip().split()[0])
     except OSError:
-        pass
-    return None
+        return None, "no ncu summary"
+    if per_pair is None:
+        return None, f"no ncu figure for {key}"
+    if digest != kernel_source_digest():
+        return None, "ncu summary is of other kernel sources"
+    return per_pair * pairs, f"ncu dram bytes per pair x pairs ({os.path.relpath(p, ROOT)})"
 
 
 def torch_cpu_baseline(sc, cam, threads):
@@ -466,16 +490,22 @@ def roofline(prof, P, views, K, vis, batched):
         T = ((c.W + 15) // 16) * ((c.H + 15) // 16)
         return algo_bytes(stage, P, n, k, c.W * c.H, T)
 
+    design = dom + "_design" if dom == "render_bwd" else dom
     if batched and dom in ("render_fwd", "render_bwd"):
         ab = sum(bytes_of(dom, v, K[v], vis[v]) for v in range(len(views)))   # one launch covers all views
+        db = sum(bytes_of(design, v, K[v], vis[v]) for v in range(len(views)))
         key, pairs = "batched." + dom, float(sum(K))
     else:
         ab = float(np.mean([bytes_of(dom, v, K[v], vis[v]) for v in range(len(views))]))
+        db = float(np.mean([bytes_of(design, v, K[v], vis[v]) for v in range(len(views))]))
         key, pairs = ("batched." if batched else "") + dom, float(np.mean(K))
     peak, kind = measured_peak()
     achieved = ab / (per_call_ms / 1000.0) / 1e9
+    traffic, traffic_src = ncu_traffic(key, pairs)
     return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": ncu_traffic(key, pairs), "algorithmic_bytes_per_launch": ab,
+            "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
+            "algorithmic_bytes_per_launch": ab, "bytes_formula": "survey 8(d) per view, summed over the views",
+            "design_bytes_per_launch": db, "design_frac": db / (per_call_ms / 1000.0) / 1e9 / peak,
             "launch_ms": per_call_ms, "peak_source": f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured"
             else "fallback 6650 GB/s",
             "timing": "CUDA events around each launch, eager pass of the same K steps" if batched
@@ -713,17 +743,18 @@ def main():
         del head["br"]
         torch.cuda.empty_cache()
     if args.impl == "ours" and path == "batched" and not args.no_plain:
-        plain = measure_plain(args, mod, scene, views, bg, dev, ref_dist, rank)
+        plain = measure_plain(args, mod, scene, views, bg, dev, ref_dist, rank, clocks=clocks)
     if args.impl == "ours" and path == "batched" and not args.no_mixed:
         mv = make_views(args.views, dev, rank, mixed=True)
-        mb = measure_batched(args, scene, mv, bg, dev, ref_dist, rank, profile=False)
+        mb = measure_batched(args, scene, mv, bg, dev, ref_dist, rank, clocks=clocks, profile=False)
         del mb["br"]
         torch.cuda.empty_cache()
-        mp = measure_plain(args, mod, scene, mv, bg, dev, ref_dist, rank)
+        mp = measure_plain(args, mod, scene, mv, bg, dev, ref_dist, rank, clocks=clocks)
         mixed = {"resolutions": [f"{v['cam'].W}x{v['cam'].H}" for v in mv],
                  "batched_value": n_ranks * nv * args.steps / (mb["ms"] / 1000.0),
                  "plain_value": n_ranks * nv * args.steps / (mp["ms"] / 1000.0),
                  "unit": "views/s", "batched_render_config": mb["tuned"], "plain_render_config": mp["tuned"],
+                 "batched_clocks": mb["clocks"], "plain_clocks": mp["clocks"],
                  "pairs_K": mb["K"], "visible_V": mb["vis"], "altitude_m": "80-300", "pitch_deg": "30-75"}
     lod_res = train_res = None
     if not args.no_lod and rank == 0:
@@ -763,6 +794,7 @@ def main():
                 res["plain"] = {"value": n_ranks * nv * args.steps / (plain["ms"] / 1000.0), "unit": "views/s",
                                 "ms_per_step": plain["ms"] / args.steps, "render_config": plain["tuned"],
                                 "clocks": plain["clocks"]}
+                res["batched_over_plain"] = value / res["plain"]["value"]
             if mixed:
                 res["mixed_resolution"] = mixed
             if e2e:
@@ -868,7 +900,8 @@ def e2e_plain(args, mod, scene, views, bg, dev, dist, n_ranks):
     px = sum(v["cam"].W * v["cam"].H for v in views)
     return {"value": n_ranks * args.steps * nv / (ms / 1000.0), "unit": "views/s",
             "h2d_bytes_per_step": int(nv * 35 * 4 + 3 * px * 4), "d2h_bytes_per_step": int(3 * px * 4),
-            "api": "GaussianRasterizer (autograd)" if ours else "reference _C rasterize_gaussians(+_backward)"}
+            "api": "GaussianRasterizer (autograd)" if ours else "reference _C rasterize_gaussians(+_backward)",
+            "d2h": "every rendered image; the Gaussian gradients stay on the device for the optimizer step"}
 
 
 def e2e_batched(args, br, views, dev, dist, n_ranks):
@@ -939,7 +972,9 @@ def e2e_batched(args, br, views, dev, dist, n_ranks):
     px = sum(v["cam"].W * v["cam"].H for v in views)
     return {"value": n_ranks * args.steps * nv / (ms / 1000.0), "unit": "views/s",
             "h2d_bytes_per_step": int(nv * 35 * 4 + 3 * px * 4), "d2h_bytes_per_step": int(3 * px * 4),
-            "api": "BatchedRasterizer.step (CUDA-graph replay)"}
+            "api": "BatchedRasterizer.step (CUDA-graph replay)",
+            "d2h": "every rendered image; the summed Gaussian gradients stay on the device for the optimizer "
+                   "step (as in the reference's training loop), as they do in the reference arm"}
 
 
 if __name__ == "__main__":

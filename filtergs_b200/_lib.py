@@ -90,6 +90,7 @@ SIGNATURES = {
     "fgs_batch_forward": (i32, [vp, vp]),
     "fgs_batch_backward": (i32, [vp, vp]),
     "fgs_batch_set_view_io": (i32, [vp, i32, vp, vp, vp, vp]),
+    "fgs_batch_set_view_outputs": (i32, [vp, i32, vp, vp, vp, vp, vp]),
     "fgs_batch_pair_counts": (i32, [vp, vp, vp]),
     "fgs_batch_check": (i32, [vp, vp]),
     "fgs_batch_destroy": (None, [vp]),

@@ -53,7 +53,7 @@ class BatchedRasterizer:
 
     def __init__(self, means3D, opacities, scales, rotations, cameras, shs=None, sh_degree=0, colors_precomp=None,
                  bg=None, use_filter=True, ogfs=(0.2, 0.2, 0.05, 0.7), filter3d_scale=0.0,
-                 backward_mode="ref_compat", headroom=1.15, graph=True):
+                 backward_mode="ref_compat", headroom=1.15, graph=True, full_outputs=False):
         dev = means3D.device
         self.dev = dev
         self.P = int(means3D.shape[0])
@@ -71,6 +71,12 @@ class BatchedRasterizer:
         self.images = [torch.empty(3, c.H, c.W, device=dev) for c in self.cams]
         self.dL = [torch.zeros(3, c.H, c.W, device=dev) for c in self.cams]
         self.radii = [torch.empty(self.P, dtype=torch.int32, device=dev) for _ in self.cams]
+        # the rest of the reference's forward outputs per view (point_id, point_weight_pixel, point_weight)
+        self.full_outputs = bool(full_outputs)
+        if self.full_outputs:
+            self.point_id = [torch.empty(c.H, c.W, dtype=torch.int32, device=dev) for c in self.cams]
+            self.point_weight_pixel = [torch.empty(c.H, c.W, device=dev) for c in self.cams]
+            self.point_weight = [torch.empty(self.P, device=dev) for _ in self.cams]
         M = int(self.shs.shape[1]) if self.shs is not None else 0
         self.grad = dict(means3D=torch.zeros(self.P, 3, device=dev), opacity=torch.zeros(self.P, 1, device=dev),
                          sh=torch.zeros(self.P, M, 3, device=dev), scales=torch.zeros(self.P, 3, device=dev),
@@ -129,6 +135,15 @@ class BatchedRasterizer:
         if not h:
             _lib.check(st.value, "fgs_batch_create")
         self.handle = h
+        if self.full_outputs:
+            n = self.V
+            ids = (C.c_int * n)(*range(n))
+            pid = (C.c_void_p * n)(*[t.data_ptr() for t in self.point_id])
+            pwp = (C.c_void_p * n)(*[t.data_ptr() for t in self.point_weight_pixel])
+            pw = (C.c_void_p * n)(*[t.data_ptr() for t in self.point_weight])
+            _lib.check(L.fgs_batch_set_view_outputs(h, n, C.cast(ids, C.c_void_p), C.cast(pid, C.c_void_p),
+                                                    C.cast(pwp, C.c_void_p), C.cast(pw, C.c_void_p), _s()),
+                       "fgs_batch_set_view_outputs")
 
     def _capture(self):
         L = _L()

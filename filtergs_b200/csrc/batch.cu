@@ -85,6 +85,16 @@ struct Layout {
     size_t args_off, begin_off, misc_off, vis_off, list_off, fold_off, long_off;
 };
 
+// Zero every view's per-Gaussian maximum weight (out_point_weight, when the view has one)
+// before the forward compositing takes its maxima; the pointers are read from the device
+// descriptors, so a captured graph follows fgs_batch_set_view_outputs.
+__global__ void zero_point_weight_kernel(const TileArgs* __restrict__ views, int P)
+{
+    float* pw = views[blockIdx.y].out_point_weight;
+    if (!pw) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) pw[i] = 0.f;
+}
+
 Layout plan(int P, int V, const fgs_view_args* views)
 {
     Layout L;
@@ -290,6 +300,26 @@ int fgs_batch_set_view_io(void* handle, int count, const int* view_ids, float* c
     return FGS_OK;
 }
 
+int fgs_batch_set_view_outputs(void* handle, int count, const int* view_ids, int* const* out_point_id,
+                               float* const* out_point_weight_pixel, float* const* out_point_weight, void* stream)
+{
+    Batch* B = static_cast<Batch*>(handle);
+    if (!B || count < 0 || (count > 0 && !view_ids)) return FGS_ERR_ARG;
+    for (int i = 0; i < count; i++)
+        if (view_ids[i] < 0 || view_ids[i] >= B->V) return FGS_ERR_ARG;
+    for (int i = 0; i < count; i++) {
+        TileArgs& f = B->h_args[view_ids[i]];
+        f.out_point_id = out_point_id ? out_point_id[i] : nullptr;
+        f.out_pw_pixel = out_point_weight_pixel ? out_point_weight_pixel[i] : nullptr;
+        f.out_point_weight = out_point_weight ? out_point_weight[i] : nullptr;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(B->d_args_fwd, B->h_args.data(), sizeof(TileArgs) * B->h_args.size(), cudaMemcpyHostToDevice,
+                        s) != cudaSuccess)
+        return FGS_ERR_CUDA;
+    return FGS_OK;
+}
+
 int fgs_batch_forward(void* handle, void* stream)
 {
     Batch* B = static_cast<Batch*>(handle);
@@ -331,6 +361,9 @@ int fgs_batch_forward(void* handle, void* stream)
         cudaStreamWaitEvent(s, B->joined[i], 0);
     }
     StageTimer t(FGS_STAGE_RENDER_FWD, s);
+    zero_point_weight_kernel<<<dim3((unsigned)((B->P + 255) / 256 < 592 ? (B->P + 255) / 256 : 592), (unsigned)B->V),
+                               256, 0, s>>>(B->d_args_fwd, B->P);
+    note_launches(1);
     launch_render_fwd_multi(B->d_args_fwd, B->d_begin, B->V, B->total_tiles, B->d_queue, B->d_long,
                             B->d_long + 32 * (size_t)B->total_tiles, B->d_err, s);
     return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;

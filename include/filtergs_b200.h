@@ -176,6 +176,14 @@ int fgs_batch_backward(void *handle, void *stream);
  * (double-buffered I/O).  dL_dout_color, or an entry of it, may be null (kept).     */
 int fgs_batch_set_view_io(void *handle, int count, const int *view_ids, float *const *out_color,
                           const float *const *dL_dout_color, void *stream);
+/* Optional per-view forward outputs of the reference's call (rasterize_points.cu:178):
+ * out_point_id [H,W] (the strongest contributor of each pixel, -1 for none),
+ * out_point_weight_pixel [H,W] (its weight T*alpha) and out_point_weight [P] (each
+ * Gaussian's largest weight in the view, zeroed by every forward).  Arrays or entries
+ * may be null (that output off).  Like fgs_batch_set_view_io, a captured graph follows
+ * the change without re-capture.  No reference counterpart for the batching itself. */
+int fgs_batch_set_view_outputs(void *handle, int count, const int *view_ids, int *const *out_point_id,
+                               float *const *out_point_weight_pixel, float *const *out_point_weight, void *stream);
 /* Pair counts of the last forward per view (host [nviews]); synchronises. */
 int fgs_batch_pair_counts(void *handle, long long *counts, void *stream);
 /* Synchronise and return the first device-side error of the batch (FGS_OK when none). */

@@ -178,3 +178,23 @@ def test_batched_long_tile_bands(cuda):
         _lib.set_render_split(*was)
     for x, y in zip(*out):
         assert torch.equal(x, y)
+
+
+def test_batched_full_forward_outputs_match_plain(cuda):
+    """With full_outputs the batched path also returns the reference call's point_id,
+    point_weight_pixel and point_weight per view: equal to the plain path's, over two replays."""
+    sc = _scene(P=200_000, seed=5011)
+    cams = _cams(3, seed=5012)
+    bg = torch.zeros(3, device="cuda")
+    br = BatchedRasterizer(sc["means3D"], sc["opacities"], sc["scales"], sc["rotations"], cams, shs=sc["shs"],
+                           sh_degree=3, bg=bg, graph=True, full_outputs=True)
+    for _ in range(2):
+        br.step()
+    br.check()
+    torch.cuda.synchronize()
+    for v, cam in enumerate(cams):
+        f, _ = _plain(sc, cam, br.dL[v], bg)
+        assert torch.equal(br.images[v], f[1]), v
+        assert torch.equal(br.point_id[v], f[2]), v
+        assert torch.equal(br.point_weight_pixel[v], f[3]), v
+        assert torch.equal(br.point_weight[v], f[4]), v
