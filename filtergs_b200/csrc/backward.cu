@@ -234,14 +234,14 @@ __device__ __forceinline__ void geo_backward(const PreParams& p, int idx, float 
         for (int k = 0; k < 6; k++) cov3D[k] = p.cov3D[6 * (size_t)idx + k];
     } else {
         const float4 q = {p.rots[4 * idx], p.rots[4 * idx + 1], p.rots[4 * idx + 2], p.rots[4 * idx + 3]};
-        cov3d_from_scale_rot(p.scales[3 * idx], p.scales[3 * idx + 1], p.scales[3 * idx + 2], p.scale_mod, q,
-                             cov3D);
+        // the forward's cov3D (the reference's backward reads the one its forward stored)
+        cov3d_ref(p.scales[3 * idx], p.scales[3 * idx + 1], p.scales[3 * idx + 2], p.scale_mod, q, cov3D);
     }
     if (p.filter3d > 0.f) {
         const float3 pv = xform_point4x3(mean, p.view);
-        const float sf = p.filter3d * pv.z / p.fx;
-        const float v = sf * sf;
-        cov3D[0] += v; cov3D[3] += v; cov3D[5] += v;
+        const float sf = __fdiv_rn(__fmul_rn(p.filter3d, pv.z), p.fx);
+        const float v = __fmul_rn(sf, sf);
+        cov3D[0] = __fadd_rn(cov3D[0], v); cov3D[3] = __fadd_rn(cov3D[3], v); cov3D[5] = __fadd_rn(cov3D[5], v);
     }
     Ewa e;
     const float3 c2 = ewa_cov2d(mean, p.fx, p.fy, p.tanx, p.tany, cov3D, p.view, &e);

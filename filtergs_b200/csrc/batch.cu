@@ -77,12 +77,13 @@ struct Batch {
     DensifyStats dens{nullptr, nullptr, nullptr};  // optional (fgs_batch_set_densify)
     int M;
     bool has_sr;
+    float4* packed;  // [3][P] (PreParams::packed), refreshed by every forward
 };
 
 struct Layout {
     size_t total;
     std::vector<size_t> geom_off, img_off, bin_off, grad_off;
-    size_t args_off, begin_off, misc_off, vis_off, list_off, fold_off, long_off;
+    size_t args_off, begin_off, misc_off, vis_off, list_off, fold_off, long_off, packed_off;
 };
 
 // Zero every view's per-Gaussian maximum weight (out_point_weight, when the view has one)
@@ -126,6 +127,8 @@ Layout plan(int P, int V, const fgs_view_args* views)
         tiles += (size_t)((views[v].width + kTileX - 1) / kTileX) * ((views[v].height + kTileY - 1) / kTileY);
     L.long_off = off;  // long-tile bins [32][tiles] + 34 counters
     off = align_up(off + sizeof(uint32_t) * (32 * tiles + 34));
+    L.packed_off = off;  // the Gaussians' packed float4 planes, shared by the views' preprocess
+    off = align_up(off + 3 * sizeof(float4) * (size_t)P);
     L.total = off;
     return L;
 }
@@ -200,6 +203,7 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
     B->d_seen = reinterpret_cast<uint32_t*>(base + L.list_off + 16);
     B->vis_words = (nviews + 31) / 32;
     B->d_fold = reinterpret_cast<FoldView*>(base + L.fold_off);
+    B->packed = reinterpret_cast<float4*>(base + L.packed_off);
     std::vector<TileArgs> fa(nviews), ba(nviews);
     std::vector<uint32_t> begin(nviews + 1, 0);
     for (int v = 0; v < nviews; v++) {
@@ -219,6 +223,7 @@ void* fgs_batch_create(const fgs_raster_args* shared, int nviews, const fgs_view
             delete B;
             return fail(st ? st : FGS_ERR_ARG);
         }
+        s.pre.packed = B->packed;  // every view's preprocess reads the packed copy
         const int gx = (va.width + kTileX - 1) / kTileX, gy = (va.height + kTileY - 1) / kTileY;
         s.num_tiles = gx * gy;
         s.tile_bits = tile_bits_of(s.num_tiles);
@@ -329,6 +334,12 @@ int fgs_batch_forward(void* handle, void* stream)
     // look-back, small sorts): they run on kFrontStreams streams forked from `s`
     // and joined back before the one compositing launch over all views.
     const int ns = (int)B->aux.size();
+    {
+        // one structure-of-arrays copy of the Gaussians per forward, read by every view
+        StageTimer t(FGS_STAGE_PREPROCESS, s);
+        const PreParams& p0 = B->views[0].pre;
+        launch_pack_gaussians(B->P, p0.means, p0.opac, p0.scales, p0.rots, B->packed, s);
+    }
     if (cudaEventRecord(B->forked, s) != cudaSuccess) return FGS_ERR_CUDA;
     for (int i = 0; i < ns; i++) cudaStreamWaitEvent(B->aux[i], B->forked, 0);
     for (int vi = 0; vi < B->V; vi++) {

@@ -172,6 +172,7 @@ int make_params(const fgs_raster_args* a, PreParams& p, bool backward)
     p.energy_floor = a->ogfs_energy_floor;
     p.ratio_min = a->ogfs_radius_ratio_min;
     p.filter3d = a->filter3d_scale;
+    p.packed = nullptr;
     p.aligned = aligned16(p.means) && (!p.opac || aligned16(p.opac)) && (!p.scales || aligned16(p.scales)) &&
                 (!p.rots || aligned16(p.rots)) && (!p.shs || aligned16(p.shs));
     return FGS_OK;

@@ -54,6 +54,33 @@ __device__ __forceinline__ void set_error(unsigned int* err, unsigned int code)
     if (err) atomicOr(err, 1u << code);
 }
 
+// ---------------------------------------------------------------- pinned multiply-add grouping
+// The reference build leaves the fusion of its sums of products to nvcc.  Where
+// an output must equal the reference's bits, the grouping nvcc chose there (found
+// by comparing candidate groupings with the reference build's outputs) is written
+// out with round-to-nearest intrinsics, which the compiler never re-fuses.
+//   dot3<M>:  ((a0 b0 + a1 b1) + a2 b2); M / 2 picks the inner step (0: a0 b0 fused
+//             into the add, 1: a1 b1 fused, 2: no fusion), M % 2 the outer one
+//             (0: a2 b2 fused, 1: not).
+//   sum2<M>:  a b + c d; M = 0: a b fused, 1: c d fused, 2: no fusion.
+template <int M>
+__device__ __forceinline__ float dot3(float a0, float b0, float a1, float b1, float a2, float b2)
+{
+    float x;
+    if constexpr (M / 2 == 0) x = __fmaf_rn(a0, b0, __fmul_rn(a1, b1));
+    else if constexpr (M / 2 == 1) x = __fmaf_rn(a1, b1, __fmul_rn(a0, b0));
+    else x = __fadd_rn(__fmul_rn(a0, b0), __fmul_rn(a1, b1));
+    if constexpr (M % 2 == 0) return __fmaf_rn(a2, b2, x);
+    else return __fadd_rn(x, __fmul_rn(a2, b2));
+}
+template <int M>
+__device__ __forceinline__ float sum2(float a, float b, float c, float d)
+{
+    if constexpr (M == 0) return __fmaf_rn(a, b, __fmul_rn(c, d));
+    else if constexpr (M == 1) return __fmaf_rn(c, d, __fmul_rn(a, b));
+    else return __fadd_rn(__fmul_rn(a, b), __fmul_rn(c, d));
+}
+
 // ---------------------------------------------------------------- 4x4 transforms
 // Column-major 16-float matrices as stored by the reference (auxiliary.h:58-106).
 __device__ __forceinline__ float3 xform_point4x3(const float3& p, const float* m)
@@ -172,6 +199,68 @@ __device__ __forceinline__ float3 ewa_cov2d(const float3& mean, float fx, float 
     return {C.m[0][0], C.m[0][1], C.m[1][1]};
 }
 
+// The forward preprocess's covariance chain with the reference build's grouping
+// spelled out (found by comparing candidate groupings with the reference build's
+// cov3D and conic outputs; every visible Gaussian of three 1080p views of the
+// 2M-Gaussian scene agrees bit for bit).  cov3d_ref: computeCov3D (forward.cu:151-185):
+// in the rotation matrix the products shared by two entries (y y, z z; x z) are the
+// ones left unfused, M = S R takes one product per entry, Sigma = M^T M fuses the
+// first and last products of each dot.  ewa_cov2d_ref: computeCov2D
+// (forward.cu:102-146) with every dot fusing its first and last product.
+__device__ __forceinline__ void cov3d_ref(float sx, float sy, float sz, float mod, float4 q, float cov[6])
+{
+    const float r = q.x, x = q.y, y = q.z, z = q.w;
+    float R[3][3];  // R[c][k]: glm column c, row k
+    R[0][0] = __fsub_rn(1.f, __fmul_rn(2.f, sum2<2>(y, y, z, z)));
+    R[0][1] = __fmul_rn(2.f, sum2<0>(x, y, -r, z));
+    R[0][2] = __fmul_rn(2.f, sum2<1>(x, z, r, y));
+    R[1][0] = __fmul_rn(2.f, sum2<0>(x, y, r, z));
+    R[1][1] = __fsub_rn(1.f, __fmul_rn(2.f, sum2<0>(x, x, z, z)));
+    R[1][2] = __fmul_rn(2.f, sum2<0>(y, z, -r, x));
+    R[2][0] = __fmul_rn(2.f, sum2<1>(x, z, -r, y));
+    R[2][1] = __fmul_rn(2.f, sum2<0>(y, z, r, x));
+    R[2][2] = __fsub_rn(1.f, __fmul_rn(2.f, sum2<0>(x, x, y, y)));
+    const float s[3] = {__fmul_rn(mod, sx), __fmul_rn(mod, sy), __fmul_rn(mod, sz)};
+    float M[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) M[c][k] = __fmul_rn(s[k], R[c][k]);
+    auto sig = [&](int c, int k) { return dot3<0>(M[k][0], M[c][0], M[k][1], M[c][1], M[k][2], M[c][2]); };
+    cov[0] = sig(0, 0); cov[1] = sig(0, 1); cov[2] = sig(0, 2);
+    cov[3] = sig(1, 1); cov[4] = sig(1, 2); cov[5] = sig(2, 2);
+}
+
+__device__ __forceinline__ float3 ewa_cov2d_ref(const float3& mean, float fx, float fy, float tanx, float tany,
+                                                const float* cov3D, const float* v)
+{
+    float tx = __fadd_rn(dot3<0>(v[0], mean.x, v[4], mean.y, v[8], mean.z), v[12]);
+    float ty = __fadd_rn(dot3<0>(v[1], mean.x, v[5], mean.y, v[9], mean.z), v[13]);
+    const float tz = __fadd_rn(dot3<0>(v[2], mean.x, v[6], mean.y, v[10], mean.z), v[14]);
+    const float limx = __fmul_rn(1.3f, tanx), limy = __fmul_rn(1.3f, tany);
+    tx = __fmul_rn(fminf(limx, fmaxf(-limx, __fdiv_rn(tx, tz))), tz);
+    ty = __fmul_rn(fminf(limy, fmaxf(-limy, __fdiv_rn(ty, tz))), tz);
+    const float tz2 = __fmul_rn(tz, tz);
+    const float j00 = __fdiv_rn(fx, tz), j02 = __fdiv_rn(-__fmul_rn(fx, tx), tz2);
+    const float j11 = __fdiv_rn(fy, tz), j12 = __fdiv_rn(-__fmul_rn(fy, ty), tz2);
+    // T = W J (W[c][k] = v[4k + c]); J's zero entries add exact zeros
+    float T[2][3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        T[0][k] = __fmaf_rn(v[4 * k + 2], j02, __fmul_rn(v[4 * k], j00));
+        T[1][k] = __fmaf_rn(v[4 * k + 2], j12, __fmul_rn(v[4 * k + 1], j11));
+    }
+    const float V[3][3] = {{cov3D[0], cov3D[1], cov3D[2]}, {cov3D[1], cov3D[3], cov3D[4]},
+                           {cov3D[2], cov3D[4], cov3D[5]}};
+    float X[3][2];  // X = T^T V^T (rows 0, 1)
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+        for (int k = 0; k < 2; k++) X[c][k] = dot3<0>(T[k][0], V[0][c], T[k][1], V[1][c], T[k][2], V[2][c]);
+    auto cv = [&](int c, int k) { return dot3<0>(X[0][k], T[c][0], X[1][k], T[c][1], X[2][k], T[c][2]); };
+    return {cv(0, 0), cv(0, 1), cv(1, 1)};
+}
+
 // DILATE_PIXEL is a double literal in the reference: max() and += run in double.
 __device__ __forceinline__ float dilate_max(float c) { return (float)fmax((double)c, 0.3); }
 __device__ __forceinline__ float dilate_add(float c) { return (float)((double)c + 0.3); }
@@ -224,45 +313,72 @@ __device__ constexpr float kSH_C3_4 = -0.4570457994644658f;
 __device__ constexpr float kSH_C3_5 = 1.445305721320277f;
 __device__ constexpr float kSH_C3_6 = -0.5900435899266435f;
 
-// Colour of one Gaussian from its SH row `sh` ([M][3] floats).  Writes the
-// per-channel clamp bits (bit c set when channel c was negative).
+// Colour of one Gaussian from its SH row `sh` ([M][3] floats) -- computeColorFromSH
+// (forward.cu:48-99) with the multiply-add grouping of the reference build spelled
+// out (found by comparing candidate groupings with the reference build's colours:
+// every visible Gaussian of three 1080p views of the 2M-Gaussian scene agrees bit
+// for bit).  Writes the per-channel clamp bits (bit c set when channel c was
+// negative).
 __device__ __forceinline__ float3 sh_to_rgb(int deg, const float* __restrict__ sh, float3 pos, float3 campos,
                                             uint8_t& clamp_bits)
 {
-    float3 dir = {pos.x - campos.x, pos.y - campos.y, pos.z - campos.z};
-    const float len = sqrtf(dir.x * dir.x + dir.y * dir.y + dir.z * dir.z);
-    dir.x = dir.x / len; dir.y = dir.y / len; dir.z = dir.z / len;
+    float3 dir = {__fsub_rn(pos.x, campos.x), __fsub_rn(pos.y, campos.y), __fsub_rn(pos.z, campos.z)};
+    const float len = __fsqrt_rn(dot3<0>(dir.x, dir.x, dir.y, dir.y, dir.z, dir.z));  // glm::length
+    dir.x = __fdiv_rn(dir.x, len); dir.y = __fdiv_rn(dir.y, len); dir.z = __fdiv_rn(dir.z, len);
     float res[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) res[c] = kSH_C0 * sh[c];
+    for (int c = 0; c < 3; c++) res[c] = __fmul_rn(kSH_C0, sh[c]);
     if (deg > 0) {
         const float x = dir.x, y = dir.y, z = dir.z;
+        const float c1y = __fmul_rn(kSH_C1, y), c1z = __fmul_rn(kSH_C1, z), c1x = __fmul_rn(kSH_C1, x);
 #pragma unroll
-        for (int c = 0; c < 3; c++)
-            res[c] = res[c] - kSH_C1 * y * sh[3 + c] + kSH_C1 * z * sh[6 + c] - kSH_C1 * x * sh[9 + c];
+        for (int c = 0; c < 3; c++) {
+            // result - C1 y sh1 + C1 z sh2 - C1 x sh3: the first product of the chain is the one fused
+            float r = __fmaf_rn(-c1y, sh[3 + c], res[c]);
+            r = __fmaf_rn(c1z, sh[6 + c], r);
+            res[c] = __fmaf_rn(-c1x, sh[9 + c], r);
+        }
         if (deg > 1) {
-            const float xx = x * x, yy = y * y, zz = z * z;
-            const float xy = x * y, yz = y * z, xz = x * z;
+            const float xx = __fmul_rn(x, x), yy = __fmul_rn(y, y), zz = __fmul_rn(z, z);
+            const float xy = __fmul_rn(x, y), yz = __fmul_rn(y, z), xz = __fmul_rn(x, z);
+            const float f0 = __fmul_rn(kSH_C2_0, xy), f1 = __fmul_rn(kSH_C2_1, yz);
+            const float f2 = __fmul_rn(kSH_C2_2, __fsub_rn(__fsub_rn(__fmul_rn(2.0f, zz), xx), yy));
+            const float f3 = __fmul_rn(kSH_C2_3, xz), f4 = __fmul_rn(kSH_C2_4, __fsub_rn(xx, yy));
 #pragma unroll
-            for (int c = 0; c < 3; c++)
-                res[c] = res[c] + kSH_C2_0 * xy * sh[12 + c] + kSH_C2_1 * yz * sh[15 + c] +
-                         kSH_C2_2 * (2.0f * zz - xx - yy) * sh[18 + c] + kSH_C2_3 * xz * sh[21 + c] +
-                         kSH_C2_4 * (xx - yy) * sh[24 + c];
+            for (int c = 0; c < 3; c++) {
+                float r = __fmaf_rn(f0, sh[12 + c], res[c]);
+                r = __fmaf_rn(f1, sh[15 + c], r);
+                r = __fmaf_rn(f2, sh[18 + c], r);
+                r = __fmaf_rn(f3, sh[21 + c], r);
+                res[c] = __fmaf_rn(f4, sh[24 + c], r);
+            }
             if (deg > 2) {
+                const float q4 = __fsub_rn(__fsub_rn(__fmul_rn(4.0f, zz), xx), yy);  // 4 zz - xx - yy
+                const float g0 = __fmul_rn(__fmul_rn(kSH_C3_0, y), __fmaf_rn(3.0f, xx, -yy));
+                const float g1 = __fmul_rn(__fmul_rn(kSH_C3_1, xy), z);
+                const float g2 = __fmul_rn(__fmul_rn(kSH_C3_2, y), q4);
+                const float g3 = __fmul_rn(__fmul_rn(kSH_C3_3, z),
+                                           __fmaf_rn(-3.0f, yy, __fmaf_rn(-3.0f, xx, __fmul_rn(2.0f, zz))));
+                const float g4 = __fmul_rn(__fmul_rn(kSH_C3_4, x), q4);
+                const float g5 = __fmul_rn(__fmul_rn(kSH_C3_5, z), __fsub_rn(xx, yy));
+                const float g6 = __fmul_rn(__fmul_rn(kSH_C3_6, x), __fmaf_rn(-3.0f, yy, xx));
 #pragma unroll
-                for (int c = 0; c < 3; c++)
-                    res[c] = res[c] + kSH_C3_0 * y * (3.0f * xx - yy) * sh[27 + c] + kSH_C3_1 * xy * z * sh[30 + c] +
-                             kSH_C3_2 * y * (4.0f * zz - xx - yy) * sh[33 + c] +
-                             kSH_C3_3 * z * (2.0f * zz - 3.0f * xx - 3.0f * yy) * sh[36 + c] +
-                             kSH_C3_4 * x * (4.0f * zz - xx - yy) * sh[39 + c] + kSH_C3_5 * z * (xx - yy) * sh[42 + c] +
-                             kSH_C3_6 * x * (xx - 3.0f * yy) * sh[45 + c];
+                for (int c = 0; c < 3; c++) {
+                    float r = __fmaf_rn(g0, sh[27 + c], res[c]);
+                    r = __fmaf_rn(g1, sh[30 + c], r);
+                    r = __fmaf_rn(g2, sh[33 + c], r);
+                    r = __fmaf_rn(g3, sh[36 + c], r);
+                    r = __fmaf_rn(g4, sh[39 + c], r);
+                    r = __fmaf_rn(g5, sh[42 + c], r);
+                    res[c] = __fmaf_rn(g6, sh[45 + c], r);
+                }
             }
         }
     }
     clamp_bits = 0;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        res[c] += 0.5f;
+        res[c] = __fadd_rn(res[c], 0.5f);
         if (res[c] < 0) clamp_bits |= (uint8_t)(1u << c);
     }
     return {fmaxf(res[0], 0.0f), fmaxf(res[1], 0.0f), fmaxf(res[2], 0.0f)};

@@ -28,7 +28,15 @@ struct PreParams {
     float eps_scale, eps_max, energy_floor, ratio_min;
     float filter3d;
     int aligned;              // means/scales/rots/opac 16-byte aligned: stage with float4 loads
+    // Optional structure-of-arrays copy of the per-Gaussian inputs the preprocess reads
+    // ([3][P] float4: {mean, opacity}, {scale, 0}, rotation), one coalesced float4 load
+    // each; null: the reference's AoS tensors above are read instead.
+    const float4* packed;
 };
+// Writes the packed copy (PreParams::packed) of P Gaussians' means, opacities,
+// scales and rotations (the last two planes only when scales/rots are given).
+void launch_pack_gaussians(int P, const float* means, const float* opac, const float* scales, const float* rots,
+                           float4* packed, cudaStream_t s);
 
 // Geometry workspace views (per-Gaussian state kept from forward to backward).
 struct GeomState {

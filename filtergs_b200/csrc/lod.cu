@@ -119,20 +119,34 @@ __global__ void gather_kernel(const int64_t* __restrict__ index, long long N, co
 }
 
 // eval_sh_wobase (LoG/model/sh_utils.py:31-68) for one channel of the rest
-// coefficients rest[k*3 + c], k = 0 .. (deg+1)^2 - 2.
+// coefficients rest[k*3 + c], k = 0 .. (deg+1)^2 - 2.  The reference evaluates it
+// as a chain of torch element-wise ops, each rounded on its own (a Python scalar
+// becomes a float operand): the same ops in the same order here, with
+// round-to-nearest intrinsics so that no multiply-add is fused.
 __device__ __forceinline__ float sh_wobase(int deg, const float* rest, int c, float x, float y, float z)
 {
     auto R = [&](int k) { return rest[k * 3 + c]; };
-    float r = -kSH_C1 * y * R(0) + kSH_C1 * z * R(1) - kSH_C1 * x * R(2);
+    auto M = [](float a, float b) { return __fmul_rn(a, b); };
+    auto P = [](float a, float b) { return __fadd_rn(a, b); };
+    auto D = [](float a, float b) { return __fsub_rn(a, b); };
+    // - C1 * y * sh0 + C1 * z * sh1 - C1 * x * sh2
+    float r = D(P(M(M(-kSH_C1, y), R(0)), M(M(kSH_C1, z), R(1))), M(M(kSH_C1, x), R(2)));
     if (deg > 1) {
-        const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
-        r = r + kSH_C2_0 * xy * R(3) + kSH_C2_1 * yz * R(4) + kSH_C2_2 * (2.0f * zz - xx - yy) * R(5) +
-            kSH_C2_3 * xz * R(6) + kSH_C2_4 * (xx - yy) * R(7);
-        if (deg > 2)
-            r = r + kSH_C3_0 * y * (3 * xx - yy) * R(8) + kSH_C3_1 * xy * z * R(9) +
-                kSH_C3_2 * y * (4 * zz - xx - yy) * R(10) + kSH_C3_3 * z * (2 * zz - 3 * xx - 3 * yy) * R(11) +
-                kSH_C3_4 * x * (4 * zz - xx - yy) * R(12) + kSH_C3_5 * z * (xx - yy) * R(13) +
-                kSH_C3_6 * x * (xx - 3 * yy) * R(14);
+        const float xx = M(x, x), yy = M(y, y), zz = M(z, z), xy = M(x, y), yz = M(y, z), xz = M(x, z);
+        r = P(r, M(M(kSH_C2_0, xy), R(3)));
+        r = P(r, M(M(kSH_C2_1, yz), R(4)));
+        r = P(r, M(M(kSH_C2_2, D(D(M(2.0f, zz), xx), yy)), R(5)));
+        r = P(r, M(M(kSH_C2_3, xz), R(6)));
+        r = P(r, M(M(kSH_C2_4, D(xx, yy)), R(7)));
+        if (deg > 2) {
+            r = P(r, M(M(M(kSH_C3_0, y), D(M(3.0f, xx), yy)), R(8)));
+            r = P(r, M(M(M(kSH_C3_1, xy), z), R(9)));
+            r = P(r, M(M(M(kSH_C3_2, y), D(D(M(4.0f, zz), xx), yy)), R(10)));
+            r = P(r, M(M(M(kSH_C3_3, z), D(D(M(2.0f, zz), M(3.0f, xx)), M(3.0f, yy))), R(11)));
+            r = P(r, M(M(M(kSH_C3_4, x), D(D(M(4.0f, zz), xx), yy)), R(12)));
+            r = P(r, M(M(M(kSH_C3_5, z), D(xx, yy)), R(13)));
+            r = P(r, M(M(M(kSH_C3_6, x), D(xx, M(3.0f, yy))), R(14)));
+        }
     }
     return r;
 }
@@ -154,18 +168,26 @@ __global__ void gather_activate_kernel(const int64_t* __restrict__ index, const 
         o_xyz[3 * n] = px; o_xyz[3 * n + 1] = py; o_xyz[3 * n + 2] = pz;
 #pragma unroll
         for (int k = 0; k < 3; k++) o_scale[3 * n + k] = expf(log_scale[3 * s + k]);
+        // torch.nn.functional.normalize: x / max(|x|, 1e-12), where torch's norm over the
+        // last dim of 4 adds the rounded squares as (x0^2 + x2^2) + (x1^2 + x3^2) (and
+        // over 3 as (x0^2 + x2^2) + x1^2), matched bit for bit against torch on the GPU
         const float4 q = *reinterpret_cast<const float4*>(rot + 4 * s);
-        const float nr = fmaxf(sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w), 1e-12f);
-        *reinterpret_cast<float4*>(o_rot + 4 * n) = make_float4(q.x / nr, q.y / nr, q.z / nr, q.w / nr);
-        o_opac[n] = 1.0f / (1.0f + expf(-opac_raw[s]));
-        float dx = px - campos[0], dy = py - campos[1], dz = pz - campos[2];
-        const float dl = sqrtf(dx * dx + dy * dy + dz * dz);
-        dx /= dl; dy /= dl; dz /= dl;
+        const float q2 = __fadd_rn(__fadd_rn(__fmul_rn(q.x, q.x), __fmul_rn(q.z, q.z)),
+                                   __fadd_rn(__fmul_rn(q.y, q.y), __fmul_rn(q.w, q.w)));
+        const float nr = fmaxf(__fsqrt_rn(q2), 1e-12f);
+        *reinterpret_cast<float4*>(o_rot + 4 * n) =
+            make_float4(__fdiv_rn(q.x, nr), __fdiv_rn(q.y, nr), __fdiv_rn(q.z, nr), __fdiv_rn(q.w, nr));
+        o_opac[n] = __fdiv_rn(1.0f, __fadd_rn(1.0f, expf(-opac_raw[s])));
+        // dir_pp = xyz - camera_center; dir_pp / torch.norm(dir_pp, dim=-1) (activation.py:36-43)
+        float dx = __fsub_rn(px, campos[0]), dy = __fsub_rn(py, campos[1]), dz = __fsub_rn(pz, campos[2]);
+        const float dl = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz)), __fmul_rn(dy, dy)));
+        dx = __fdiv_rn(dx, dl); dy = __fdiv_rn(dy, dl); dz = __fdiv_rn(dz, dl);
         const float* rs = rest ? rest + (size_t)s * rest_coeffs * 3 : nullptr;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            float col = dc[3 * s + c] * kSH_C0 + 0.5f;
-            if (deg > 0 && rs) col += sh_wobase(deg, rs, c, dx, dy, dz);
+            // SH2RGB (sh_utils.py:78): two torch ops, then the add of activation.py:40
+            float col = __fadd_rn(__fmul_rn(dc[3 * s + c], kSH_C0), 0.5f);
+            if (deg > 0 && rs) col = __fadd_rn(col, sh_wobase(deg, rs, c, dx, dy, dz));
             o_rgb[3 * n + c] = col;
         }
     }

@@ -26,6 +26,53 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Per-Gaussian inputs: from the packed structure-of-arrays copy when there is one
+// (one float4 per plane), else from the reference's AoS tensors.
+__device__ __forceinline__ float3 in_mean(const PreParams& p, int idx)
+{
+    if (p.packed) {
+        const float4 v = __ldg(p.packed + idx);
+        return {v.x, v.y, v.z};
+    }
+    return {__ldg(p.means + 3 * (size_t)idx), __ldg(p.means + 3 * (size_t)idx + 1),
+            __ldg(p.means + 3 * (size_t)idx + 2)};
+}
+__device__ __forceinline__ float in_opacity(const PreParams& p, int idx)
+{
+    return p.packed ? __ldg(p.packed + idx).w : __ldg(p.opac + idx);
+}
+__device__ __forceinline__ float3 in_scale(const PreParams& p, int idx)
+{
+    if (p.packed) {
+        const float4 v = __ldg(p.packed + (size_t)p.P + idx);
+        return {v.x, v.y, v.z};
+    }
+    return {__ldg(p.scales + 3 * (size_t)idx), __ldg(p.scales + 3 * (size_t)idx + 1),
+            __ldg(p.scales + 3 * (size_t)idx + 2)};
+}
+__device__ __forceinline__ float4 in_rot(const PreParams& p, int idx)
+{
+    if (p.packed) return __ldg(p.packed + 2 * (size_t)p.P + idx);
+    if (p.aligned) return __ldg(reinterpret_cast<const float4*>(p.rots) + idx);
+    return make_float4(__ldg(p.rots + 4 * (size_t)idx), __ldg(p.rots + 4 * (size_t)idx + 1),
+                       __ldg(p.rots + 4 * (size_t)idx + 2), __ldg(p.rots + 4 * (size_t)idx + 3));
+}
+
+__global__ void pack_gaussians_kernel(int P, const float* __restrict__ means, const float* __restrict__ opac,
+                                      const float* __restrict__ scales, const float* __restrict__ rots,
+                                      float4* __restrict__ out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+        out[i] = make_float4(means[3 * (size_t)i], means[3 * (size_t)i + 1], means[3 * (size_t)i + 2], opac[i]);
+        if (scales && rots) {
+            out[(size_t)P + i] =
+                make_float4(scales[3 * (size_t)i], scales[3 * (size_t)i + 1], scales[3 * (size_t)i + 2], 0.f);
+            out[2 * (size_t)P + i] = make_float4(rots[4 * (size_t)i], rots[4 * (size_t)i + 1],
+                                                 rots[4 * (size_t)i + 2], rots[4 * (size_t)i + 3]);
+        }
+    }
+}
+
 // trace(cov3D) for cov3D = M^T M, M = S R (forward.cu:151-185): the sum of the
 // squared entries of M, row r of R scaled by s_r.
 __device__ __forceinline__ float cov3d_trace(float sx, float sy, float sz, float mod, float4 q)
@@ -91,8 +138,7 @@ __global__ void __launch_bounds__(kThreads) preprocess_cull_kernel(PreParams p, 
         const int idx = idx0 + threadIdx.x;
         bool cand = false;
         if (idx < p.P) {
-            const float3 p_orig = {__ldg(p.means + 3 * (size_t)idx), __ldg(p.means + 3 * (size_t)idx + 1),
-                                   __ldg(p.means + 3 * (size_t)idx + 2)};
+            const float3 p_orig = in_mean(p, idx);
             const float3 p_view = xform_point4x3(p_orig, p.view);
             if (p_view.z <= 0.2f) {  // auxiliary.h:139-164
                 if (p.prefiltered) set_error(g.err, FGS_ERR_PREFILTERED);
@@ -102,11 +148,9 @@ __global__ void __launch_bounds__(kThreads) preprocess_cull_kernel(PreParams p, 
                 const float4 p_hom = xform_point4x4(p_orig, p.proj);
                 const float p_w = 1.0f / (p_hom.w + 0.0000001f);
                 const float px = ndc_to_pix(p_hom.x * p_w, p.W), py = ndc_to_pix(p_hom.y * p_w, p.H);
-                const float4 q = p.aligned ? __ldg(reinterpret_cast<const float4*>(p.rots) + idx)
-                                           : make_float4(__ldg(p.rots + 4 * (size_t)idx), __ldg(p.rots + 4 * (size_t)idx + 1),
-                                                         __ldg(p.rots + 4 * (size_t)idx + 2), __ldg(p.rots + 4 * (size_t)idx + 3));
-                float tr = cov3d_trace(__ldg(p.scales + 3 * (size_t)idx), __ldg(p.scales + 3 * (size_t)idx + 1),
-                                       __ldg(p.scales + 3 * (size_t)idx + 2), p.scale_mod, q);
+                const float4 q = in_rot(p, idx);
+                const float3 sc = in_scale(p, idx);
+                float tr = cov3d_trace(sc.x, sc.y, sc.z, p.scale_mod, q);
                 if (p.filter3d > 0.f) {
                     const float sf = p.filter3d * p_view.z / p.fx;
                     tr += 3.f * sf * sf;
@@ -178,8 +222,7 @@ __global__ void __launch_bounds__(kThreads) preprocess_full_kernel(PreParams p, 
         int radius_px = 0;
         uint8_t clamp_bits = 0;
         PairRecord rec;
-        const float3 p_orig = {__ldg(p.means + 3 * (size_t)idx), __ldg(p.means + 3 * (size_t)idx + 1),
-                               __ldg(p.means + 3 * (size_t)idx + 2)};
+        const float3 p_orig = in_mean(p, idx);
         const float4 p_hom = xform_point4x4(p_orig, p.proj);
         const float p_w = 1.0f / (p_hom.w + 0.0000001f);
         const float3 p_proj = {p_hom.x * p_w, p_hom.y * p_w, p_hom.z * p_w};
@@ -190,29 +233,29 @@ __global__ void __launch_bounds__(kThreads) preprocess_full_kernel(PreParams p, 
 #pragma unroll
             for (int c = 0; c < 6; c++) cov3D[c] = __ldg(p.cov3D + (size_t)idx * 6 + c);
         } else {
-            const float4 q = vec ? __ldg(reinterpret_cast<const float4*>(p.rots) + idx)
-                                 : make_float4(__ldg(p.rots + 4 * (size_t)idx), __ldg(p.rots + 4 * (size_t)idx + 1),
-                                               __ldg(p.rots + 4 * (size_t)idx + 2), __ldg(p.rots + 4 * (size_t)idx + 3));
-            cov3d_from_scale_rot(__ldg(p.scales + 3 * (size_t)idx), __ldg(p.scales + 3 * (size_t)idx + 1),
-                                 __ldg(p.scales + 3 * (size_t)idx + 2), p.scale_mod, q, cov3D);
+            const float4 q = in_rot(p, idx);
+            const float3 sc = in_scale(p, idx);
+            cov3d_ref(sc.x, sc.y, sc.z, p.scale_mod, q, cov3D);
         }
         if (p.filter3d > 0.f) {
-            // 3D filter: isotropic variance of a sigma = s * z / focal blur.
-            const float sf = p.filter3d * p_view.z / p.fx;
-            const float v = sf * sf;
-            cov3D[0] += v; cov3D[3] += v; cov3D[5] += v;
+            // 3D filter: isotropic variance of a sigma = s * z / focal blur, added as its own
+            // rounded terms (what feeding the filtered covariance to the reference gives)
+            const float sf = __fdiv_rn(__fmul_rn(p.filter3d, p_view.z), p.fx);
+            const float v = __fmul_rn(sf, sf);
+            cov3D[0] = __fadd_rn(cov3D[0], v); cov3D[3] = __fadd_rn(cov3D[3], v); cov3D[5] = __fadd_rn(cov3D[5], v);
         }
-        float3 cov = ewa_cov2d(p_orig, p.fx, p.fy, p.tanx, p.tany, cov3D, p.view);
+        float3 cov = ewa_cov2d_ref(p_orig, p.fx, p.fy, p.tanx, p.tany, cov3D, p.view);
         if (p.use_filter) {
             cov.x = dilate_max(cov.x);
             cov.z = dilate_max(cov.z);
         }
-        const float det = (cov.x * cov.z - cov.y * cov.y);
+        // forward.cu:328-330, the first product fused as in the reference build
+        const float det = __fmaf_rn(cov.x, cov.z, -__fmul_rn(cov.y, cov.y));
         if (det != 0.0f) {
-            const float det_inv = 1.f / det;
-            const float3 conic = {cov.z * det_inv, -cov.y * det_inv, cov.x * det_inv};
+            const float det_inv = __fdiv_rn(1.f, det);
+            const float3 conic = {__fmul_rn(cov.z, det_inv), __fmul_rn(-cov.y, det_inv), __fmul_rn(cov.x, det_inv)};
             // forward.cu:345-369: OGFS radius
-            const float opacity = fmaxf(__ldg(p.opac + idx), 1e-6f);
+            const float opacity = fmaxf(in_opacity(p, idx), 1e-6f);
             const float log_opacity = logf(opacity);
             const float radius_energy = log_opacity - s_log_lambda_G;
             const float energy_clamped = fmaxf(radius_energy, p.energy_floor);
@@ -523,6 +566,15 @@ void launch_preprocess(const PreParams& p, const GeomState& g, int* radii, cudaS
     compact_visible_kernel<<<nch, kThreads, 0, s>>>(p.P, g.tiles, g.grec, g.chunk_counts, g.sort_ids_b,
                                                     g.depth_key);
     note_launches(4);
+}
+
+void launch_pack_gaussians(int P, const float* means, const float* opac, const float* scales, const float* rots,
+                           float4* packed, cudaStream_t s)
+{
+    if (P <= 0) return;
+    const int blocks = (int)min((P + 255) / 256, 148 * 8);
+    pack_gaussians_kernel<<<blocks, 256, 0, s>>>(P, means, opac, scales, rots, packed);
+    note_launches(1);
 }
 
 void launch_compute_radius(int variant, int P, const float* means, const float* scales, const float* rots,

@@ -81,10 +81,49 @@ def lod_case(name, P, seed):
     print(name, "nodes", P, "kept", int(out["mask"].sum()))
 
 
+def urban_case(name="urban_1080", n=3000, out_dir=HERE):
+    """The headline scene (2,000,000 Gaussians, 1920x1080 camera 0 of the benchmark) through the
+    reference's forward; a seeded sample of n visible Gaussians with their inputs and the
+    reference's per-Gaussian cov3D, conic and colour (for the CPU pin of oracle/ref_fp32.py)."""
+    import bench
+    ref = build_ref.load("ref_rasterizer_C")
+    sc, scene = bench.make_scene(2_000_000, torch.device("cuda"))
+    cam = bench.rank_cameras(1, 0)[0]
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()  # noqa: E731
+    bg, e = torch.zeros(3, device="cuda"), torch.Tensor([])
+    fwd = ref.rasterize_gaussians(bg, scene["means3D"], e, scene["opacities"], scene["scales"], scene["rotations"],
+                                  1.0, e, t(cam.viewmatrix), t(cam.projmatrix), cam.tanfovx, cam.tanfovy, cam.H, cam.W,
+                                  scene["shs"], 3, t(cam.campos), False, True, False, 0.2, 0.2, 0.05, 0.7, False)
+    torch.cuda.synchronize()
+    P = 2_000_000
+    rb = ref_buffers(fwd, P, cam.W, cam.H)
+    geom, o = fwd[6], 0
+    for nbytes in (4 * P, 3 * P, 4 * P, 8 * P):       # depths, clamped, internal radii, means2D
+        o = (o + nbytes + 127) & ~127
+    cov3D = geom[o:o + 24 * P].view(torch.float32).view(P, 6)
+    radii = fwd[5].cpu().numpy()
+    vis = np.nonzero(radii > 0)[0]
+    pick = np.sort(np.random.default_rng(2105).choice(vis, size=n, replace=False))
+    tp = torch.from_numpy(pick).cuda()
+    out = dict(means3D=sc["means3D"][pick], scales=sc["scales"][pick], rotations=sc["rotations"][pick],
+               opacities=sc["opacities"][pick], shs=sc["shs"][pick], sh_degree=3, colors=np.zeros((0, 3), np.float32),
+               use_filter=1, W=cam.W, H=cam.H, tanfovx=cam.tanfovx, tanfovy=cam.tanfovy,
+               viewmatrix=cam.viewmatrix, projmatrix=cam.projmatrix, campos=cam.campos, radii=radii[pick],
+               index=pick, ref_cov3D=cov3D[tp].cpu().numpy(), ref_conic_opacity=rb["conic_opacity"][tp].cpu().numpy(),
+               ref_rgb=rb["rgb"][tp].cpu().numpy(), ref_means2D=rb["means2D"][tp].cpu().numpy(),
+               ref_depths=rb["depths"][tp].cpu().numpy())
+    np.savez_compressed(os.path.join(out_dir, f"ref_{name}.npz"), **out)
+    print(name, "visible", len(vis), "sampled", n)
+
+
 if __name__ == "__main__":
     assert build_ref.load("ref_rasterizer_C") is not None, "reference build missing"
+    if sys.argv[1:2] == ["urban"]:                  # only the headline-scene sample, into the given directory
+        urban_case(out_dir=sys.argv[2] if len(sys.argv) > 2 else HERE)
+        sys.exit(0)
     raster_case("sh3_filter", P=1200, W=96, H=64, seed=2101)
     raster_case("colors_nofilter_ragged", P=900, W=90, H=52, seed=2102, degree=0, colors_precomp=True,
                 use_filter=False, bg=(0.3, 0.1, 0.7))
     raster_case("sh1_dense", P=3000, W=64, H=64, seed=2103, degree=1)
     lod_case("lod_tree", P=6000, seed=2104)
+    urban_case()

@@ -1,14 +1,17 @@
 """GPU: the headline workload at its full size (2,000,000 Gaussians of the urban aerial
-scene, SH 3, the benchmark's 1920x1080 cameras) checked through properties that do not
-depend on size, and against the reference's own CUDA build.
+scene, SH 3, the benchmark's 1920x1080 cameras) against the reference's own CUDA build and
+through properties that do not depend on size.
 
-* the reference build: num_rendered, radii, the 2D means and depths bit-exact.  The conic
-  of a few percent of the visible Gaussians differs from the reference's by some ulps (the
-  compilers fuse the covariance chain's multiply-adds differently), which moves the
-  early-termination test T < 1e-4 of a handful of pixels per view and the colour of a few
-  hundred: n_contrib and point_id are held to all but 1e-5 of the pixels (measured: 2-3 and
-  0 of 2,073,600), image values to 1e-5 in all but 2e-4 of them (measured: 419 of 6.2 M
-  values beyond it, the largest 2.9e-4);
+* the reference build, forward: num_rendered, radii, 2D means, depths, conics, colours,
+  sorted keys, tile ranges, n_contrib, point_id, final T and the image bit for bit on two
+  cameras (the preprocess writes out the reference build's multiply-add grouping, and the
+  compositing arithmetic is the reference's);
+* the reference build, backward (ref_compat): the screen-space, colour, opacity, mean and SH
+  gradients within 1e-4 norm-relative; the covariance, scale and rotation gradients -- sums
+  of many cancelling per-pixel terms, which the reference adds with float atomics in
+  arbitrary order -- within 1e-4 or twice the reference's own run-to-run difference on the
+  same inputs, whichever is larger; a 2-view batched step's summed gradients against the sum
+  of the reference's per-view gradients the same way;
 * binning: num_rendered equals the sum of tiles touched; the sorted keys are non-decreasing
   (tile, then depth bits); the tile ranges partition [0, K) in tile order; n_contrib never
   exceeds its tile's range;
@@ -19,12 +22,15 @@ import numpy as np
 import pytest
 import torch
 
-from _helpers import ours, ref_buffers
+from _helpers import norm_rel, ours, ref_buffers
 
 pytestmark = pytest.mark.gpu
 
-IMG_TOL = 1e-5
-PIXEL_FRACTION = 1e-5
+GRAD_TOL = 1e-4
+GRAD_NAMES = ["means2D", "colors", "opacity", "means3D", "cov3D", "sh", "scales", "rotations"]
+# gradients that sum many cancelling per-pixel terms: the reference's own atomic summation
+# order moves them by more than 1e-4 from run to run
+ILL_CONDITIONED = ("cov3D", "scales", "rotations")
 
 
 @pytest.fixture(scope="module")
@@ -47,9 +53,10 @@ def _fwd(mod, scene, c):
                                    scene["shs"], 3, _t(c.campos), False, True, False, 0.2, 0.2, 0.05, 0.7, False)
 
 
-def _bwd(scene, c, f, dL):
-    e = torch.empty(0, device="cuda")
-    return ours.rasterize_gaussians_backward(torch.zeros(3, device="cuda"), scene["means3D"], f[5], e,
+def _bwd(scene, c, f, dL, mod=None):
+    mod = mod or ours
+    e = torch.empty(0, device="cuda") if mod is ours else torch.Tensor([])
+    return mod.rasterize_gaussians_backward(torch.zeros(3, device="cuda"), scene["means3D"], f[5], e,
                                              scene["scales"], scene["rotations"], 1.0, e, _t(c.viewmatrix),
                                              _t(c.projmatrix), c.tanfovx, c.tanfovy, dL, scene["shs"], 3,
                                              _t(c.campos), f[6], f[0], f[7], f[8], False)
@@ -57,23 +64,27 @@ def _bwd(scene, c, f, dL):
 
 def test_fullsize_vs_reference_and_binning_properties(cuda, ref, full):
     scene, cams = full
-    c = cams[0]
-    P, N = int(scene["means3D"].shape[0]), c.W * c.H
-    mine = _fwd(ours, scene, c)
-    theirs = _fwd(ref, scene, c)
-    torch.cuda.synchronize()
-    K = mine[0]
-    assert K == theirs[0] and K > 1_000_000
-    assert torch.equal(mine[5], theirs[5]), "radii"
-    po = ours.preprocess_outputs(mine[6], P)
-    rb = ref_buffers(theirs, P, c.W, c.H)
-    vis = mine[5] > 0
-    assert torch.equal(po["means2D"][vis], rb["means2D"][vis]) and torch.equal(po["depths"][vis], rb["depths"][vis])
-    io = ours.image_outputs(mine[8], c.W, c.H)
-    assert int((io["n_contrib"] != rb["n_contrib"]).sum()) <= PIXEL_FRACTION * N, "n_contrib"
-    assert int((mine[2] != theirs[2]).sum()) <= PIXEL_FRACTION * N, "point_id"
-    d = (mine[1] - theirs[1]).abs()
-    assert float(d.max()) <= 1e-3 and int((d > IMG_TOL).sum()) <= 2e-4 * 3 * N, "image"
+    P = int(scene["means3D"].shape[0])
+    for c in cams:
+        mine = _fwd(ours, scene, c)
+        theirs = _fwd(ref, scene, c)
+        torch.cuda.synchronize()
+        K = mine[0]
+        assert K == theirs[0] and K > 1_000_000
+        assert torch.equal(mine[5], theirs[5]), "radii"
+        po = ours.preprocess_outputs(mine[6], P)
+        rb = ref_buffers(theirs, P, c.W, c.H)
+        vis = mine[5] > 0
+        for k in ("means2D", "depths", "conic_opacity", "rgb", "tiles_touched"):
+            assert torch.equal(po[k][vis], rb[k][vis]), k
+        keys, vals = ours.sorted_pairs(mine[6], mine[7], P, K)
+        assert torch.equal(keys, rb["keys"]) and torch.equal(vals, rb["vals"]), "sorted pairs"
+        io = ours.image_outputs(mine[8], c.W, c.H)
+        for k in ("ranges", "n_contrib", "final_T"):
+            assert torch.equal(io[k], rb[k]), k
+        assert torch.equal(mine[2], theirs[2]), "point_id"
+        assert torch.equal(mine[3], theirs[3]), "point_weight_pixel"
+        assert torch.equal(mine[1], theirs[1]), "image"
     # binning properties
     assert int(po["tiles_touched"][vis].sum()) == K
     keys, _vals = ours.sorted_pairs(mine[6], mine[7], P, K)
@@ -137,3 +148,57 @@ def test_fullsize_batched_equals_plain(cuda, full):
         sums["opacity"] += gr[2]
     for k in ("means3D", "sh", "opacity"):
         assert torch.equal(br.grad[k], sums[k]), k
+
+
+def _grad_check(name, mine, ref1, ref2):
+    """mine vs the reference within GRAD_TOL, or (ill-conditioned sums) within twice the
+    reference's own run-to-run difference ref2 vs ref1."""
+    d = norm_rel(mine, ref1)
+    if name in ILL_CONDITIONED:
+        tol = max(GRAD_TOL, 2.0 * norm_rel(ref2, ref1))
+    else:
+        tol = GRAD_TOL
+    assert d <= tol, (name, d, tol)
+    return d
+
+
+def test_fullsize_gradients_vs_reference(cuda, ref, full):
+    scene, cams = full
+    for i, c in enumerate(cams):
+        g = torch.Generator(device="cuda").manual_seed(40 + i)
+        dL = torch.randn(3, c.H, c.W, device="cuda", generator=g)
+        mine = _bwd(scene, c, _fwd(ours, scene, c), dL)
+        rf = _fwd(ref, scene, c)
+        r1, r2 = _bwd(scene, c, rf, dL, ref), _bwd(scene, c, rf, dL, ref)
+        torch.cuda.synchronize()
+        for n, a, b1, b2 in zip(GRAD_NAMES, mine, r1, r2):
+            assert a.shape == b1.shape, n
+            _grad_check(n, a, b1, b2)
+
+
+def test_fullsize_batched_gradients_vs_reference(cuda, ref, full):
+    """One 2-view batched step: the shared gradients against the sums of the reference's
+    per-view gradients (means3D, opacity, SH, scales, rotations)."""
+    from filtergs_b200.batched import BatchedRasterizer, Camera
+    scene, cams = full
+    bc = [Camera(c.W, c.H, c.tanfovx, c.tanfovy, _t(c.viewmatrix), _t(c.projmatrix), _t(c.campos)) for c in cams]
+    br = BatchedRasterizer(scene["means3D"], scene["opacities"], scene["scales"], scene["rotations"], bc,
+                           shs=scene["shs"], sh_degree=3, bg=torch.zeros(3, device="cuda"), graph=True)
+    g = torch.Generator(device="cuda").manual_seed(44)
+    dls = [torch.randn(3, c.H, c.W, device="cuda", generator=g) for c in cams]
+    for v, d in enumerate(dls):
+        br.dL[v].copy_(d)
+    br.step()
+    br.check()
+    keys = {"means3D": 3, "opacity": 2, "sh": 5, "scales": 6, "rotations": 7}
+    s1 = {k: torch.zeros_like(v) for k, v in br.grad.items()}
+    s2 = {k: torch.zeros_like(v) for k, v in br.grad.items()}
+    for c, d in zip(cams, dls):
+        rf = _fwd(ref, scene, c)
+        r1, r2 = _bwd(scene, c, rf, d, ref), _bwd(scene, c, rf, d, ref)
+        for k, j in keys.items():
+            s1[k] += r1[j].reshape(s1[k].shape)
+            s2[k] += r2[j].reshape(s2[k].shape)
+    torch.cuda.synchronize()
+    for k in keys:
+        _grad_check(k, br.grad[k], s1[k], s2[k])
