@@ -80,6 +80,7 @@ SIGNATURES = {
     "fgs_compact_scratch_bytes": (sz, [i32]),
     "fgs_compact_mask": (i32, [i32, vp, vp, vp, vp, vp]),
     "fgs_gather_activate": (i32, [i64, vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, vp]),
+    "fgs_rows_valid": (i32, [i64, vp, vp, vp, vp, vp, vp, vp, vp]),
     "fgs_radius_raw": (i32, [i32, vp, vp, vp, vp, vp, f32, f32, f32, f32, vp, vp]),
     "fgs_log_cut_scratch_bytes": (sz, [i32, i32, i32, i32]),
     "fgs_log_cut": (i32, [i32, vp, i32, vp, vp, i32, vp, f32, i32, vp, vp, vp, vp]),

@@ -427,6 +427,30 @@ void launch_gather(const int64_t* index, long long N, const float* xyz, const fl
     note_launches(1);
 }
 
+namespace {
+// FilterGS/filtergs.py:159-172: a gathered, activated row is rendered only when xyz,
+// scaling, rotation, opacity and colour are all finite, the smallest scale is > 0 and
+// the opacity is > 0.  Writes keep[n] (1 = render) and counts the rows dropped.
+__global__ void rows_valid_kernel(long long N, const float* __restrict__ xyz, const float* __restrict__ sc,
+                                  const float* __restrict__ rot, const float* __restrict__ opac,
+                                  const float* __restrict__ col, uint8_t* __restrict__ keep,
+                                  unsigned long long* __restrict__ dropped)
+{
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < N; n += (long long)gridDim.x * blockDim.x) {
+        bool ok = isfinite(opac[n]) && opac[n] > 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            ok = ok && isfinite(xyz[3 * n + k]) && isfinite(col[3 * n + k]) && isfinite(sc[3 * n + k]);
+        }
+        ok = ok && fminf(fminf(sc[3 * n], sc[3 * n + 1]), sc[3 * n + 2]) > 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; k++) ok = ok && isfinite(rot[4 * n + k]);
+        keep[n] = ok ? 1 : 0;
+        if (!ok) atomicAdd(dropped, 1ull);
+    }
+}
+}  // namespace
+
 void launch_gather_activate(const int64_t* index, const unsigned long long* count, long long N_cap, const float* xyz,
                             const float* log_scale, const float* rot, const float* opac_raw, const float* dc,
                             const float* rest, int deg, int rest_coeffs, const float* campos, float* o_xyz,
@@ -558,6 +582,21 @@ int fgs_compact_mask(int n, const uint8_t* mask, int64_t* out_index, unsigned lo
     unsigned* err = reinterpret_cast<unsigned*>(sc + 2 + (n + 255) / 256);
     cudaMemsetAsync(err, 0, sizeof(unsigned), static_cast<cudaStream_t>(stream));
     launch_compact(mask, (uint32_t)n, out_index, count, sc, err, static_cast<cudaStream_t>(stream));
+    return launch_status();
+}
+
+int fgs_rows_valid(long long N, const float* xyz, const float* scaling, const float* rotation, const float* opacity,
+                   const float* colors, uint8_t* keep, unsigned long long* dropped, void* stream)
+{
+    if (N < 0 || !dropped) return FGS_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaMemsetAsync(dropped, 0, sizeof(unsigned long long), s);
+    if (N == 0) return launch_status();
+    if (!xyz || !scaling || !rotation || !opacity || !colors || !keep) return FGS_ERR_ARG;
+    const long long want = (N + 255) / 256;
+    rows_valid_kernel<<<(int)(want < 1184 ? want : 1184), 256, 0, s>>>(N, xyz, scaling, rotation, opacity, colors,
+                                                                    keep, dropped);
+    note_launches(1);
     return launch_status();
 }
 

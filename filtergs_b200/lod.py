@@ -139,10 +139,28 @@ def gather_activate(scene, index, count, campos, cap=None):
     return o
 
 
+def drop_invalid_rows(rows):
+    """FilterGS.render's guard (FilterGS/filtergs.py:159-172): keep the rows whose attributes are all
+    finite with min(scale) > 0 and opacity > 0, in order.  Rows are returned unchanged when none is
+    dropped (the common case: one device flag read)."""
+    dev = rows["xyz"].device
+    n = int(rows["xyz"].shape[0])
+    keep = torch.empty(n, dtype=torch.uint8, device=dev)
+    dropped = torch.zeros(1, dtype=torch.int64, device=dev)
+    call("fgs_rows_valid", n, _p(rows["xyz"]), _p(rows["scaling"]), _p(rows["rotation"]), _p(rows["opacity"]),
+         _p(rows["colors"]), _p(keep), _p(dropped), _s())
+    if int(dropped.item()) == 0:
+        return rows
+    idx, cnt = compact(keep)
+    idx = idx[:int(cnt.item())]
+    return {k: v.index_select(0, idx) for k, v in rows.items()}
+
+
 def render_selected(scene, index, count, view, proj, campos, cam, bg, use_filter=True, stats=False):
-    """Gather + activate the selected rows and rasterize them (forward only, colours precomputed)."""
-    n = int(count.item())                       # the one host synchronisation
-    rows = gather_activate(scene, index, count, campos, cap=n)
+    """Gather + activate the selected rows, drop the invalid ones as FilterGS.render does, and rasterize
+    them (forward only, colours precomputed)."""
+    n = int(count.item())                       # the host synchronisation for the row count
+    rows = drop_invalid_rows(gather_activate(scene, index, count, campos, cap=n))
     e = torch.empty(0, device=scene.xyz.device)
     return _C.rasterize_gaussians(bg, rows["xyz"], rows["colors"], rows["opacity"], rows["scaling"],
                                   rows["rotation"], 1.0, e, view, proj, cam.tanfovx, cam.tanfovy, cam.H, cam.W, e, 0,

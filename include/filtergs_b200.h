@@ -255,6 +255,11 @@ int fgs_gather_activate(long long N_cap, const int64_t *index, const unsigned lo
                         const float *features_dc, const float *shs_rest, int sh_degree, int rest_coeffs,
                         const float *campos, float *o_xyz, float *o_scaling, float *o_rotation, float *o_opacity,
                         float *o_colors, void *stream);
+/* FilterGS.render's guard (FilterGS/filtergs.py:159-172): keep[n] = 1 for the rows whose xyz,
+ * scaling, rotation, opacity and colour (the activated rows of fgs_gather_activate) are all
+ * finite, with min(scaling) > 0 and opacity > 0; *dropped (device, u64) counts the others.  */
+int fgs_rows_valid(long long N, const float *xyz, const float *scaling, const float *rotation, const float *opacity,
+                   const float *colors, uint8_t *keep, unsigned long long *dropped, void *stream);
 /* The LoG node radius (LoG/model/level_of_gaussian.py:66-88 -> compute_radius_kernel_v2.cu:180-229)
  * from raw parameters: exp(log_scales) and the normalised quaternion are applied in the kernel.        */
 int fgs_radius_raw(int P, const float *means3D, const float *log_scales, const float *rotations,

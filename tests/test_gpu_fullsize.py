@@ -7,11 +7,12 @@ through properties that do not depend on size.
   cameras (the preprocess writes out the reference build's multiply-add grouping, and the
   compositing arithmetic is the reference's);
 * the reference build, backward (ref_compat): the screen-space, colour, opacity, mean and SH
-  gradients within 1e-4 norm-relative; the covariance, scale and rotation gradients -- sums
-  of many cancelling per-pixel terms, which the reference adds with float atomics in
-  arbitrary order -- within 1e-4 or twice the reference's own run-to-run difference on the
-  same inputs, whichever is larger; a 2-view batched step's summed gradients against the sum
-  of the reference's per-view gradients the same way;
+  gradients within 1e-4 norm-relative of the reference; the covariance, scale and rotation
+  gradients are sums of many cancelling per-pixel terms that the reference adds with float
+  atomics in arbitrary order, so its own runs differ by more than 1e-4 -- they are held to
+  the mean of three reference runs within 1e-4 or three times the largest distance of a
+  reference run from that mean, whichever is larger; a 2-view batched step's summed
+  gradients against the sum of the reference's per-view gradients the same way;
 * binning: num_rendered equals the sum of tiles touched; the sorted keys are non-decreasing
   (tile, then depth bits); the tile ranges partition [0, K) in tile order; n_contrib never
   exceeds its tile's range;
@@ -150,14 +151,14 @@ def test_fullsize_batched_equals_plain(cuda, full):
         assert torch.equal(br.grad[k], sums[k]), k
 
 
-def _grad_check(name, mine, ref1, ref2):
-    """mine vs the reference within GRAD_TOL, or (ill-conditioned sums) within twice the
-    reference's own run-to-run difference ref2 vs ref1."""
-    d = norm_rel(mine, ref1)
+def _grad_check(name, mine, refs):
+    """mine against the mean of the reference runs `refs`: within GRAD_TOL, or (ill-conditioned
+    sums) within three times the largest distance of a reference run from that mean."""
+    m = sum(r.double() for r in refs) / len(refs)
+    d = norm_rel(mine, m)
+    tol = GRAD_TOL
     if name in ILL_CONDITIONED:
-        tol = max(GRAD_TOL, 2.0 * norm_rel(ref2, ref1))
-    else:
-        tol = GRAD_TOL
+        tol = max(GRAD_TOL, 3.0 * max(norm_rel(r, m) for r in refs))
     assert d <= tol, (name, d, tol)
     return d
 
@@ -169,11 +170,12 @@ def test_fullsize_gradients_vs_reference(cuda, ref, full):
         dL = torch.randn(3, c.H, c.W, device="cuda", generator=g)
         mine = _bwd(scene, c, _fwd(ours, scene, c), dL)
         rf = _fwd(ref, scene, c)
-        r1, r2 = _bwd(scene, c, rf, dL, ref), _bwd(scene, c, rf, dL, ref)
+        runs = [_bwd(scene, c, rf, dL, ref) for _ in range(3)]
         torch.cuda.synchronize()
-        for n, a, b1, b2 in zip(GRAD_NAMES, mine, r1, r2):
-            assert a.shape == b1.shape, n
-            _grad_check(n, a, b1, b2)
+        for j, n in enumerate(GRAD_NAMES):
+            assert mine[j].shape == runs[0][j].shape, n
+            _grad_check(n, mine[j], [r[j] for r in runs])
+        del runs
 
 
 def test_fullsize_batched_gradients_vs_reference(cuda, ref, full):
@@ -191,14 +193,13 @@ def test_fullsize_batched_gradients_vs_reference(cuda, ref, full):
     br.step()
     br.check()
     keys = {"means3D": 3, "opacity": 2, "sh": 5, "scales": 6, "rotations": 7}
-    s1 = {k: torch.zeros_like(v) for k, v in br.grad.items()}
-    s2 = {k: torch.zeros_like(v) for k, v in br.grad.items()}
+    sums = [{k: torch.zeros_like(v) for k, v in br.grad.items()} for _ in range(3)]
     for c, d in zip(cams, dls):
         rf = _fwd(ref, scene, c)
-        r1, r2 = _bwd(scene, c, rf, d, ref), _bwd(scene, c, rf, d, ref)
-        for k, j in keys.items():
-            s1[k] += r1[j].reshape(s1[k].shape)
-            s2[k] += r2[j].reshape(s2[k].shape)
+        for s in sums:
+            r = _bwd(scene, c, rf, d, ref)
+            for k, j in keys.items():
+                s[k] += r[j].reshape(s[k].shape)
     torch.cuda.synchronize()
     for k in keys:
-        _grad_check(k, br.grad[k], s1[k], s2[k])
+        _grad_check(k, br.grad[k], [s[k] for s in sums])

@@ -124,10 +124,17 @@ def test_gather_activate_vs_oracle(cuda):
         np.testing.assert_allclose(rows[k][:6000].cpu().numpy(), o[ok], rtol=2e-6, atol=2e-6)
 
 
-def test_filtergs_selected_render_vs_reference_pipeline(cuda, v2, ref):
-    """The device path (mask -> compaction -> fused gather/activation -> rasterizer) against the
-    reference's own pieces (its visibility kernel, torch.nonzero, torch activations, its rasterizer)."""
+@pytest.mark.parametrize("degenerate", [False, True])
+def test_filtergs_selected_render_vs_reference_pipeline(cuda, v2, ref, degenerate):
+    """The device path (mask -> compaction -> fused gather/activation -> row guard -> rasterizer)
+    against the reference's own pieces (its visibility kernel, torch.nonzero, torch activations,
+    FilterGS.render's finite/positive guard, its rasterizer).  `degenerate` gives some nodes an
+    opacity whose sigmoid is 0 and a scale whose exp is 0, which the guard drops."""
     tr, cam = _tree(P=40000, seed=3105)
+    if degenerate:
+        tr = dict(tr, opacity_raw=tr["opacity_raw"].copy(), log_scales=tr["log_scales"].copy())
+        tr["opacity_raw"].reshape(-1)[::37] = -1000.0
+        tr["log_scales"][5::41, 1] = -300.0
     scene = lod.TreeScene.from_arrays(tr)
     view, proj, cpos = _t(cam.viewmatrix), _t(cam.projmatrix), _t(cam.campos)
     bg = torch.zeros(3, device="cuda")
@@ -146,19 +153,25 @@ def test_filtergs_selected_render_vs_reference_pipeline(cuda, v2, ref):
     C0, C1 = 0.28209479177387814, 0.4886025119029199
     col = scene.features_dc[ri] * C0 + 0.5 + (-C1 * d[:, 1:2] * rest[:, 0] + C1 * d[:, 2:3] * rest[:, 1] -
                                               C1 * d[:, 0:1] * rest[:, 2])
-    e = torch.Tensor([])
-    theirs = ref.rasterize_gaussians(bg, xyz, col, torch.sigmoid(scene.opacity_raw[ri])[:, None],
-                                     torch.exp(scene.log_scales[ri]),
-                                     torch.nn.functional.normalize(scene.rotations[ri]), 1.0, e, view, proj,
-                                     cam.tanfovx, cam.tanfovy, cam.H, cam.W, e, 0, cpos, False, True, False, 0.2, 0.2,
-                                     0.05, 0.7, False)
+    sc = torch.exp(scene.log_scales[ri])
+    rot = torch.nn.functional.normalize(scene.rotations[ri])
+    op = torch.sigmoid(scene.opacity_raw[ri])[:, None]
     # the fused gather + activation reproduces torch's op-by-op rounding (the norm's
     # summation order included), so the rasterizer sees the reference pipeline's bits
     rows = lod.gather_activate(scene, idx, cnt, cpos, cap=int(cnt.item()))
-    assert torch.equal(rows["rotation"], torch.nn.functional.normalize(scene.rotations[ri]))
-    assert torch.equal(rows["scaling"], torch.exp(scene.log_scales[ri]))
-    assert torch.equal(rows["opacity"].reshape(-1), torch.sigmoid(scene.opacity_raw[ri]))
+    assert torch.equal(rows["rotation"], rot)
+    assert torch.equal(rows["scaling"], sc)
+    assert torch.equal(rows["opacity"], op)
     assert torch.equal(rows["colors"], col)
+    # FilterGS.render (FilterGS/filtergs.py:159-172)
+    ok = (torch.isfinite(xyz).all(-1) & torch.isfinite(sc).all(-1) & torch.isfinite(rot).all(-1) &
+          torch.isfinite(op).all(-1) & torch.isfinite(col).all(-1))
+    ok = ok & (sc.min(dim=-1).values > 0.0) & (op[:, 0] > 0.0)
+    assert bool(ok.all()) != degenerate
+    xyz, col, op, sc, rot = xyz[ok], col[ok], op[ok], sc[ok], rot[ok]
+    e = torch.Tensor([])
+    theirs = ref.rasterize_gaussians(bg, xyz, col, op, sc, rot, 1.0, e, view, proj, cam.tanfovx, cam.tanfovy, cam.H,
+                                     cam.W, e, 0, cpos, False, True, False, 0.2, 0.2, 0.05, 0.7, False)
     assert mine[0] == theirs[0], "num_rendered"
     assert torch.equal(mine[5], theirs[5]), "radii"
     assert torch.equal(mine[2], theirs[2]), "point_id"
