@@ -6,7 +6,10 @@
  * A plain-C restatement of the reference algorithm, compiled twice: once with
  * REAL=float (the FP32 oracle, same expression order as the reference CUDA) and
  * once with REAL=double (the FP64 evaluation of the same splat equations used
- * for the finite-difference check and the FP32-vs-FP64 error report).
+ * for the finite-difference check and the FP32-vs-FP64 error report).  In the
+ * forward preprocess (cov3D, the view transform, the EWA projection, det, SH
+ * colour) the FP32 build also fuses the products the reference build fuses
+ * (FMA below), so those outputs equal that build's bit for bit.
  *
  * Reference anchors (paths inside the reference project):
  *   preprocess + OGFS radius ..... antialias/cuda_rasterizer/forward.cu:266-401
@@ -47,6 +50,7 @@
 #define FMAXR(a, b) fmax(a, b)
 #define FMINR(a, b) fmin(a, b)
 #define LIT(x) ((double)(x))
+#define FMA(a, b, c) fma(a, b, c)
 #else
 #define SFX(name) name##_f32
 #define EXPR(x) expf(x)
@@ -57,6 +61,7 @@
 #define FMAXR(a, b) fmaxf(a, b)
 #define FMINR(a, b) fminf(a, b)
 #define LIT(x) ((float)(x))
+#define FMA(a, b, c) fmaf(a, b, c)
 #endif
 
 #define BLOCK_X 16
@@ -133,6 +138,77 @@ static void cov3d_from(const real *s, real mod, const real *q, real *cov)
     cov[3] = Sig.m[1][1]; cov[4] = Sig.m[1][2]; cov[5] = Sig.m[2][2];
 }
 
+/* The forward preprocess's covariance chain and view transform with the
+ * multiply-add grouping of the reference build (nvcc fuses a product into the
+ * add that consumes it; which one was found by comparing candidate groupings
+ * with the reference build's cov3D, conic and colour bits on three 1080p views
+ * of a 2M-Gaussian scene).  dot3r: ((a0 b0 + a1 b1) + a2 b2) with the first and
+ * last products fused. */
+static inline real dot3r(real a0, real b0, real a1, real b1, real a2, real b2)
+{
+    return FMA(a2, b2, FMA(a0, b0, a1 * b1));
+}
+static inline void xform4x3_ref(const real *p, const real *m, real *o)
+{
+    for (int r = 0; r < 3; r++) o[r] = dot3r(m[r], p[0], m[4 + r], p[1], m[8 + r], p[2]) + m[12 + r];
+}
+static inline void xform4x4_ref(const real *p, const real *m, real *o)
+{
+    for (int r = 0; r < 4; r++) o[r] = dot3r(m[r], p[0], m[4 + r], p[1], m[8 + r], p[2]) + m[12 + r];
+}
+
+/* forward.cu:151-185 in the reference build's grouping: y y + z z unfused, the
+ * entries that share x z fuse r y, the others fuse their first product. */
+static void cov3d_ref(const real *s, real mod, const real *q, real *cov)
+{
+    const real r = q[0], x = q[1], y = q[2], z = q[3];
+    real R[3][3];
+    R[0][0] = 1 - 2 * (y * y + z * z);
+    R[0][1] = 2 * FMA(x, y, -(r * z));
+    R[0][2] = 2 * FMA(r, y, x * z);
+    R[1][0] = 2 * FMA(x, y, r * z);
+    R[1][1] = 1 - 2 * FMA(x, x, z * z);
+    R[1][2] = 2 * FMA(y, z, -(r * x));
+    R[2][0] = 2 * FMA(-r, y, x * z);
+    R[2][1] = 2 * FMA(y, z, r * x);
+    R[2][2] = 1 - 2 * FMA(x, x, y * y);
+    const real sc[3] = {mod * s[0], mod * s[1], mod * s[2]};
+    real M[3][3];
+    for (int c = 0; c < 3; c++)
+        for (int k = 0; k < 3; k++) M[c][k] = sc[k] * R[c][k];
+#define SIG(c, k) dot3r(M[k][0], M[c][0], M[k][1], M[c][1], M[k][2], M[c][2])
+    cov[0] = SIG(0, 0); cov[1] = SIG(0, 1); cov[2] = SIG(0, 2);
+    cov[3] = SIG(1, 1); cov[4] = SIG(1, 2); cov[5] = SIG(2, 2);
+#undef SIG
+}
+
+/* forward.cu:102-146 in the reference build's grouping (every dot fuses its
+ * first and last product; W J fuses its J[2] term). */
+static void ewa_ref(const real *mean, real fx, real fy, real tanx, real tany, const real *cov3D, const real *v,
+                    real *c00, real *c01, real *c11)
+{
+    real t[3];
+    xform4x3_ref(mean, v, t);
+    const real limx = LIT(1.3) * tanx, limy = LIT(1.3) * tany;
+    t[0] = rmin(limx, rmax(-limx, t[0] / t[2])) * t[2];
+    t[1] = rmin(limy, rmax(-limy, t[1] / t[2])) * t[2];
+    const real tz2 = t[2] * t[2];
+    const real j00 = fx / t[2], j02 = -(fx * t[0]) / tz2, j11 = fy / t[2], j12 = -(fy * t[1]) / tz2;
+    real T[2][3];
+    for (int k = 0; k < 3; k++) {
+        T[0][k] = FMA(v[4 * k + 2], j02, v[4 * k] * j00);
+        T[1][k] = FMA(v[4 * k + 2], j12, v[4 * k + 1] * j11);
+    }
+    const real V[3][3] = {{cov3D[0], cov3D[1], cov3D[2]}, {cov3D[1], cov3D[3], cov3D[4]},
+                          {cov3D[2], cov3D[4], cov3D[5]}};
+    real X[3][2];
+    for (int c = 0; c < 3; c++)
+        for (int k = 0; k < 2; k++) X[c][k] = dot3r(T[k][0], V[0][c], T[k][1], V[1][c], T[k][2], V[2][c]);
+#define CV(c, k) dot3r(X[0][k], T[c][0], X[1][k], T[c][1], X[2][k], T[c][2])
+    *c00 = CV(0, 0); *c01 = CV(0, 1); *c11 = CV(1, 1);
+#undef CV
+}
+
 /* EWA projection shared by forward, backward and the radius kernels
  * (forward.cu:102-146, backward.cu:166-194).  Fills T (= W*J) and the
  * clamp flags; returns the un-dilated 2D covariance. */
@@ -186,32 +262,38 @@ static const double SH_C3[7] = {-0.5900435899266435, 2.890611442640554, -0.45704
                                 -0.5900435899266435};
 
 /* forward.cu:48-99 */
+/* forward.cu:48-99 in the reference build's grouping: |dir|^2 like dot3r,
+ * C0 sh0 - C1 y sh1 fuses C1 y sh1, each later term fuses its final product with
+ * the coefficient into the running sum, 3 xx - yy, xx - 3 yy and
+ * (2 zz - 3 xx) - 3 yy fuse the product by 3. */
 static void sh_to_rgb(int deg, int M, const real *pos, const real *campos, const real *sh_all, int idx,
                       real *rgb, uint8_t *clamped)
 {
     const real c0 = (real)SH_C0, c1 = (real)SH_C1;
     real dir[3] = {pos[0] - campos[0], pos[1] - campos[1], pos[2] - campos[2]};
-    real len = SQRTR(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+    real len = SQRTR(dot3r(dir[0], dir[0], dir[1], dir[1], dir[2], dir[2]));
     dir[0] = dir[0] / len; dir[1] = dir[1] / len; dir[2] = dir[2] / len;
     const real *sh = sh_all + (size_t)idx * M * 3;
     real x = dir[0], y = dir[1], z = dir[2];
+    real xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+    real f[5] = {(real)SH_C2[0] * xy, (real)SH_C2[1] * yz, (real)SH_C2[2] * (LIT(2.0) * zz - xx - yy),
+                 (real)SH_C2[3] * xz, (real)SH_C2[4] * (xx - yy)};
+    real q4 = LIT(4.0) * zz - xx - yy;
+    real g[7] = {(real)SH_C3[0] * y * FMA(LIT(3.0), xx, -yy), (real)SH_C3[1] * xy * z, (real)SH_C3[2] * y * q4,
+                 (real)SH_C3[3] * z * FMA(LIT(-3.0), yy, FMA(LIT(-3.0), xx, LIT(2.0) * zz)),
+                 (real)SH_C3[4] * x * q4, (real)SH_C3[5] * z * (xx - yy),
+                 (real)SH_C3[6] * x * FMA(LIT(-3.0), yy, xx)};
     for (int ch = 0; ch < 3; ch++) {
 #define S(k) sh[(k) * 3 + ch]
         real res = c0 * S(0);
         if (deg > 0) {
-            res = res - c1 * y * S(1) + c1 * z * S(2) - c1 * x * S(3);
+            res = FMA(-(c1 * y), S(1), res);
+            res = FMA(c1 * z, S(2), res);
+            res = FMA(-(c1 * x), S(3), res);
             if (deg > 1) {
-                real xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
-                res = res + (real)SH_C2[0] * xy * S(4) + (real)SH_C2[1] * yz * S(5) +
-                      (real)SH_C2[2] * (LIT(2.0) * zz - xx - yy) * S(6) + (real)SH_C2[3] * xz * S(7) +
-                      (real)SH_C2[4] * (xx - yy) * S(8);
-                if (deg > 2) {
-                    res = res + (real)SH_C3[0] * y * (LIT(3.0) * xx - yy) * S(9) + (real)SH_C3[1] * xy * z * S(10) +
-                          (real)SH_C3[2] * y * (LIT(4.0) * zz - xx - yy) * S(11) +
-                          (real)SH_C3[3] * z * (LIT(2.0) * zz - LIT(3.0) * xx - LIT(3.0) * yy) * S(12) +
-                          (real)SH_C3[4] * x * (LIT(4.0) * zz - xx - yy) * S(13) +
-                          (real)SH_C3[5] * z * (xx - yy) * S(14) + (real)SH_C3[6] * x * (xx - LIT(3.0) * yy) * S(15);
-                }
+                for (int i = 0; i < 5; i++) res = FMA(f[i], S(4 + i), res);
+                if (deg > 2)
+                    for (int i = 0; i < 7; i++) res = FMA(g[i], S(9 + i), res);
             }
         }
 #undef S
@@ -254,25 +336,24 @@ void SFX(orc_preprocess)(const SFX(orc_pre_args) * a, int *radii, real *means2D,
         conic_o[4 * i] = conic_o[4 * i + 1] = conic_o[4 * i + 2] = conic_o[4 * i + 3] = 0;
         const real *p = a->means + 3 * (size_t)i;
         real ph[4], pv[3];
-        xform4x4(p, a->proj, ph);
+        xform4x4_ref(p, a->proj, ph);
         real pw = LIT(1.0) / (ph[3] + LIT(0.0000001));
         real pp[3] = {ph[0] * pw, ph[1] * pw, ph[2] * pw};
-        xform4x3(p, a->view, pv);
+        xform4x3_ref(p, a->view, pv);
         if (pv[2] <= LIT(0.2)) continue; /* auxiliary.h:154 */
         real cov[6];
         if (a->cov3D_precomp) memcpy(cov, a->cov3D_precomp + 6 * (size_t)i, sizeof(cov));
-        else cov3d_from(a->scales + 3 * (size_t)i, a->scale_mod, a->rots + 4 * (size_t)i, cov);
+        else cov3d_ref(a->scales + 3 * (size_t)i, a->scale_mod, a->rots + 4 * (size_t)i, cov);
         if (a->filter3d > 0) {
             real sf = a->filter3d * pv[2] / fx;
             real v = sf * sf;
             cov[0] += v; cov[3] += v; cov[5] += v;
         }
         if (cov3D_out) memcpy(cov3D_out + 6 * (size_t)i, cov, sizeof(cov));
-        ewa_t e;
         real c00, c01, c11;
-        ewa(p, fx, fy, a->tanx, a->tany, cov, a->view, &e, &c00, &c01, &c11);
+        ewa_ref(p, fx, fy, a->tanx, a->tany, cov, a->view, &c00, &c01, &c11);
         if (a->use_filter) { c00 = dil_max(c00); c11 = dil_max(c11); }
-        real det = c00 * c11 - c01 * c01;
+        real det = FMA(c00, c11, -(c01 * c01));
         if (det == LIT(0.0)) continue;
         real dinv = LIT(1.0) / det;
         real con[3] = {c11 * dinv, -c01 * dinv, c00 * dinv};

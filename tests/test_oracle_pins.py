@@ -5,9 +5,10 @@ torchref_*.npz  -- the reference's own Python/torch code run on the CPU
 ref_*.npz       -- the reference's own CUDA build run on a B200
                    (tests/golden/make_golden_ref.py)
 
-Integer outputs are compared exactly; float outputs with the tolerance a CPU
-float32 evaluation without FMA contraction can meet against the GPU build
-(which contracts multiply-adds)."""
+Integer outputs are compared exactly.  The forward preprocess of the oracle evaluates the
+reference build's multiply-add grouping (fused where nvcc fused), so its per-Gaussian
+floats match that build bit for bit; the rest of the oracle (radius, LoD, backward) keeps
+plain float32 evaluation and is compared with a tolerance."""
 import glob
 import os
 
@@ -17,6 +18,10 @@ import pytest
 from _helpers import O, S
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.int32)
 
 
 def _load(name):
@@ -96,20 +101,20 @@ def test_oracle_forward_vs_reference_build(name):
     sc = _scene(d)
     f = O.forward(sc)
     vis = d["radii"] > 0
-    # integer outputs: allow at most a handful of float-rounding flips at exact thresholds
-    assert np.mean(f["pre"]["radii"] != d["radii"]) <= 2e-3
-    if np.array_equal(f["pre"]["radii"], d["radii"]):
-        assert f["num_rendered"] == int(d["num_rendered"])
-    np.testing.assert_allclose(f["pre"]["means2D"][vis], d["ref_means2D"][vis], rtol=1e-5, atol=1e-4)
-    np.testing.assert_allclose(f["pre"]["depths"][vis], d["ref_depths"][vis], rtol=1e-6)
-    np.testing.assert_allclose(f["pre"]["conic_opacity"][vis], d["ref_conic_opacity"][vis], rtol=1e-4, atol=1e-6)
-    if np.array_equal(f["pre"]["radii"], d["radii"]):
-        assert np.array_equal(f["keys"].view(np.int64), d["ref_keys"]) or \
-            np.array_equal(f["vals"].astype(np.int32), d["ref_vals"])
-        assert np.array_equal(f["ranges"].astype(np.int32), d["ref_ranges"])
-        assert np.mean(f["n_contrib"].astype(np.int32) != d["ref_n_contrib"]) <= 1e-3
-    np.testing.assert_allclose(f["color"], d["color"], atol=1e-4)
-    assert np.mean(np.abs(f["color"] - d["color"]) > 1e-5) <= 1e-2
+    # The preprocess follows the reference build's multiply-add grouping, so every per-Gaussian
+    # output is bit-identical; the binning and the per-pixel contributor counts follow from it.
+    assert np.array_equal(f["pre"]["radii"], d["radii"])
+    assert f["num_rendered"] == int(d["num_rendered"])
+    for k in ("means2D", "depths", "conic_opacity"):
+        assert np.array_equal(_bits(f["pre"][k][vis]), _bits(d["ref_" + k][vis])), k
+    if d["colors"].size == 0:
+        assert np.array_equal(_bits(f["pre"]["rgb"][vis]), _bits(d["ref_rgb"][vis]))
+    assert np.array_equal(f["keys"].view(np.int64), d["ref_keys"]) or \
+        np.array_equal(f["vals"].astype(np.int32), d["ref_vals"])
+    assert np.array_equal(f["ranges"].astype(np.int32), d["ref_ranges"])
+    assert np.array_equal(f["n_contrib"].astype(np.int32), d["ref_n_contrib"])
+    # the host libm exp differs from the device exp in the last bit, which the blend carries
+    np.testing.assert_allclose(f["color"], d["color"], rtol=0, atol=1e-6)
 
 
 @pytest.mark.parametrize("name", ["ref_sh3_filter.npz", "ref_colors_nofilter_ragged.npz", "ref_sh1_dense.npz"])
