@@ -7,12 +7,13 @@ through properties that do not depend on size.
   cameras (the preprocess writes out the reference build's multiply-add grouping, and the
   compositing arithmetic is the reference's);
 * the reference build, backward (ref_compat): the screen-space, colour, opacity, mean and SH
-  gradients within 1e-4 norm-relative of the reference; the covariance, scale and rotation
-  gradients are sums of many cancelling per-pixel terms that the reference adds with float
-  atomics in arbitrary order, so its own runs differ by more than 1e-4 -- they are held to
-  the mean of three reference runs within 1e-4 or three times the largest distance of a
-  reference run from that mean, whichever is larger; a 2-view batched step's summed
-  gradients against the sum of the reference's per-view gradients the same way;
+  gradients within 1e-4 norm-relative of the mean of three reference runs.  The covariance,
+  scale and rotation gradients are sums of many cancelling per-pixel terms that the
+  reference adds with float atomics in arbitrary order (its own runs differ by 4e-4 to 9e-4
+  norm-relative), so they are held to accuracy instead: against an FP64 evaluation of the
+  same equations (the CPU oracle in FP64) they must be no further than 1.05 times the mean
+  distance of the reference's runs from it.  A 2-view batched step's summed gradients are
+  checked against the sums of the per-view gradients the same way;
 * binning: num_rendered equals the sum of tiles touched; the sorted keys are non-decreasing
   (tile, then depth bits); the tile ranges partition [0, K) in tile order; n_contrib never
   exceeds its tile's range;
@@ -35,11 +36,20 @@ ILL_CONDITIONED = ("cov3D", "scales", "rotations")
 
 
 @pytest.fixture(scope="module")
-def full():
+def _scene_pair():
     import bench
-    sc, scene = bench.make_scene(2_000_000, torch.device("cuda"))
-    cams = bench.rank_cameras(2, 0)
-    return scene, cams
+    return bench.make_scene(2_000_000, torch.device("cuda"))
+
+
+@pytest.fixture(scope="module")
+def full(_scene_pair):
+    import bench
+    return _scene_pair[1], bench.rank_cameras(2, 0)
+
+
+@pytest.fixture(scope="module")
+def full_np(_scene_pair):
+    return _scene_pair[0]
 
 
 def _t(a):
@@ -151,19 +161,41 @@ def test_fullsize_batched_equals_plain(cuda, full):
         assert torch.equal(br.grad[k], sums[k]), k
 
 
-def _grad_check(name, mine, refs):
-    """mine against the mean of the reference runs `refs`: within GRAD_TOL, or (ill-conditioned
-    sums) within three times the largest distance of a reference run from that mean."""
+def _fp64_grads(scene_np, c, dL):
+    """The reference's splat math in FP64 (CPU oracle, ref_compat backward) for one view."""
+    from oracle import oracle as O
+    import os
+    O.set_threads(os.cpu_count() or 1)
+    f64 = lambda a: np.asarray(a, np.float64)  # noqa: E731
+    s64 = O.Scene(f64(scene_np["means3D"]), f64(scene_np["opacities"]), c.W, c.H, c.tanfovx, c.tanfovy,
+                  f64(c.viewmatrix).reshape(-1), f64(c.projmatrix).reshape(-1), f64(c.campos), shs=f64(scene_np["shs"]),
+                  sh_degree=3, scales=f64(scene_np["scales"]), rotations=f64(scene_np["rotations"]))
+    of = O.forward(s64, dtype=np.float64)
+    return O.backward(s64, of, dL.cpu().numpy().astype(np.float64), dtype=np.float64)
+
+
+def _nr(a, b):
+    a = np.asarray(a, np.float64).reshape(-1)
+    b = np.asarray(b, np.float64).reshape(-1)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def _grad_check(name, mine, refs, exact=None):
+    """Well-conditioned gradients: mine within GRAD_TOL of the mean of the reference runs.
+    Ill-conditioned sums: mine no further from the FP64 evaluation `exact` than 1.05 times the
+    reference runs' mean distance from it."""
     m = sum(r.double() for r in refs) / len(refs)
-    d = norm_rel(mine, m)
-    tol = GRAD_TOL
     if name in ILL_CONDITIONED:
-        tol = max(GRAD_TOL, 3.0 * max(norm_rel(r, m) for r in refs))
-    assert d <= tol, (name, d, tol)
+        ours = _nr(mine.cpu(), exact)
+        theirs = float(np.mean([_nr(r.cpu(), exact) for r in refs]))
+        assert ours <= 1.05 * theirs, (name, ours, theirs)
+        return ours
+    d = norm_rel(mine, m)
+    assert d <= GRAD_TOL, (name, d, GRAD_TOL)
     return d
 
 
-def test_fullsize_gradients_vs_reference(cuda, ref, full):
+def test_fullsize_gradients_vs_reference(cuda, ref, full, full_np):
     scene, cams = full
     for i, c in enumerate(cams):
         g = torch.Generator(device="cuda").manual_seed(40 + i)
@@ -172,13 +204,14 @@ def test_fullsize_gradients_vs_reference(cuda, ref, full):
         rf = _fwd(ref, scene, c)
         runs = [_bwd(scene, c, rf, dL, ref) for _ in range(3)]
         torch.cuda.synchronize()
+        x = _fp64_grads(full_np, c, dL)
         for j, n in enumerate(GRAD_NAMES):
             assert mine[j].shape == runs[0][j].shape, n
-            _grad_check(n, mine[j], [r[j] for r in runs])
+            _grad_check(n, mine[j], [r[j] for r in runs], x.get(n))
         del runs
 
 
-def test_fullsize_batched_gradients_vs_reference(cuda, ref, full):
+def test_fullsize_batched_gradients_vs_reference(cuda, ref, full, full_np):
     """One 2-view batched step: the shared gradients against the sums of the reference's
     per-view gradients (means3D, opacity, SH, scales, rotations)."""
     from filtergs_b200.batched import BatchedRasterizer, Camera
@@ -194,12 +227,16 @@ def test_fullsize_batched_gradients_vs_reference(cuda, ref, full):
     br.check()
     keys = {"means3D": 3, "opacity": 2, "sh": 5, "scales": 6, "rotations": 7}
     sums = [{k: torch.zeros_like(v) for k, v in br.grad.items()} for _ in range(3)]
+    exact = {k: 0.0 for k in keys}
     for c, d in zip(cams, dls):
         rf = _fwd(ref, scene, c)
         for s in sums:
             r = _bwd(scene, c, rf, d, ref)
             for k, j in keys.items():
                 s[k] += r[j].reshape(s[k].shape)
+        x = _fp64_grads(full_np, c, d)
+        for k in keys:
+            exact[k] = exact[k] + np.asarray(x[k], np.float64).reshape(-1)
     torch.cuda.synchronize()
     for k in keys:
-        _grad_check(k, br.grad[k], [s[k] for s in sums])
+        _grad_check(k, br.grad[k], [s[k] for s in sums], exact[k])
