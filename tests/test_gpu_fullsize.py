@@ -11,9 +11,12 @@ through properties that do not depend on size.
   scale and rotation gradients are sums of many cancelling per-pixel terms that the
   reference adds with float atomics in arbitrary order (its own runs differ by 4e-4 to 9e-4
   norm-relative), so they are held to accuracy instead: against an FP64 evaluation of the
-  same equations (the CPU oracle in FP64) they must be no further than 1.05 times the mean
-  distance of the reference's runs from it.  A 2-view batched step's summed gradients are
-  checked against the sums of the per-view gradients the same way;
+  same equations (the CPU oracle in FP64) they must be no further than 1.25 times the mean
+  distance of three reference runs from it.  The reference's own runs scatter widely around
+  that mean (six runs of the 2-view batch: rotations 1.16e-3 to 1.52e-3), and a 3-run mean
+  moves by about 5%, so 1.25 keeps the check from failing on the reference's noise while a
+  wrong term (errors of 1e-2 and more) still fails it.  A 2-view batched step's summed
+  gradients are checked against the sums of the per-view gradients the same way;
 * binning: num_rendered equals the sum of tiles touched; the sorted keys are non-decreasing
   (tile, then depth bits); the tile ranges partition [0, K) in tile order; n_contrib never
   exceeds its tile's range;
@@ -33,6 +36,8 @@ GRAD_NAMES = ["means2D", "colors", "opacity", "means3D", "cov3D", "sh", "scales"
 # gradients that sum many cancelling per-pixel terms: the reference's own atomic summation
 # order moves them by more than 1e-4 from run to run
 ILL_CONDITIONED = ("cov3D", "scales", "rotations")
+# ours against FP64, relative to the mean distance of three reference runs from FP64
+ACCURACY_MARGIN = 1.25
 
 
 @pytest.fixture(scope="module")
@@ -182,13 +187,13 @@ def _nr(a, b):
 
 def _grad_check(name, mine, refs, exact=None):
     """Well-conditioned gradients: mine within GRAD_TOL of the mean of the reference runs.
-    Ill-conditioned sums: mine no further from the FP64 evaluation `exact` than 1.05 times the
+    Ill-conditioned sums: mine no further from the FP64 evaluation `exact` than 1.25 times the
     reference runs' mean distance from it."""
     m = sum(r.double() for r in refs) / len(refs)
     if name in ILL_CONDITIONED:
         ours = _nr(mine.cpu(), exact)
         theirs = float(np.mean([_nr(r.cpu(), exact) for r in refs]))
-        assert ours <= 1.05 * theirs, (name, ours, theirs)
+        assert ours <= ACCURACY_MARGIN * theirs, (name, ours, theirs)
         return ours
     d = norm_rel(mine, m)
     assert d <= GRAD_TOL, (name, d, GRAD_TOL)
