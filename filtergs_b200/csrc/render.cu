@@ -261,7 +261,7 @@ __device__ __forceinline__ void render_fwd_tile(FwdSmem<kBatch>& sm, const TileA
     const int px = bx * kTileX + lx;
     const uint2 range = a.ranges[tile];
     const uint32_t n = range.y - range.x;
-    if (split_min && n >= split_min) return;  // rendered in bands (render_fwd_band)
+    if (split_min && n >= split_min) return;  // rendered in bands (render_long_tile)
     const int nb = (int)((n + kBatch - 1) / kBatch);
     const bool stats = stats_smem && a.kv_sum != nullptr;  // the sums exist only in a launch that has them
     const PairRecord* recs = a.recs;
@@ -487,50 +487,88 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas<PPT>())
 // A tile with a long record list (dense small splats: distant LoD levels, a
 // horizon) is the critical path of the one-CTA-per-tile render: its few warps
 // walk every record while the rest of the GPU has finished.  Tiles with at
-// least split_min records are rendered instead as bands of BW x BH pixels, one
-// warp each and every warp on its own, longest tiles first.  The warp pulls the
-// tile's records through its own ring of kBandRing shared-memory chunks of 32
-// records (one bulk copy per chunk, completed on the slot's mbarrier, two chunks
-// in flight), culls each chunk against its band (one record per lane, then a
-// ballot), and composites the touched records with the tile path's per-pixel
-// functions, one pixel per lane (lanes past BW x BH only cull).  A long tile so
-// spreads over 256 / (BW BH) warps on different SMs, each culling against a
-// small rectangle, and each warp evaluates the alphas of two touched records
-// before it accumulates them, so that the exp of one overlaps the other's
-// arithmetic.  Every pixel composites the same records in the same order with
-// the same arithmetic as on the tile path.  Per record, a contributing lane
-// folds its weight into the record's shared slot; the slots leave once per chunk
-// (atomicMax into the per-Gaussian max weight, atomicAdd into the statistics,
-// which are zeroed before the launch when on).
+// least split_min records are rendered instead in bands of BW x BH pixels, one
+// warp per band and four bands per CTA (a tile's 256 / (BW BH) bands spread over
+// several SMs), longest tiles first.  The CTA stages the tile's records in
+// chunks of one record per thread (plain coalesced loads; the next chunk is
+// loaded into registers while the current one is composited), and each thread
+// works out which bands its record can reach (band_mask), so a record is tested
+// once per four bands instead of once per band, and a warp finds its band's
+// records with one ballot per 32.  The
+// warp composites them with the tile path's per-pixel functions; a band of
+// fewer than 32 pixels evaluates several records per step (lane = slot * pixels
+// + pixel) and the pixel's owner lane composites them in order.  Every pixel
+// composites the same records in the same order with the same arithmetic as on
+// the tile path.  Per record, a contributing lane folds its weight into the
+// record's shared slot; the slots leave once per chunk (atomicMax into the
+// per-Gaussian max weight, atomicAdd into the statistics, which are zeroed
+// before the launch when on).
 //
 // Order: long tiles are binned by floor(log2(records)) (kLongBuckets bins of
-// capacity `cap` each); the band queue hands out the bins from the longest down.
-constexpr int kBandWarps = 8;  // warps per CTA of the band kernel
-constexpr int kBandRing = 3;   // chunks per warp: one being composited, two in flight
+// capacity `cap` each); the queue hands out the bins from the longest down.
 constexpr int kLongBuckets = 32;
 
-struct BandSmem {
-    PairRecord rec[kBandRing][32];
-    uint64_t bar[kBandRing];
-    uint32_t wmax[32];  // per record of the current chunk: max weight over this band's pixels
-    float ksum[32];     // statistics: weight sum and count over this band's pixels
-    uint32_t kcnt[32];
+template <int BW, int BH>
+struct LongTile {
+    static_assert(BW * BH <= 32 && kTileX % BW == 0 && kTileY % BH == 0, "band shape");
+    static constexpr int kPix = BW * BH;                   // pixels per band
+    static constexpr int kPerRow = kTileX / BW;            // bands per row of the tile
+    static constexpr int kRows = kTileY / BH;
+    static constexpr int kBands = kPerRow * kRows;         // bands per tile
+    static constexpr int kGroup = kBands < 4 ? kBands : 4; // bands (warps) per CTA
+    static constexpr int kGroups = kBands / kGroup;        // CTAs per tile
+    static constexpr int kThreads = 32 * kGroup;           // also the records staged per chunk
+    static constexpr int kSlots = 32 / kPix;               // records evaluated per step
 };
 
-__device__ __forceinline__ void band_smem_init(BandSmem& sm)
+template <int kChunk>
+struct LongSmem {
+    PairRecord rec[kChunk];
+    uint32_t mask[kChunk];  // bands each record can reach
+    uint32_t wmax[kChunk];  // per record: max weight over the tile's pixels
+    float ksum[kChunk];     // statistics: weight sum and count over the tile's pixels
+    uint32_t kcnt[kChunk];
+};
+
+// The bands of the tile at (tx0, ty0) that a record can reach.  The record
+// reaches alpha >= 1/255 only inside the ellipse Q(d) = a dx^2 + 2 b dx dy +
+// c dy^2 <= 2 ln(255 o); the test uses the axis-aligned box around Q(d) <= t,
+// t = 1.01 * 2 ln(255 o) + 0.1, whose half-widths are sqrt(t c / det) and
+// sqrt(t a / det) (det = a c - b^2), grown by 0.01 px.  With det >= 0.01 a c the
+// per-pixel float evaluation of Q errs by under 5e-7 of a dx^2 + c dy^2 +
+// 2|b dx dy|, which is at most 400 Q there, far inside the 1% margin; the fast
+// log and divide err by less than the 0.1 absolute margin.  So a pixel outside
+// the box gets alpha < 1/255 and is skipped by the per-pixel test anyway.  Band
+// k of a row covers the pixel columns tx0 + k BW .. tx0 + k BW + BW - 1, so the
+// box reaches it when mx - ex <= tx0 + k BW + BW - 1 and mx + ex >= tx0 + k BW
+// (rows alike).  0 when the record cannot reach alpha >= 1/255 in the tile;
+// every band for a conic the box does not cover (near-degenerate, not positive
+// definite, not finite) and for a mean that is not finite.
+template <int BW, int BH>
+__device__ __forceinline__ uint32_t band_mask(const float4 ea, const float4 eb, float tx0, float ty0)
 {
-    const int lane = threadIdx.x & 31;
-    sm.wmax[lane] = 0;
-    sm.ksum[lane] = 0.f;
-    sm.kcnt[lane] = 0;
-    if (lane == 0) {
-        for (int i = 0; i < kBandRing; i++) mbar_init(&sm.bar[i], 1);
-        mbar_fence_init();
-    }
-    __syncwarp();
+    using L = LongTile<BW, BH>;
+    constexpr uint32_t kAll = L::kBands == 32 ? 0xffffffffu : ((1u << L::kBands) - 1u);
+    const float mx = ea.x, my = ea.y, a = ea.z, b = ea.w, c = eb.x, o = eb.y;
+    if (!(o >= 1.0f / 255.0f)) return 0u;
+    const float det = a * c - b * b;
+    if (!(a > 0.f && c > 0.f && det >= 0.01f * a * c) || !isfinite(mx) || !isfinite(my)) return kAll;
+    const float t = 1.01f * (2.f * __logf(255.f * o)) + 0.1f;
+    const float s = __fdividef(t, det);
+    const float ex = sqrtf(s * c) + 0.01f, ey = sqrtf(s * a) + 0.01f;
+    const float lo_x = (mx - ex - tx0 - (BW - 1)) * (1.f / BW), hi_x = (mx + ex - tx0) * (1.f / BW);
+    const float lo_y = (my - ey - ty0 - (BH - 1)) * (1.f / BH), hi_y = (my + ey - ty0) * (1.f / BH);
+    const int c0 = (int)ceilf(fmaxf(lo_x, 0.f)), c1 = (int)floorf(fminf(hi_x, (float)(L::kPerRow - 1)));
+    const int r0 = (int)ceilf(fmaxf(lo_y, 0.f)), r1 = (int)floorf(fminf(hi_y, (float)(L::kRows - 1)));
+    if (c0 > c1 || r0 > r1) return 0u;
+    const uint32_t cols = ((2u << (c1 - c0)) - 1u) << c0;
+    uint32_t m = 0u;
+    for (int r = r0; r <= r1; r++) m |= cols << (r * L::kPerRow);
+    return m;
 }
 
-__device__ __forceinline__ void band_fold(BandSmem& sm, uint32_t j, float w, bool stats)
+template <int kChunk>
+__device__ __forceinline__ void long_fold(LongSmem<kChunk>& sm, uint32_t j, float w, bool stats)
 {
     if (w > 0.f) {
         atomicMax(&sm.wmax[j], __float_as_uint(w));
@@ -541,98 +579,105 @@ __device__ __forceinline__ void band_fold(BandSmem& sm, uint32_t j, float w, boo
     }
 }
 
-// `g` counts the chunks this warp has ever waited for: chunk g lives in slot
-// g % kBandRing and completes phase (g / kBandRing) & 1 of that slot's barrier.
+// Bands group * kGroup .. group * kGroup + kGroup - 1 of one long tile by one
+// CTA; warp w renders band group * kGroup + w.
 template <int BW, int BH>
-__device__ __forceinline__ void render_fwd_band(BandSmem& sm, const TileArgs& a, int tile, int band, uint32_t& g,
-                                                unsigned* err)
+__device__ __forceinline__ void render_long_tile(LongSmem<LongTile<BW, BH>::kThreads>& sm, const TileArgs& a,
+                                                 int tile, int group)
 {
-    static_assert(BW * BH <= 32 && kTileX % BW == 0 && kTileY % BH == 0, "band shape");
-    constexpr int kPerRow = kTileX / BW;
-    const int lane = threadIdx.x & 31;
+    using L = LongTile<BW, BH>;
+    constexpr int kPix = L::kPix, kSlots = L::kSlots, kChunk = L::kThreads;
+    const int tid = threadIdx.x, lane = tid & 31, band = group * L::kGroup + (tid >> 5);
     const int W = a.W, H = a.H;
     const int gx = (W + kTileX - 1) / kTileX;
     const int bx = tile % gx, by = tile / gx;
-    const int ox = bx * kTileX + (band % kPerRow) * BW, oy = by * kTileY + (band / kPerRow) * BH;
-    const bool mine = lane < BW * BH;
-    const int px = ox + lane % BW, py = oy + lane / BW;
+    const float tx0 = (float)(bx * kTileX), ty0 = (float)(by * kTileY);
+    const int ox = bx * kTileX + (band % L::kPerRow) * BW, oy = by * kTileY + (band / L::kPerRow) * BH;
+    const int pix_lane = lane % kPix, slot = lane / kPix;
+    const bool mine = lane < kPix;  // the pixel's owner lane keeps its state
+    const int px = ox + pix_lane % BW, py = oy + pix_lane / BW;
     const uint2 range = a.ranges[tile];
     const uint32_t n = range.y - range.x;
-    const uint32_t nc = (n + 31) / 32;
     const bool stats = a.kv_sum != nullptr;
     const PairRecord* recs = a.recs + range.x;
     const float pxf = (float)px, pyf = (float)py;
-    const float rx0 = (float)ox, rx1 = rx0 + (BW - 1);
-    const float ry0 = (float)oy, ry1 = ry0 + (BH - 1);
     float T = 1.0f, C[3] = {0.f, 0.f, 0.f}, wmax = 0.f;
     uint32_t last = 0;
     int maxid = -1;
     bool done = !(mine && px < W && py < H);
 
-    if (!__all_sync(0xffffffffu, done)) {
-        uint32_t issued = nc < (uint32_t)(kBandRing - 1) ? nc : (uint32_t)(kBandRing - 1);
-        if (lane == 0)
-            for (uint32_t c = 0; c < issued; c++) {
-                const uint32_t q = (g + c) % kBandRing;
-                issue_batch(sm.rec[q], &sm.bar[q], recs, c * 32, min(32u, n - c * 32));
-            }
-        uint32_t c = 0;
-        for (; c < nc; c++) {
-            // keep two chunks in flight: the slot refilled here was released at the end of chunk c-1
-            if (lane == 0 && issued < nc) {
-                const uint32_t q = (g + issued) % kBandRing;
-                issue_batch(sm.rec[q], &sm.bar[q], recs, issued * 32, min(32u, n - issued * 32));
-            }
-            if (issued < nc) issued++;
-            const uint32_t q = (g + c) % kBandRing;
-            if (!mbar_wait(&sm.bar[q], ((g + c) / kBandRing) & 1, err)) done = true;
-            const PairRecord* R = sm.rec[q];
-            const uint32_t k0 = c * 32;
-            const uint32_t e = k0 + lane;
-            bool t = false;
-            if (e < n) {
-                const float4 ea = R[lane].a, eb = R[lane].b;
-                t = may_touch(ea.x, ea.y, ea.z, ea.w, eb.x, eb.y, rx0, rx1, ry0, ry1);
-            }
-            uint32_t live = __ballot_sync(0xffffffffu, t);
-            while (live) {
-                const uint32_t j1 = (uint32_t)(__ffs(live) - 1);
-                live &= live - 1;
-                const bool two = live != 0;
-                const uint32_t j2 = two ? (uint32_t)(__ffs(live) - 1) : j1;
-                if (two) live &= live - 1;
-                const float4 ra1 = R[j1].a, rb1 = R[j1].b, ra2 = R[j2].a, rb2 = R[j2].b;
-                const float al1 = done ? 0.f : fwd_alpha(ra1, rb1, pxf, pyf);
-                const float al2 = (done || !two) ? 0.f : fwd_alpha(ra2, rb2, pxf, pyf);
-                band_fold(sm, j1, fwd_accumulate(al1, rb1, R[j1], k0 + j1 + 1, T, C, wmax, maxid, last, done),
-                          stats);
-                band_fold(sm, j2, fwd_accumulate(al2, rb2, R[j2], k0 + j2 + 1, T, C, wmax, maxid, last, done),
-                          stats);
-            }
-            __syncwarp();
-            const uint32_t wm = sm.wmax[lane];
-            if (wm) {
-                if (a.out_point_weight)
-                    atomicMax(reinterpret_cast<unsigned*>(a.out_point_weight) + __float_as_int(R[lane].c.y), wm);
-                sm.wmax[lane] = 0;
-            }
-            if (stats && e < n && sm.kcnt[lane]) {
-                atomicAdd(a.kv_sum + range.x + e, sm.ksum[lane]);
-                atomicAdd(a.kv_cnt + range.x + e, sm.kcnt[lane]);
-                sm.ksum[lane] = 0.f;
-                sm.kcnt[lane] = 0;
-            }
-            __syncwarp();  // every lane is done with slot q before it is refilled
-            if (__all_sync(0xffffffffu, done)) {
-                c++;
-                break;
+    PairRecord nxt;
+    if ((uint32_t)tid < n) nxt = recs[tid];
+    for (uint32_t c0 = 0; c0 < n; c0 += kChunk) {
+        const uint32_t e = c0 + (uint32_t)tid;
+        const bool have = e < n;
+        if (have) sm.rec[tid] = nxt;
+        sm.mask[tid] = have ? band_mask<BW, BH>(nxt.a, nxt.b, tx0, ty0) : 0u;
+        sm.wmax[tid] = 0u;
+        if (stats) {
+            sm.ksum[tid] = 0.f;
+            sm.kcnt[tid] = 0u;
+        }
+        if (e + kChunk < n) nxt = recs[e + kChunk];  // in flight while this chunk is composited
+        __syncthreads();
+        for (int k = 0; k < kChunk / 32 && !__all_sync(0xffffffffu, done); k++) {
+            uint32_t live = __ballot_sync(0xffffffffu, (sm.mask[k * 32 + lane] >> band) & 1u);
+            const PairRecord* R = sm.rec + k * 32;
+            const uint32_t k0 = c0 + (uint32_t)(k * 32);  // tile position of R[0]
+            if constexpr (kSlots == 1) {
+                while (live) {
+                    const uint32_t j1 = (uint32_t)(__ffs(live) - 1);
+                    live &= live - 1;
+                    const bool two = live != 0;
+                    const uint32_t j2 = two ? (uint32_t)(__ffs(live) - 1) : j1;
+                    if (two) live &= live - 1;
+                    const float4 ra1 = R[j1].a, rb1 = R[j1].b, ra2 = R[j2].a, rb2 = R[j2].b;
+                    const float al1 = done ? 0.f : fwd_alpha(ra1, rb1, pxf, pyf);
+                    const float al2 = (done || !two) ? 0.f : fwd_alpha(ra2, rb2, pxf, pyf);
+                    long_fold(sm, k * 32 + j1,
+                              fwd_accumulate(al1, rb1, R[j1], k0 + j1 + 1, T, C, wmax, maxid, last, done), stats);
+                    long_fold(sm, k * 32 + j2,
+                              fwd_accumulate(al2, rb2, R[j2], k0 + j2 + 1, T, C, wmax, maxid, last, done), stats);
+                }
+            } else {
+                while (live) {
+                    // the next kSlots live records, in order (32: none); lanes of slot s
+                    // evaluate record js[s] at their pixel
+                    uint32_t js[kSlots];
+                    uint32_t mj = 32u;
+#pragma unroll
+                    for (int s = 0; s < kSlots; s++) {
+                        js[s] = live ? (uint32_t)(__ffs(live) - 1) : 32u;
+                        live &= live - 1;
+                        if (s == slot) mj = js[s];
+                    }
+                    const bool pdone = __shfl_sync(0xffffffffu, done, pix_lane);
+                    const float al = (mj < 32u && !pdone) ? fwd_alpha(R[mj].a, R[mj].b, pxf, pyf) : 0.f;
+#pragma unroll
+                    for (int s = 0; s < kSlots; s++) {
+                        const float as = __shfl_sync(0xffffffffu, al, s * kPix + pix_lane);
+                        const uint32_t j = js[s];
+                        if (j < 32u)
+                            long_fold(sm, k * 32 + j,
+                                      fwd_accumulate(as, R[j].b, R[j], k0 + j + 1, T, C, wmax, maxid, last, done),
+                                      stats);
+                    }
+                }
             }
         }
-        // drain the chunks still in flight, so that every slot's phase count stays in step
-        if (lane == 0)
-            for (uint32_t k = c; k < issued; k++) mbar_wait(&sm.bar[(g + k) % kBandRing], ((g + k) / kBandRing) & 1, err);
-        __syncwarp();
-        g += issued;
+        __syncthreads();
+        if (have) {
+            const uint32_t wm = sm.wmax[tid];
+            if (wm && a.out_point_weight)
+                atomicMax(reinterpret_cast<unsigned*>(a.out_point_weight) + __float_as_int(sm.rec[tid].c.y), wm);
+            if (stats && sm.kcnt[tid]) {
+                atomicAdd(a.kv_sum + range.x + e, sm.ksum[tid]);
+                atomicAdd(a.kv_cnt + range.x + e, sm.kcnt[tid]);
+            }
+        }
+        // every pixel of the tile done: no later record can contribute (also the
+        // barrier before the next chunk overwrites the shared records)
+        if (__syncthreads_and(done)) break;
     }
     if (mine && px < W && py < H) {
         const int pix = W * py + px;
@@ -657,7 +702,7 @@ __device__ __forceinline__ void long_tile_push(uint32_t n, uint32_t id, uint32_t
 
 // The long tiles of one view (ids are tiles) or of a multi-view batch (ids are
 // global work items, mapped to (view, tile) by begin[]).  ctr: [0] long tiles,
-// [1] band queue, [2 + b] tiles in bin b.
+// [1] tile queue, [2 + b] tiles in bin b.
 __global__ void long_tiles_kernel(const uint2* __restrict__ ranges, uint32_t num_tiles, uint32_t split_min,
                                   uint32_t* __restrict__ list, uint32_t* __restrict__ ctr)
 {
@@ -678,19 +723,16 @@ __global__ void long_tiles_multi_kernel(const TileArgs* __restrict__ views, cons
     if (r.y - r.x >= split_min) long_tile_push(r.y - r.x, i, total, list, ctr);
 }
 
-// Band item -> long tile id, longest bins first.  False when the queue is empty.
-template <int kBandsPerTile>
-__device__ __forceinline__ bool next_band(uint32_t* ctr, const uint32_t* __restrict__ list, uint32_t cap,
-                                          uint32_t& id, int& band)
+// The next (long tile, band group) for this CTA (thread 0), longest bins first.
+// False when the queue is empty.
+template <int kGroups>
+__device__ __forceinline__ bool next_long_tile(uint32_t* ctr, const uint32_t* __restrict__ list, uint32_t cap,
+                                               uint32_t& id, int& group)
 {
-    const int lane = threadIdx.x & 31;
-    uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(ctr + 1, 1u);
-    item = __shfl_sync(0xffffffffu, item, 0);
-    const uint32_t total = *(volatile uint32_t*)ctr;
-    if (item >= total * kBandsPerTile) return false;
-    uint32_t r = item / kBandsPerTile;
-    band = (int)(item % kBandsPerTile);
+    const uint32_t item = atomicAdd(ctr + 1, 1u);
+    if (item >= *(volatile uint32_t*)ctr * kGroups) return false;
+    uint32_t r = item / kGroups;
+    group = (int)(item % kGroups);
     for (int b = kLongBuckets - 1; b >= 0; b--) {
         const uint32_t c = *(volatile uint32_t*)(ctr + 2 + b);
         if (r < c) {
@@ -703,31 +745,51 @@ __device__ __forceinline__ bool next_band(uint32_t* ctr, const uint32_t* __restr
 }
 
 template <int BW, int BH>
-__global__ void __launch_bounds__(32 * kBandWarps)
-    render_fwd_band_kernel(TileArgs a, const uint32_t* __restrict__ list, uint32_t* ctr, uint32_t cap, unsigned* err)
+__global__ void __launch_bounds__(LongTile<BW, BH>::kThreads)
+    render_fwd_long_kernel(TileArgs a, const uint32_t* __restrict__ list, uint32_t* ctr, uint32_t cap)
 {
-    __shared__ __align__(128) BandSmem sm[kBandWarps];
-    BandSmem& my = sm[threadIdx.x >> 5];
-    band_smem_init(my);
-    uint32_t g = 0, id = 0;
-    int band = 0;
-    while (next_band<kTileX * kTileY / (BW * BH)>(ctr, list, cap, id, band))
-        render_fwd_band<BW, BH>(my, a, (int)id, band, g, err);
+    extern __shared__ __align__(128) unsigned char long_dyn[];
+    auto& sm = *reinterpret_cast<LongSmem<LongTile<BW, BH>::kThreads>*>(long_dyn);
+    __shared__ uint32_t s_id;
+    __shared__ int s_ok, s_group;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            uint32_t id = 0;
+            int group = 0;
+            s_ok = next_long_tile<LongTile<BW, BH>::kGroups>(ctr, list, cap, id, group);
+            s_id = id;
+            s_group = group;
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        render_long_tile<BW, BH>(sm, a, (int)s_id, s_group);
+        __syncthreads();  // s_id / s_group / s_ok are rewritten for the next item
+    }
 }
 
 template <int BW, int BH>
-__global__ void __launch_bounds__(32 * kBandWarps)
-    render_fwd_band_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin, int nviews,
-                                 const uint32_t* __restrict__ list, uint32_t* ctr, uint32_t cap, unsigned* err)
+__global__ void __launch_bounds__(LongTile<BW, BH>::kThreads)
+    render_fwd_long_multi_kernel(const TileArgs* __restrict__ views, const uint32_t* __restrict__ begin, int nviews,
+                                 const uint32_t* __restrict__ list, uint32_t* ctr, uint32_t cap)
 {
-    __shared__ __align__(128) BandSmem sm[kBandWarps];
-    BandSmem& my = sm[threadIdx.x >> 5];
-    band_smem_init(my);
-    uint32_t g = 0, id = 0;
-    int band = 0;
-    while (next_band<kTileX * kTileY / (BW * BH)>(ctr, list, cap, id, band)) {
+    extern __shared__ __align__(128) unsigned char long_dyn[];
+    auto& sm = *reinterpret_cast<LongSmem<LongTile<BW, BH>::kThreads>*>(long_dyn);
+    __shared__ uint32_t s_id;
+    __shared__ int s_ok, s_group;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            uint32_t id = 0;
+            int group = 0;
+            s_ok = next_long_tile<LongTile<BW, BH>::kGroups>(ctr, list, cap, id, group);
+            s_id = id;
+            s_group = group;
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        const uint32_t id = s_id;
         const int v = view_of(begin, nviews, id);
-        render_fwd_band<BW, BH>(my, views[v], (int)(id - begin[v]), band, g, err);
+        render_long_tile<BW, BH>(sm, views[v], (int)(id - begin[v]), s_group);
+        __syncthreads();
     }
 }
 
@@ -984,36 +1046,56 @@ size_t fwd_smem_bytes(bool stats)
     return stats ? sizeof(FwdSmem<kBatch>) : offsetof(FwdSmem<kBatch>, ksum);
 }
 
+// Dynamic shared memory of a long-tile kernel (opted in once per process and device
+// ordinal; Tag tells the kernels apart: single-view 0, multi-view 1).
+template <int BW, int BH, int Tag, typename Kern>
+size_t long_smem_bytes(Kern k)
+{
+    static bool done[64] = {};
+    const size_t bytes = sizeof(LongSmem<LongTile<BW, BH>::kThreads>);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !done[dev]) {
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (dev >= 0 && dev < 64) done[dev] = true;
+    }
+    return bytes;
+}
+
 // Band shapes (fgs_set_render_split): 0 = 16x2, 1 = 8x4, 2 = 4x4, 3 = 4x2 pixels per warp.
 template <int BW, int BH>
-void band_launch(const TileArgs& a, const uint32_t* list, uint32_t* ctr, uint32_t cap, unsigned* err, cudaStream_t s)
+void long_launch(const TileArgs& a, const uint32_t* list, uint32_t* ctr, uint32_t cap, cudaStream_t s)
 {
-    render_fwd_band_kernel<BW, BH><<<resident_ctas(render_fwd_band_kernel<BW, BH>, 32 * kBandWarps), 32 * kBandWarps,
-                                     0, s>>>(a, list, ctr, cap, err);
+    constexpr int kThreads = LongTile<BW, BH>::kThreads;
+    const size_t smem = long_smem_bytes<BW, BH, 0>(render_fwd_long_kernel<BW, BH>);
+    render_fwd_long_kernel<BW, BH><<<resident_ctas(render_fwd_long_kernel<BW, BH>, kThreads), kThreads, smem, s>>>(
+        a, list, ctr, cap);
 }
-void launch_band_kernel(int shape, const TileArgs& a, const uint32_t* list, uint32_t* ctr, uint32_t cap, unsigned* err,
+void launch_long_kernel(int shape, const TileArgs& a, const uint32_t* list, uint32_t* ctr, uint32_t cap,
                         cudaStream_t s)
 {
-    if (shape == 1) band_launch<8, 4>(a, list, ctr, cap, err, s);
-    else if (shape == 2) band_launch<4, 4>(a, list, ctr, cap, err, s);
-    else if (shape == 3) band_launch<4, 2>(a, list, ctr, cap, err, s);
-    else band_launch<16, 2>(a, list, ctr, cap, err, s);
+    if (shape == 1) long_launch<8, 4>(a, list, ctr, cap, s);
+    else if (shape == 2) long_launch<4, 4>(a, list, ctr, cap, s);
+    else if (shape == 3) long_launch<4, 2>(a, list, ctr, cap, s);
+    else long_launch<16, 2>(a, list, ctr, cap, s);
 }
 template <int BW, int BH>
-void band_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, const uint32_t* list, uint32_t* ctr,
-                       uint32_t cap, unsigned* err, cudaStream_t s)
+void long_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, const uint32_t* list, uint32_t* ctr,
+                       uint32_t cap, cudaStream_t s)
 {
-    render_fwd_band_multi_kernel<BW, BH>
-        <<<resident_ctas(render_fwd_band_multi_kernel<BW, BH>, 32 * kBandWarps), 32 * kBandWarps, 0, s>>>(
-            views, begin, nviews, list, ctr, cap, err);
+    constexpr int kThreads = LongTile<BW, BH>::kThreads;
+    const size_t smem = long_smem_bytes<BW, BH, 1>(render_fwd_long_multi_kernel<BW, BH>);
+    render_fwd_long_multi_kernel<BW, BH>
+        <<<resident_ctas(render_fwd_long_multi_kernel<BW, BH>, kThreads), kThreads, smem, s>>>(views, begin, nviews,
+                                                                                             list, ctr, cap);
 }
-void launch_band_multi_kernel(int shape, const TileArgs* views, const uint32_t* begin, int nviews,
-                              const uint32_t* list, uint32_t* ctr, uint32_t cap, unsigned* err, cudaStream_t s)
+void launch_long_multi_kernel(int shape, const TileArgs* views, const uint32_t* begin, int nviews,
+                              const uint32_t* list, uint32_t* ctr, uint32_t cap, cudaStream_t s)
 {
-    if (shape == 1) band_multi_launch<8, 4>(views, begin, nviews, list, ctr, cap, err, s);
-    else if (shape == 2) band_multi_launch<4, 4>(views, begin, nviews, list, ctr, cap, err, s);
-    else if (shape == 3) band_multi_launch<4, 2>(views, begin, nviews, list, ctr, cap, err, s);
-    else band_multi_launch<16, 2>(views, begin, nviews, list, ctr, cap, err, s);
+    if (shape == 1) long_multi_launch<8, 4>(views, begin, nviews, list, ctr, cap, s);
+    else if (shape == 2) long_multi_launch<4, 4>(views, begin, nviews, list, ctr, cap, s);
+    else if (shape == 3) long_multi_launch<4, 2>(views, begin, nviews, list, ctr, cap, s);
+    else long_multi_launch<16, 2>(views, begin, nviews, list, ctr, cap, s);
 }
 
 template <int PPT, int B>
@@ -1035,7 +1117,7 @@ void fwd_launch(int grid, const ImageState& im, const BinState& b, long long K, 
         }
         long_tiles_kernel<<<(grid + 255) / 256, 256, 0, s>>>(im.ranges, (uint32_t)grid, (uint32_t)split, im.long_list,
                                                              im.long_ctr);
-        launch_band_kernel(band_shape, a, im.long_list, im.long_ctr, (uint32_t)grid, err, s);
+        launch_long_kernel(band_shape, a, im.long_list, im.long_ctr, (uint32_t)grid, s);
         note_launches(2);
     }
     render_fwd_kernel<PPT, B><<<grid, 256 / PPT, fwd_smem_bytes<B>(stats), s>>>(a, (uint32_t)(split > 0 ? split : 0),
@@ -1122,7 +1204,7 @@ void fwd_multi_launch(const TileArgs* views, const uint32_t* begin, int nviews, 
         cudaMemsetAsync(long_ctr, 0, (2 + kLongBuckets) * sizeof(uint32_t), s);
         long_tiles_multi_kernel<<<(total + 255) / 256, 256, 0, s>>>(views, begin, nviews, total, (uint32_t)split,
                                                                     long_list, long_ctr);
-        launch_band_multi_kernel(band_shape, views, begin, nviews, long_list, long_ctr, total, err, s);
+        launch_long_multi_kernel(band_shape, views, begin, nviews, long_list, long_ctr, total, s);
         note_launches(2);
     }
     int dev = 0, sms = 148, per_sm = 1;

@@ -352,7 +352,8 @@ int fgs_profile_enable(int on);
 int fgs_set_render_config(int fwd_ppt, int fwd_batch, int bwd_ppt, int bwd_batch);
 int fgs_get_render_config(int *cfg);
 /* Forward: tiles with at least min_records tile/Gaussian pairs are rendered in bands of pixels, one
- * warp per band, longest tiles first, before the other tiles (min_records 0, the default: never).
+ * warp per band and four bands per CTA, longest tiles first, before the other tiles (min_records 0,
+ * the default: never).
  * band_shape: 0 = 16x2, 1 = 8x4, 2 = 4x4, 3 = 4x2 pixels per band.  The outputs do not change; long
  * tiles stop being the critical path of the forward.  Process-wide, like the above.
  * fgs_get_render_split: cfg int[2] out (min_records, band_shape).                                   */
