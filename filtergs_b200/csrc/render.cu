@@ -490,7 +490,7 @@ __global__ void __launch_bounds__(256 / PPT, fwd_min_ctas<PPT>())
 // least split_min records are rendered instead in bands of BW x BH pixels, one
 // warp per band and four bands per CTA (a tile's 256 / (BW BH) bands spread over
 // several SMs), longest tiles first.  The CTA stages the tile's records in
-// chunks of one record per thread (plain coalesced loads; the next chunk is
+// chunks of two records per thread (plain coalesced loads; the next chunk is
 // loaded into registers while the current one is composited), and each thread
 // works out which bands its record can reach (band_mask), so a record is tested
 // once per four bands instead of once per band, and a warp finds its band's
@@ -517,7 +517,9 @@ struct LongTile {
     static constexpr int kBands = kPerRow * kRows;         // bands per tile
     static constexpr int kGroup = kBands < 4 ? kBands : 4; // bands (warps) per CTA
     static constexpr int kGroups = kBands / kGroup;        // CTAs per tile
-    static constexpr int kThreads = 32 * kGroup;           // also the records staged per chunk
+    static constexpr int kThreads = 32 * kGroup;
+    static constexpr int kPer = 2;                         // records each thread stages per chunk
+    static constexpr int kChunk = kPer * kThreads;
     static constexpr int kSlots = 32 / kPix;               // records evaluated per step
 };
 
@@ -582,11 +584,11 @@ __device__ __forceinline__ void long_fold(LongSmem<kChunk>& sm, uint32_t j, floa
 // Bands group * kGroup .. group * kGroup + kGroup - 1 of one long tile by one
 // CTA; warp w renders band group * kGroup + w.
 template <int BW, int BH>
-__device__ __forceinline__ void render_long_tile(LongSmem<LongTile<BW, BH>::kThreads>& sm, const TileArgs& a,
+__device__ __forceinline__ void render_long_tile(LongSmem<LongTile<BW, BH>::kChunk>& sm, const TileArgs& a,
                                                  int tile, int group)
 {
     using L = LongTile<BW, BH>;
-    constexpr int kPix = L::kPix, kSlots = L::kSlots, kChunk = L::kThreads;
+    constexpr int kPix = L::kPix, kSlots = L::kSlots, kPer = L::kPer, kChunk = L::kChunk;
     const int tid = threadIdx.x, lane = tid & 31, band = group * L::kGroup + (tid >> 5);
     const int W = a.W, H = a.H;
     const int gx = (W + kTileX - 1) / kTileX;
@@ -606,19 +608,47 @@ __device__ __forceinline__ void render_long_tile(LongSmem<LongTile<BW, BH>::kThr
     int maxid = -1;
     bool done = !(mine && px < W && py < H);
 
-    PairRecord nxt;
-    if ((uint32_t)tid < n) nxt = recs[tid];
-    for (uint32_t c0 = 0; c0 < n; c0 += kChunk) {
-        const uint32_t e = c0 + (uint32_t)tid;
-        const bool have = e < n;
-        if (have) sm.rec[tid] = nxt;
-        sm.mask[tid] = have ? band_mask<BW, BH>(nxt.a, nxt.b, tx0, ty0) : 0u;
-        sm.wmax[tid] = 0u;
-        if (stats) {
-            sm.ksum[tid] = 0.f;
-            sm.kcnt[tid] = 0u;
+    // A contributing record's per-chunk sums leave through global atomics; slot i
+    // of chunk cbase is flushed by the thread that staged it, before it restages
+    // the slot (no other thread touches the slot between the barriers around the
+    // compositing).
+    auto flush = [&](uint32_t cbase) {
+#pragma unroll
+        for (int q = 0; q < kPer; q++) {
+            const int i = q * L::kThreads + tid;
+            const uint32_t e = cbase + (uint32_t)i;
+            if (e >= n) continue;
+            const uint32_t wm = sm.wmax[i];
+            if (wm && a.out_point_weight)
+                atomicMax(reinterpret_cast<unsigned*>(a.out_point_weight) + __float_as_int(sm.rec[i].c.y), wm);
+            if (stats && sm.kcnt[i]) {
+                atomicAdd(a.kv_sum + range.x + e, sm.ksum[i]);
+                atomicAdd(a.kv_cnt + range.x + e, sm.kcnt[i]);
+            }
         }
-        if (e + kChunk < n) nxt = recs[e + kChunk];  // in flight while this chunk is composited
+    };
+    PairRecord nxt[kPer];
+#pragma unroll
+    for (int q = 0; q < kPer; q++)
+        if ((uint32_t)(q * L::kThreads + tid) < n) nxt[q] = recs[q * L::kThreads + tid];
+    uint32_t last_c = 0;
+    bool pending = false;
+    for (uint32_t c0 = 0; c0 < n; c0 += kChunk) {
+        if (pending) flush(last_c);
+#pragma unroll
+        for (int q = 0; q < kPer; q++) {
+            const int i = q * L::kThreads + tid;
+            const uint32_t e = c0 + (uint32_t)i;
+            const bool have = e < n;
+            if (have) sm.rec[i] = nxt[q];
+            sm.mask[i] = have ? band_mask<BW, BH>(nxt[q].a, nxt[q].b, tx0, ty0) : 0u;
+            sm.wmax[i] = 0u;
+            if (stats) {
+                sm.ksum[i] = 0.f;
+                sm.kcnt[i] = 0u;
+            }
+            if (e + kChunk < n) nxt[q] = recs[e + kChunk];  // in flight while this chunk is composited
+        }
         __syncthreads();
         for (int k = 0; k < kChunk / 32 && !__all_sync(0xffffffffu, done); k++) {
             uint32_t live = __ballot_sync(0xffffffffu, (sm.mask[k * 32 + lane] >> band) & 1u);
@@ -665,20 +695,13 @@ __device__ __forceinline__ void render_long_tile(LongSmem<LongTile<BW, BH>::kThr
                 }
             }
         }
-        __syncthreads();
-        if (have) {
-            const uint32_t wm = sm.wmax[tid];
-            if (wm && a.out_point_weight)
-                atomicMax(reinterpret_cast<unsigned*>(a.out_point_weight) + __float_as_int(sm.rec[tid].c.y), wm);
-            if (stats && sm.kcnt[tid]) {
-                atomicAdd(a.kv_sum + range.x + e, sm.ksum[tid]);
-                atomicAdd(a.kv_cnt + range.x + e, sm.kcnt[tid]);
-            }
-        }
-        // every pixel of the tile done: no later record can contribute (also the
-        // barrier before the next chunk overwrites the shared records)
+        last_c = c0;
+        pending = true;
+        // every pixel of this band group done: no later record can contribute (also
+        // the barrier before the next chunk's staging)
         if (__syncthreads_and(done)) break;
     }
+    if (pending) flush(last_c);
     if (mine && px < W && py < H) {
         const int pix = W * py + px;
         a.final_T[pix] = T;
@@ -749,7 +772,7 @@ __global__ void __launch_bounds__(LongTile<BW, BH>::kThreads)
     render_fwd_long_kernel(TileArgs a, const uint32_t* __restrict__ list, uint32_t* ctr, uint32_t cap)
 {
     extern __shared__ __align__(128) unsigned char long_dyn[];
-    auto& sm = *reinterpret_cast<LongSmem<LongTile<BW, BH>::kThreads>*>(long_dyn);
+    auto& sm = *reinterpret_cast<LongSmem<LongTile<BW, BH>::kChunk>*>(long_dyn);
     __shared__ uint32_t s_id;
     __shared__ int s_ok, s_group;
     for (;;) {
@@ -773,7 +796,7 @@ __global__ void __launch_bounds__(LongTile<BW, BH>::kThreads)
                                  const uint32_t* __restrict__ list, uint32_t* ctr, uint32_t cap)
 {
     extern __shared__ __align__(128) unsigned char long_dyn[];
-    auto& sm = *reinterpret_cast<LongSmem<LongTile<BW, BH>::kThreads>*>(long_dyn);
+    auto& sm = *reinterpret_cast<LongSmem<LongTile<BW, BH>::kChunk>*>(long_dyn);
     __shared__ uint32_t s_id;
     __shared__ int s_ok, s_group;
     for (;;) {
@@ -1052,7 +1075,7 @@ template <int BW, int BH, int Tag, typename Kern>
 size_t long_smem_bytes(Kern k)
 {
     static bool done[64] = {};
-    const size_t bytes = sizeof(LongSmem<LongTile<BW, BH>::kThreads>);
+    const size_t bytes = sizeof(LongSmem<LongTile<BW, BH>::kChunk>);
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || !done[dev]) {
