@@ -840,9 +840,11 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
     // dot product with dL/dpixel, so the pixel carries that dot product (acc_dot)
     // and the previous contributor's colour dotted the same way (last_dot): the
     // same sums, regrouped, in 2 values instead of 6.
-    float T[PPT], T_final[PPT], dpix[PPT][3], acc_dot[PPT], last_dot[PPT], last_alpha[PPT], pyf[PPT];
+    float T[PPT], dpix[PPT][3], acc_dot[PPT], last_dot[PPT], last_alpha[PPT];
     uint32_t last[PPT];
-    float bg_dot[PPT];
+    // the background term of dL/dalpha, -T_final (bg . dL/dpixel) / (1 - alpha): its
+    // numerator per pixel (zero for a black background, and then skipped)
+    float bgT[PPT];
     const float bg0 = a.bg[0], bg1 = a.bg[1], bg2 = a.bg[2];
     uint32_t my_max = 0;
 #pragma unroll
@@ -850,8 +852,7 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
         const int py = by * kTileY + ly0 + k;
         const bool inside = px < W && py < H;
         const int pix = W * py + px;
-        T_final[k] = inside ? a.final_T[pix] : 0.f;
-        T[k] = T_final[k];
+        T[k] = inside ? a.final_T[pix] : 0.f;
         last[k] = inside ? a.n_contrib[pix] : 0;
         my_max = max(my_max, last[k]);
 #pragma unroll
@@ -859,8 +860,7 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
         acc_dot[k] = 0.f;
         last_dot[k] = 0.f;
         last_alpha[k] = 0.f;
-        bg_dot[k] = bg0 * dpix[k][0] + bg1 * dpix[k][1] + bg2 * dpix[k][2];
-        pyf[k] = (float)py;
+        bgT[k] = -T[k] * (bg0 * dpix[k][0] + bg1 * dpix[k][1] + bg2 * dpix[k][2]);
     }
     const float pxf = (float)px;
     const float rx0 = (float)(bx * kTileX), rx1 = rx0 + (kTileX - 1);
@@ -923,7 +923,7 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
                     if (contributor >= last[k]) continue;
                     // G and alpha in the forward's arithmetic (fwd_alpha): the same
                     // bits, so this pass skips exactly the pairs the forward skipped
-                    const float dx = ra.x - pxf, dy = ra.y - pyf[k];
+                    const float dx = ra.x - pxf, dy = ra.y - (float)(by * kTileY + ly0 + k);
                     const float qf = __fmaf_rn(__fmul_rn(ra.z, dx), dx, __fmul_rn(__fmul_rn(rb.x, dy), dy));
                     const float power = __fmaf_rn(-0.5f, qf, -__fmul_rn(__fmul_rn(ra.w, dx), dy));
                     if (power > 0.0f) continue;
@@ -945,7 +945,7 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
                     last_alpha[k] = alpha;
                     float dL_dalpha = (cdot - acc_dot[k]) * T[k];
                     // background term; exactly zero (and skipped) for a black background
-                    if (bg_dot[k] != 0.f) dL_dalpha += (-T_final[k] * inv_1ma) * bg_dot[k];
+                    if (bgT[k] != 0.f) dL_dalpha += bgT[k] * inv_1ma;
                     if (kConsistent && oG > 0.99f) dL_dalpha = 0.f;
                     // s = G dL/dG; the sums below, times gscale, are dL/dmean2D
                     // (G (a dx + b dy), G (b dx + c dy)) and dL/dconic (G dx dx, G dx dy,
