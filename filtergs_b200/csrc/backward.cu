@@ -143,10 +143,11 @@ __device__ __forceinline__ void load_sh_row(const float* __restrict__ shrow, int
 // Gaussians are taken in depth rank j, whose pairs are the contiguous rows
 // [pair_off[j], pair_off[j + 1]) (the last ends at K), so a warp reads its next
 // Gaussian's row range while it sums the current one.  One warp per Gaussian:
-// lane l takes rows l, l+32, ... (coalesced 36-byte rows, 128 rows in flight per
+// lane l takes rows l, l+32, ... (coalesced 36-byte rows, 64 rows in flight per
 // round trip, so a splat over thousands of tiles does not stall the kernel) and a
 // fixed shuffle tree adds them, 32 rows at a time in emission order -- the same
-// sum on every run.  Row layout: dcolor r,g,b | dmean2D x,y | dconic x,y,w |
+// sum on every run.  Two Gaussians of at most 32 rows each (the common case) share
+// one round trip.  Row layout: dcolor r,g,b | dmean2D x,y | dconic x,y,w |
 // dopacity.  vis (optional): the view sets vis_bit in vis[idx] for every Gaussian
 // it sees.  Compiled for 4 blocks per SM (64 registers; measured faster than the
 // compiler's 76 with fewer warps).
@@ -167,20 +168,15 @@ __global__ void __launch_bounds__(256, 4)
         e1 = max(e0, min(jj + 1 < V ? __ldg(pair_off + jj + 1) : K, rows));
         idx = (int)__ldg(visible_ids + jj);
     };
-    uint32_t e0 = 0, e1 = 0;
-    int idx = 0;
-    if (j < V) range(j, e0, e1, idx);
-    while (j < V) {
-        const uint32_t jn = j + nwarps;
-        uint32_t n0 = 0, n1 = 0;
-        int nidx = 0;
-        if (jn < V) range(jn, n0, n1, nidx);  // the next Gaussian's rows, in flight meanwhile
+    // sum of rows [e0, e1) on lanes 2q and 2q+1 (component q): 32 rows at a time in
+    // emission order, each group through the same shuffle tree, added to 0 in turn
+    auto sum_rows = [&](uint32_t e0, uint32_t e1) {
         const uint32_t ne = e1 - e0;
-        float acc = 0.f;  // lanes 2q and 2q+1: component q
-        for (uint32_t k = 0; k < ne; k += 128) {
-            float v[4][9];
+        float acc = 0.f;
+        for (uint32_t k = 0; k < ne; k += 64) {
+            float v[2][9];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < 2; u++) {
                 if (k + 32 * u >= ne) continue;  // (warp-uniform) no rows in this group
                 const uint32_t r = k + 32 * u + lane;
                 const float* src = pgrad + (size_t)(e0 + r) * 9;
@@ -188,9 +184,12 @@ __global__ void __launch_bounds__(256, 4)
                 for (int q = 0; q < 9; q++) v[u][q] = r < ne ? __ldg(src + q) : 0.f;
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+            for (int u = 0; u < 2; u++)
                 if (k + 32 * u < ne) acc += warp_transpose_sum9(v[u]);
         }
+        return acc;
+    };
+    auto store = [&](int idx, float acc) {
         if (vis && lane == 0) atomicOr(vis + idx, vis_bit);  // this view sees Gaussian idx
         if (lane < 18 && !(lane & 1)) {
             const int q = lane >> 1;
@@ -201,10 +200,43 @@ __global__ void __launch_bounds__(256, 4)
                                : dopac + idx;
             *dst = acc;
         }
-        j = jn;
-        e0 = n0;
-        e1 = n1;
-        idx = nidx;
+    };
+    // Gaussians j and j + nwarps together when both have at most 32 rows (most do:
+    // a Gaussian covers ~20 tiles at 1080p), so one round trip brings two row sets
+    // while the next pair's ranges are fetched; the sums are the ones sum_rows forms.
+    uint32_t a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+    int ia = 0, ib = 0;
+    if (j < V) range(j, a0, a1, ia);
+    if (j + nwarps < V) range(j + nwarps, b0, b1, ib);
+    while (j < V) {
+        const uint32_t jb = j + nwarps, jc = jb + nwarps, jd = jc + nwarps;
+        uint32_t c0 = 0, c1 = 0, d0 = 0, d1 = 0;
+        int ic = 0, id = 0;
+        if (jb < V && a1 - a0 <= 32 && b1 - b0 <= 32) {
+            if (jc < V) range(jc, c0, c1, ic);  // the next pair, in flight meanwhile
+            if (jd < V) range(jd, d0, d1, id);
+            float va[9], vb[9];
+            const float* sa = pgrad + (size_t)(a0 + lane) * 9;
+            const float* sb = pgrad + (size_t)(b0 + lane) * 9;
+#pragma unroll
+            for (int q = 0; q < 9; q++) {
+                va[q] = lane < a1 - a0 ? __ldg(sa + q) : 0.f;
+                vb[q] = lane < b1 - b0 ? __ldg(sb + q) : 0.f;
+            }
+            const float ta = warp_transpose_sum9(va), tb = warp_transpose_sum9(vb);
+            store(ia, a1 > a0 ? 0.f + ta : 0.f);
+            store(ib, b1 > b0 ? 0.f + tb : 0.f);
+            j = jc;
+            a0 = c0; a1 = c1; ia = ic;
+            b0 = d0; b1 = d1; ib = id;
+            continue;
+        }
+        // one Gaussian (long row ranges, or the last one): the next ranges in flight
+        if (jc < V) range(jc, c0, c1, ic);
+        store(ia, sum_rows(a0, a1));
+        j = jb;
+        a0 = b0; a1 = b1; ia = ib;
+        b0 = c0; b1 = c1; ib = ic;
     }
 }
 

@@ -158,15 +158,17 @@ def test_batched_set_io_retargets_captured_graph(cuda):
 
 def test_batched_long_tile_bands(cuda):
     """The multi-view forward with long tiles split into bands (a low threshold, so that most tiles
-    of every view take the band path): images equal the unsplit batch's."""
+    of every view take the band path), at every band shape (16x2 and 8x4 take two records per
+    step, 4x4 and 4x2 evaluate several records per step across lanes): images equal the unsplit
+    batch's."""
     sc = _scene(P=200_000, seed=5011)
     cams = _cams(3, seed=5012)
     bg = torch.zeros(3, device="cuda")
     was = _lib.get_render_split()
     out = []
     try:
-        for split in (0, 64):
-            _lib.set_render_split(split, 2)
+        for split, shape in ((0, 0), (64, 0), (64, 1), (64, 2), (64, 3)):
+            _lib.set_render_split(split, shape)
             br = BatchedRasterizer(sc["means3D"], sc["opacities"], sc["scales"], sc["rotations"], cams,
                                    shs=sc["shs"], sh_degree=3, bg=bg, graph=False)
             br.forward()
@@ -176,8 +178,9 @@ def test_batched_long_tile_bands(cuda):
             del br
     finally:
         _lib.set_render_split(*was)
-    for x, y in zip(*out):
-        assert torch.equal(x, y)
+    for shape_out in out[1:]:
+        for x, y in zip(out[0], shape_out):
+            assert torch.equal(x, y)
 
 
 def test_batched_full_forward_outputs_match_plain(cuda):
