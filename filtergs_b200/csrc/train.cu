@@ -188,16 +188,38 @@ __global__ void __launch_bounds__(kTX* kTY)
     }
 }
 
-// sums[0] += sum(l1 partials), sums[1] += sum(ssim partials), in index order (one thread)
-__global__ void loss_reduce_kernel(const float* __restrict__ l1p, int nl1, const float* __restrict__ sp, int ns,
-                                   double* __restrict__ sums)
+// sums[0] += sum(l1 partials), sums[1] += sum(ssim partials), by one block in a
+// fixed order: thread t adds partials t, t + blockDim.x, ... in turn, a butterfly of
+// shuffles adds the warp's 32 values (every lane ends with the same bits: each step
+// adds the same two operands on both lanes), and thread 0 adds the warp totals in
+// warp order.  Every call with the same partials gives the same sums.
+__global__ void __launch_bounds__(1024) loss_reduce_kernel(const float* __restrict__ l1p, int nl1,
+                                                           const float* __restrict__ sp, int ns,
+                                                           double* __restrict__ sums)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double s_a[32], s_b[32];
     double a = 0.0, b = 0.0;
-    for (int i = 0; i < nl1; i++) a += l1p[i];
-    for (int i = 0; i < ns; i++) b += sp[i];
-    sums[0] += a;
-    sums[1] += b;
+    for (int i = threadIdx.x; i < nl1; i += blockDim.x) a += l1p[i];
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) b += sp[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_a[threadIdx.x >> 5] = a;
+        s_b[threadIdx.x >> 5] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ta = 0.0, tb = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            ta += s_a[w];
+            tb += s_b[w];
+        }
+        sums[0] += ta;
+        sums[1] += tb;
+    }
 }
 
 // ---------------------------------------------------------------- activation, densification, Adam
@@ -375,7 +397,7 @@ int fgs_loss_l1_ssim(int width, int height, const float* pred, const float* targ
     static const Window win = make_window();
     ssim_forward_kernel<<<go, kTX * kTY, 0, s>>>(width, height, pred, target, win, ssim_grad_scale, gmap, sp);
     loss_grad_kernel<<<gp, kTX * kTY, 0, s>>>(width, height, pred, target, win, gmap, l1_grad_scale, dL_dpred, l1p);
-    loss_reduce_kernel<<<1, 32, 0, s>>>(l1p, (int)(gp.x * gp.y * gp.z), sp, (int)(go.x * go.y * go.z), sums);
+    loss_reduce_kernel<<<1, 1024, 0, s>>>(l1p, (int)(gp.x * gp.y * gp.z), sp, (int)(go.x * go.y * go.z), sums);
     note_launches(3);
     return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
 }
