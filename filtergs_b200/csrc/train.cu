@@ -272,15 +272,51 @@ __device__ __forceinline__ void adam_update(float& p, float& m, float& v, float 
 
 }  // namespace
 
+// Bias corrections of the global step, as the reference forms them (double), and the
+// float coefficients of the update.
+struct AdamCoef {
+    double bc1;
+    float bc2s, b1, b2, omb1, omb2, eps;
+};
+
+__device__ __forceinline__ AdamCoef adam_coef(const fgs_adam_args& a, int t)
+{
+    AdamCoef c;
+    c.bc1 = 1.0 - pow(a.beta1, (double)t);
+    c.bc2s = (float)sqrt(1.0 - pow(a.beta2, (double)t));
+    c.b1 = (float)a.beta1;
+    c.b2 = (float)a.beta2;
+    c.omb1 = (float)(1.0 - a.beta1);
+    c.omb2 = (float)(1.0 - a.beta2);
+    c.eps = a.eps;
+    return c;
+}
+
+// The SH coefficients (as given) of the visible rows: one warp per row, lane k
+// updating coefficients k, k + 32, ... (coalesced), the visible test uniform over
+// the warp.
+__global__ void adam_sh_kernel(fgs_adam_args a, const uint8_t* __restrict__ flag, const int* __restrict__ step)
+{
+    const AdamCoef c = adam_coef(a, *step);
+    const float ss = (float)(a.lr[1] / c.bc1);
+    const int F = 3 * a.M, lane = threadIdx.x & 31;
+    const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < a.P; i += nwarps) {
+        if (!flag[i]) continue;
+        for (int k = lane; k < F; k += 32) {
+            const size_t j = (size_t)F * i + k;
+            adam_update(a.shs[j], a.m_shs[j], a.v_shs[j], a.g_shs[j], c.b1, c.omb1, c.b2, c.omb2, ss, c.bc2s,
+                        c.eps);
+        }
+    }
+}
+
+// Everything but the SH coefficients, one thread per row.
 __global__ void adam_kernel(fgs_adam_args a, const uint8_t* __restrict__ flag, const int* __restrict__ step)
 {
-    const int t = *step;
-    const double bc1 = 1.0 - pow(a.beta1, (double)t);
-    const double bc2 = 1.0 - pow(a.beta2, (double)t);
-    const float bc2s = (float)sqrt(bc2);
-    const float b1 = (float)a.beta1, b2 = (float)a.beta2, eps = a.eps;
-    const float omb1 = (float)(1.0 - a.beta1), omb2 = (float)(1.0 - a.beta2);
-    const int F = 3 * a.M;
+    const AdamCoef c = adam_coef(a, *step);
+    const double bc1 = c.bc1;
+    const float bc2s = c.bc2s, b1 = c.b1, b2 = c.b2, omb1 = c.omb1, omb2 = c.omb2, eps = c.eps;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.P; i += gridDim.x * blockDim.x) {
         if (!flag[i]) continue;
         // means (as given)
@@ -290,14 +326,6 @@ __global__ void adam_kernel(fgs_adam_args a, const uint8_t* __restrict__ flag, c
             for (int k = 0; k < 3; k++) {
                 const size_t j = 3 * (size_t)i + k;
                 adam_update(a.xyz[j], a.m_xyz[j], a.v_xyz[j], a.g_xyz[j], b1, omb1, b2, omb2, ss, bc2s, eps);
-            }
-        }
-        // SH coefficients (as given)
-        if (a.shs) {
-            const float ss = (float)(a.lr[1] / bc1);
-            for (int k = 0; k < F; k++) {
-                const size_t j = (size_t)F * i + k;
-                adam_update(a.shs[j], a.m_shs[j], a.v_shs[j], a.g_shs[j], b1, omb1, b2, omb2, ss, bc2s, eps);
             }
         }
         // opacity: d/dlogit = d/dopacity * s (1 - s)
@@ -430,9 +458,16 @@ int fgs_adam_step(const fgs_adam_args* a, const unsigned char* flag, int* step, 
     if (!a->xyz || !a->opac_logit || !a->log_scale || !a->rot_raw || !a->opac || !a->scale || !a->rot) return FGS_ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     step_tick_kernel<<<1, 1, 0, s>>>(step);
-    if (a->P > 0)
+    int n = 1;
+    if (a->P > 0) {
         adam_kernel<<<(a->P + 255) / 256 < 4096 ? (a->P + 255) / 256 : 4096, 256, 0, s>>>(*a, flag, step);
-    note_launches(2);
+        n++;
+        if (a->shs && a->M > 0) {
+            adam_sh_kernel<<<(a->P + 7) / 8 < 4096 ? (a->P + 7) / 8 : 4096, 256, 0, s>>>(*a, flag, step);
+            n++;
+        }
+    }
+    note_launches(n);
     return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
 }
 
