@@ -48,11 +48,32 @@ class TreeScene:
         self.roots = t(roots, torch.int32)
         self.sh_degree = int(sh_degree)
         self.P = int(self.xyz.shape[0])
+        self.cut_levels = _frontier_levels(self.roots, self.node_index, self.tree)
 
     @classmethod
     def from_arrays(cls, d, device="cuda"):
         return cls(d["xyz"], d["log_scales"], d["rotations"], d["opacity_raw"], d["features_dc"], d.get("shs_rest"),
                    d["node_index"], d["ancestor_path"], d["tree"], d["roots"], sh_degree=1, device=device)
+
+
+def _frontier_levels(roots, node_index, tree, cap=30):
+    """Non-empty frontiers of a level-by-level walk from the roots through every child (at most
+    cap): a LoG cut never needs more levels, whatever the radii, since its frontiers are subsets
+    of these and a level with an empty frontier changes nothing."""
+    P = int(node_index.numel())
+    rows = int(tree.shape[0]) if tree.dim() >= 1 else 0
+    f = roots.long()
+    levels = 0
+    while levels < cap:
+        f = f[(f >= 0) & (f < P)]
+        if f.numel() == 0:
+            break
+        levels += 1
+        ni = node_index[f].long()
+        ni = ni[(ni >= 0) & (ni < rows)]
+        ch = tree[ni].reshape(-1).long()
+        f = ch[ch >= 0]
+    return levels
 
 
 def _focal(cam):
@@ -90,7 +111,10 @@ def node_radius(scene, view, proj, cam):
 
 
 def log_cut(scene, radius, min_resolution_pixel=1.5, levels=30):
-    """TensorTree.traverse order on the device -> (ids int32 buffer [P], count int32 [1] on device)."""
+    """TensorTree.traverse order on the device -> (ids int32 buffer [P], count int32 [1] on device).
+    levels caps the walk as traverse's 30 does; the tree's own depth caps it further (the levels
+    past it find an empty frontier)."""
+    levels = min(int(levels), getattr(scene, "cut_levels", int(levels)))
     dev = scene.xyz.device
     P = scene.P
     mc = int(scene.tree.shape[1]) if scene.tree.dim() == 2 else 1
