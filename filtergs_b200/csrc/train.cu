@@ -34,26 +34,33 @@ struct Window {
 };
 
 // ---------------------------------------------------------------- SSIM forward + coefficient maps
-// One CTA: a kTX x kTY tile of valid outputs of one channel.  The input tile with
-// its halo is staged in shared memory, the 11-tap Gaussian is applied along rows,
-// then along columns (separable) to x, y, x^2, y^2 and x*y.  Per output q the loss
-// gradient w.r.t. the five local means is kept as three maps (d/dmu_x, d/dE[x^2],
-// d/dE[xy]); the SSIM values of the tile are summed in a fixed order.
-__global__ void __launch_bounds__(kTX* kTY)
+// One CTA: a kTX x kTY tile of valid outputs of one channel, kTX x kTY / kRowsPer
+// threads.  The input tile with its halo is staged in shared memory, the 11-tap
+// Gaussian is applied along rows, then along columns (separable) to x, y, x^2, y^2
+// and x*y, each pass from a sliding window in registers (a row item makes kSeg
+// outputs from kSeg + 10 loaded values, a thread kRowsPer outputs of one column from
+// kRowsPer + 10), every output summing its taps in window order.  Per output q the
+// loss gradient w.r.t. the five local means is kept as three maps (d/dmu_x,
+// d/dE[x^2], d/dE[xy]); the SSIM values of the tile are summed in a fixed order.
+constexpr int kRowsPer = 4;                       // outputs of one column per thread
+constexpr int kLossThreads = kTX * kTY / kRowsPer;
+constexpr int kSeg = 8;                           // outputs of one row per row-pass item
+
+__global__ void __launch_bounds__(kLossThreads)
     ssim_forward_kernel(int W, int H, const float* __restrict__ pred, const float* __restrict__ target, Window win,
                         float ssim_grad_scale, float* __restrict__ gmap, float* __restrict__ partial)
 {
     __shared__ float sx[kTY + kHalo][kTX + kHalo + 1];
     __shared__ float sy[kTY + kHalo][kTX + kHalo + 1];
     __shared__ float hq[5][kTY + kHalo][kTX];
-    __shared__ float red[kTX * kTY / 32];
+    __shared__ float red[kLossThreads / 32];
     const int Wo = W - kHalo, Ho = H - kHalo;
     const int c = blockIdx.z;
     const int ox0 = blockIdx.x * kTX, oy0 = blockIdx.y * kTY;
     const float* x = pred + (size_t)c * W * H;
     const float* y = target + (size_t)c * W * H;
     const int tid = threadIdx.x;
-    for (int i = tid; i < (kTY + kHalo) * (kTX + kHalo); i += kTX * kTY) {
+    for (int i = tid; i < (kTY + kHalo) * (kTX + kHalo); i += kLossThreads) {
         const int r = i / (kTX + kHalo), cc = i % (kTX + kHalo);
         const int gy = oy0 + r, gx = ox0 + cc;
         const bool in = gy < H && gx < W;
@@ -61,47 +68,69 @@ __global__ void __launch_bounds__(kTX* kTY)
         sy[r][cc] = in ? __ldg(y + (size_t)gy * W + gx) : 0.f;
     }
     __syncthreads();
-    for (int i = tid; i < (kTY + kHalo) * kTX; i += kTX * kTY) {
-        const int r = i / kTX, cc = i % kTX;
-        float a = 0.f, b = 0.f, aa = 0.f, bb = 0.f, ab = 0.f;
+    for (int i = tid; i < (kTY + kHalo) * (kTX / kSeg); i += kLossThreads) {
+        const int r = i / (kTX / kSeg), c0 = (i % (kTX / kSeg)) * kSeg;
+        float u[kSeg + kHalo], v[kSeg + kHalo];
 #pragma unroll
-        for (int j = 0; j < kWin; j++) {
-            const float u = sx[r][cc + j], v = sy[r][cc + j], w = win.g[j];
-            a += w * u;
-            b += w * v;
-            aa += w * (u * u);
-            bb += w * (v * v);
-            ab += w * (u * v);
+        for (int k = 0; k < kSeg + kHalo; k++) {
+            u[k] = sx[r][c0 + k];
+            v[k] = sy[r][c0 + k];
         }
-        hq[0][r][cc] = a; hq[1][r][cc] = b; hq[2][r][cc] = aa; hq[3][r][cc] = bb; hq[4][r][cc] = ab;
+#pragma unroll
+        for (int k = 0; k < kSeg; k++) {
+            float a = 0.f, b = 0.f, aa = 0.f, bb = 0.f, ab = 0.f;
+#pragma unroll
+            for (int j = 0; j < kWin; j++) {
+                const float uu = u[k + j], vv = v[k + j], w = win.g[j];
+                a += w * uu;
+                b += w * vv;
+                aa += w * (uu * uu);
+                bb += w * (vv * vv);
+                ab += w * (uu * vv);
+            }
+            hq[0][r][c0 + k] = a; hq[1][r][c0 + k] = b; hq[2][r][c0 + k] = aa; hq[3][r][c0 + k] = bb;
+            hq[4][r][c0 + k] = ab;
+        }
     }
     __syncthreads();
-    const int tx = tid % kTX, ty = tid / kTX;
-    const int ox = ox0 + tx, oy = oy0 + ty;
-    float s = 0.f;
-    if (ox < Wo && oy < Ho) {
-        float m[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+    const int tx = tid % kTX, ty0 = (tid / kTX) * kRowsPer;
+    float m[kRowsPer][5];
 #pragma unroll
-        for (int i = 0; i < kWin; i++) {
-            const float w = win.g[i];
+    for (int q = 0; q < 5; q++) {
+        float col[kRowsPer + kHalo];
 #pragma unroll
-            for (int q = 0; q < 5; q++) m[q] += w * hq[q][ty + i][tx];
+        for (int k = 0; k < kRowsPer + kHalo; k++) col[k] = hq[q][ty0 + k][tx];
+#pragma unroll
+        for (int rr = 0; rr < kRowsPer; rr++) {
+            float acc = 0.f;
+#pragma unroll
+            for (int i = 0; i < kWin; i++) acc += win.g[i] * col[rr + i];
+            m[rr][q] = acc;
         }
-        const float m1 = m[0], m2 = m[1];
-        const float s11 = m[2] - m1 * m1, s22 = m[3] - m2 * m2, s12 = m[4] - m1 * m2;
-        const float A = 2.f * m1 * m2 + kC1, B = 2.f * s12 + kC2;
-        const float Cc = m1 * m1 + m2 * m2 + kC1, D = s11 + s22 + kC2;
-        const float CD = Cc * D;
-        s = (A * B) / CD;
-        // d ssim / d(mu_x, E[x^2], E[xy]); the loss is 0.2 (1 - mean ssim): scale by -ssim_grad_scale
-        const float d_m1 = (2.f * m2 * B - 2.f * m2 * A) / CD - s * (2.f * m1 / Cc - 2.f * m1 / D);
-        const float d_e11 = -s / D;
-        const float d_e12 = 2.f * A / CD;
-        const size_t plane = (size_t)Wo * Ho, o = (size_t)oy * Wo + ox;
-        float* gm = gmap + (size_t)c * 3 * plane;
-        gm[o] = -ssim_grad_scale * d_m1;
-        gm[plane + o] = -ssim_grad_scale * d_e11;
-        gm[2 * plane + o] = -ssim_grad_scale * d_e12;
+    }
+    float s = 0.f;
+    const size_t plane = (size_t)Wo * Ho;
+    float* gm = gmap + (size_t)c * 3 * plane;
+#pragma unroll
+    for (int rr = 0; rr < kRowsPer; rr++) {
+        const int ox = ox0 + tx, oy = oy0 + ty0 + rr;
+        if (ox < Wo && oy < Ho) {
+            const float m1 = m[rr][0], m2 = m[rr][1];
+            const float s11 = m[rr][2] - m1 * m1, s22 = m[rr][3] - m2 * m2, s12 = m[rr][4] - m1 * m2;
+            const float A = 2.f * m1 * m2 + kC1, B = 2.f * s12 + kC2;
+            const float Cc = m1 * m1 + m2 * m2 + kC1, D = s11 + s22 + kC2;
+            const float CD = Cc * D;
+            const float ss = (A * B) / CD;
+            // d ssim / d(mu_x, E[x^2], E[xy]); the loss is 0.2 (1 - mean ssim): scale by -ssim_grad_scale
+            const float d_m1 = (2.f * m2 * B - 2.f * m2 * A) / CD - ss * (2.f * m1 / Cc - 2.f * m1 / D);
+            const float d_e11 = -ss / D;
+            const float d_e12 = 2.f * A / CD;
+            const size_t o = (size_t)oy * Wo + ox;
+            gm[o] = -ssim_grad_scale * d_m1;
+            gm[plane + o] = -ssim_grad_scale * d_e11;
+            gm[2 * plane + o] = -ssim_grad_scale * d_e12;
+            s += ss;
+        }
     }
     // fixed-order block sum of the tile's SSIM values
 #pragma unroll
@@ -110,7 +139,7 @@ __global__ void __launch_bounds__(kTX* kTY)
     __syncthreads();
     if (tid == 0) {
         float t = 0.f;
-        for (int w = 0; w < kTX * kTY / 32; w++) t += red[w];
+        for (int w = 0; w < kLossThreads / 32; w++) t += red[w];
         partial[((size_t)c * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
     }
 }
@@ -119,15 +148,16 @@ __global__ void __launch_bounds__(kTX* kTY)
 // dL/dx_p = sum over the outputs q whose window covers p of w(q, p) *
 // (G1(q) + 2 x_p G11(q) + y_p G12(q)), a transposed separable convolution of the
 // three coefficient maps, plus the L1 term w_l1 * sign(x_p - y_p).  One CTA: a
-// kTX x kTY pixel tile of one channel; also sums |x - y| over the tile.
-__global__ void __launch_bounds__(kTX* kTY)
+// kTX x kTY pixel tile of one channel, the two passes from sliding windows in
+// registers as in ssim_forward_kernel; also sums |x - y| over the tile.
+__global__ void __launch_bounds__(kLossThreads)
     loss_grad_kernel(int W, int H, const float* __restrict__ pred, const float* __restrict__ target, Window win,
                      const float* __restrict__ gmap, float l1_grad_scale, float* __restrict__ dpred,
                      float* __restrict__ partial)
 {
     __shared__ float sg[3][kTY + kHalo][kTX + kHalo + 1];
     __shared__ float hv[3][kTY + kHalo][kTX];
-    __shared__ float red[kTX * kTY / 32];
+    __shared__ float red[kLossThreads / 32];
     const int Wo = W - kHalo, Ho = H - kHalo;
     const int c = blockIdx.z;
     const int px0 = blockIdx.x * kTX, py0 = blockIdx.y * kTY;
@@ -135,7 +165,7 @@ __global__ void __launch_bounds__(kTX* kTY)
     const float* gm = gmap + (size_t)c * 3 * plane;
     const int tid = threadIdx.x;
     // outputs q in [p - kHalo, p]: rows py0 - kHalo .. py0 + kTY - 1
-    for (int i = tid; i < (kTY + kHalo) * (kTX + kHalo); i += kTX * kTY) {
+    for (int i = tid; i < (kTY + kHalo) * (kTX + kHalo); i += kLossThreads) {
         const int r = i / (kTX + kHalo), cc = i % (kTX + kHalo);
         const int qy = py0 - kHalo + r, qx = px0 - kHalo + cc;
         const bool in = qy >= 0 && qx >= 0 && qy < Ho && qx < Wo;
@@ -144,38 +174,51 @@ __global__ void __launch_bounds__(kTX* kTY)
         for (int k = 0; k < 3; k++) sg[k][r][cc] = in ? __ldg(gm + k * plane + o) : 0.f;
     }
     __syncthreads();
-    // along rows: T(r, p) = sum_j g_j G(r, p - j)
-    for (int i = tid; i < (kTY + kHalo) * kTX; i += kTX * kTY) {
-        const int r = i / kTX, cc = i % kTX;
-        float t0 = 0.f, t1 = 0.f, t2 = 0.f;
+    // along rows: T(r, p) = sum_j g_j G(r, p - j), window sg[r][c0 .. c0 + kSeg + kHalo)
+    for (int i = tid; i < (kTY + kHalo) * (kTX / kSeg); i += kLossThreads) {
+        const int r = i / (kTX / kSeg), c0 = (i % (kTX / kSeg)) * kSeg;
 #pragma unroll
-        for (int j = 0; j < kWin; j++) {
-            const float w = win.g[j];
-            t0 += w * sg[0][r][cc + kHalo - j];
-            t1 += w * sg[1][r][cc + kHalo - j];
-            t2 += w * sg[2][r][cc + kHalo - j];
+        for (int k = 0; k < 3; k++) {
+            float g[kSeg + kHalo];
+#pragma unroll
+            for (int e = 0; e < kSeg + kHalo; e++) g[e] = sg[k][r][c0 + e];
+#pragma unroll
+            for (int kk = 0; kk < kSeg; kk++) {
+                float t = 0.f;
+#pragma unroll
+                for (int jj = 0; jj < kWin; jj++) t += win.g[jj] * g[kk + kHalo - jj];
+                hv[k][r][c0 + kk] = t;
+            }
         }
-        hv[0][r][cc] = t0; hv[1][r][cc] = t1; hv[2][r][cc] = t2;
     }
     __syncthreads();
-    const int tx = tid % kTX, ty = tid / kTX;
-    const int px = px0 + tx, py = py0 + ty;
-    float l1 = 0.f;
-    if (px < W && py < H) {
-        float s1 = 0.f, s11 = 0.f, s12 = 0.f;
+    const int tx = tid % kTX, ty0 = (tid / kTX) * kRowsPer;
+    float sv[kRowsPer][3];
 #pragma unroll
-        for (int i = 0; i < kWin; i++) {
-            const float w = win.g[i];
-            s1 += w * hv[0][ty + kHalo - i][tx];
-            s11 += w * hv[1][ty + kHalo - i][tx];
-            s12 += w * hv[2][ty + kHalo - i][tx];
+    for (int k = 0; k < 3; k++) {
+        float col[kRowsPer + kHalo];
+#pragma unroll
+        for (int e = 0; e < kRowsPer + kHalo; e++) col[e] = hv[k][ty0 + e][tx];
+#pragma unroll
+        for (int rr = 0; rr < kRowsPer; rr++) {
+            float acc = 0.f;
+#pragma unroll
+            for (int ii = 0; ii < kWin; ii++) acc += win.g[ii] * col[rr + kHalo - ii];
+            sv[rr][k] = acc;
         }
-        const size_t o = (size_t)c * W * H + (size_t)py * W + px;
-        const float xv = __ldg(pred + o), yv = __ldg(target + o);
-        const float d = xv - yv;
-        const float sgn = d > 0.f ? 1.f : (d < 0.f ? -1.f : 0.f);
-        dpred[o] = s1 + 2.f * xv * s11 + yv * s12 + l1_grad_scale * sgn;
-        l1 = fabsf(d);
+    }
+    float l1 = 0.f;
+#pragma unroll
+    for (int rr = 0; rr < kRowsPer; rr++) {
+        const int px = px0 + tx, py = py0 + ty0 + rr;
+        if (px < W && py < H) {
+            const size_t o = (size_t)c * W * H + (size_t)py * W + px;
+            const float xv = __ldg(pred + o), yv = __ldg(target + o);
+            const float d = xv - yv;
+            const float sgn = d > 0.f ? 1.f : (d < 0.f ? -1.f : 0.f);
+            dpred[o] = sv[rr][0] + 2.f * xv * sv[rr][1] + yv * sv[rr][2] + l1_grad_scale * sgn;
+            l1 += fabsf(d);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) l1 += __shfl_xor_sync(0xffffffffu, l1, o);
@@ -183,7 +226,7 @@ __global__ void __launch_bounds__(kTX* kTY)
     __syncthreads();
     if (tid == 0) {
         float t = 0.f;
-        for (int w = 0; w < kTX * kTY / 32; w++) t += red[w];
+        for (int w = 0; w < kLossThreads / 32; w++) t += red[w];
         partial[((size_t)c * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = t;
     }
 }
@@ -423,8 +466,9 @@ int fgs_loss_l1_ssim(int width, int height, const float* pred, const float* targ
     float* sp = gmap + (size_t)9 * Wo * Ho;
     float* l1p = sp + (size_t)go.x * go.y * go.z;
     static const Window win = make_window();
-    ssim_forward_kernel<<<go, kTX * kTY, 0, s>>>(width, height, pred, target, win, ssim_grad_scale, gmap, sp);
-    loss_grad_kernel<<<gp, kTX * kTY, 0, s>>>(width, height, pred, target, win, gmap, l1_grad_scale, dL_dpred, l1p);
+    ssim_forward_kernel<<<go, kLossThreads, 0, s>>>(width, height, pred, target, win, ssim_grad_scale, gmap, sp);
+    loss_grad_kernel<<<gp, kLossThreads, 0, s>>>(width, height, pred, target, win, gmap, l1_grad_scale, dL_dpred,
+                                                 l1p);
     loss_reduce_kernel<<<1, 1024, 0, s>>>(l1p, (int)(gp.x * gp.y * gp.z), sp, (int)(go.x * go.y * go.z), sums);
     note_launches(3);
     return cudaGetLastError() == cudaSuccess ? FGS_OK : FGS_ERR_CUDA;
