@@ -5,7 +5,10 @@ backward with the views' gradients summed into shared dense buffers.  The
 per-view front end keeps its pair counts on the device and compositing is
 one persistent launch per direction over all views' tiles (C ABI
 fgs_batch_*), so a whole forward + backward step has no host
-synchronisation and is captured once into a CUDA graph and replayed.
+synchronisation and is captured once into two CUDA graphs (forward, backward)
+and replayed; `step()` can mark the end of the forward with an event and hold
+the backward on another, so callers overlap image downloads and gradient
+uploads with compute.
 
 Pair capacities are planned from the views' exact pair counts (one plain
 preprocess per view) with headroom; a replay that overflows a capacity is
@@ -83,7 +86,7 @@ class BatchedRasterizer:
                          rotations=torch.zeros(self.P, 4, device=dev))
         self.use_graph = graph
         self.handle = None
-        self.graph = None
+        self.graph = None      # (forward graph, backward graph) once captured
         self.capacity = self._plan_capacity()
         self._build()
 
@@ -153,10 +156,13 @@ class BatchedRasterizer:
             self._enqueue(L, s)
         torch.cuda.current_stream(self.dev).wait_stream(s)
         torch.cuda.synchronize(self.dev)
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, stream=s):
-            self._enqueue(L, s)
-        self.graph = g
+        gf, gb = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        ptr = C.c_void_p(s.cuda_stream)
+        with torch.cuda.graph(gf, stream=s):
+            _lib.check(L.fgs_batch_forward(self.handle, ptr), "fgs_batch_forward")
+        with torch.cuda.graph(gb, stream=s):
+            _lib.check(L.fgs_batch_backward(self.handle, ptr), "fgs_batch_backward")
+        self.graph = (gf, gb)
 
     def _enqueue(self, L, s):
         ptr = C.c_void_p(s.cuda_stream)
@@ -164,14 +170,27 @@ class BatchedRasterizer:
         _lib.check(L.fgs_batch_backward(self.handle, ptr), "fgs_batch_backward")
 
     # ------------------------------------------------------------------ use
-    def step(self):
-        """One forward + backward of all views (graph replay when enabled)."""
+    def step(self, forward_done=None, backward_ready=None):
+        """One forward + backward of all views (graph replays when enabled), on the current stream.
+        forward_done (a torch.cuda.Event) is recorded once the images are final, so that a copy
+        stream can download them while the backward runs; the backward waits for backward_ready
+        when given (e.g. the upload of the upstream gradients, which the forward does not read)."""
+        s = torch.cuda.current_stream(self.dev)
+        L = _L()
         if self.use_graph:
             if self.graph is None:
                 self._capture()
-            self.graph.replay()
+            self.graph[0].replay()
         else:
-            self._enqueue(_L(), torch.cuda.current_stream(self.dev))
+            _lib.check(L.fgs_batch_forward(self.handle, C.c_void_p(s.cuda_stream)), "fgs_batch_forward")
+        if forward_done is not None:
+            forward_done.record(s)
+        if backward_ready is not None:
+            s.wait_event(backward_ready)
+        if self.use_graph:
+            self.graph[1].replay()
+        else:
+            _lib.check(L.fgs_batch_backward(self.handle, C.c_void_p(s.cuda_stream)), "fgs_batch_backward")
 
     def forward(self):
         _lib.check(_L().fgs_batch_forward(self.handle, _s()), "fgs_batch_forward")
