@@ -201,3 +201,46 @@ def test_batched_full_forward_outputs_match_plain(cuda):
         assert torch.equal(br.point_id[v], f[2]), v
         assert torch.equal(br.point_weight_pixel[v], f[3]), v
         assert torch.equal(br.point_weight[v], f[4]), v
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_step_events_overlap_copies(cuda, graph):
+    """step(forward_done=, backward_ready=): the images are final when forward_done fires (a copy
+    stream that waits for it reads the finished images while the backward runs), the backward waits
+    for backward_ready (the upstream gradients written on another stream), and the results equal a
+    plain step()'s."""
+    sc = _scene(P=150_000, seed=5021)
+    cams = _cams(3, seed=5022)
+    bg = torch.zeros(3, device="cuda")
+    br = BatchedRasterizer(sc["means3D"], sc["opacities"], sc["scales"], sc["rotations"], cams, shs=sc["shs"],
+                           sh_degree=3, bg=bg, graph=graph)
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    dls = [torch.randn(d.shape, device="cuda", generator=gen) for d in br.dL]
+    for v, d in enumerate(dls):
+        br.dL[v].copy_(d)
+    br.step()
+    br.check()
+    torch.cuda.synchronize()
+    want_img = [im.clone() for im in br.images]
+    want_grad = {k: g.clone() for k, g in br.grad.items()}
+    # the same step with the upstream gradients written on a side stream after the forward started
+    for d in br.dL:
+        d.zero_()
+    side, copy = torch.cuda.Stream(), torch.cuda.Stream()
+    fwd_done, dl_ready = torch.cuda.Event(), torch.cuda.Event()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for v, d in enumerate(dls):
+            br.dL[v].copy_(d)
+        dl_ready.record(side)
+    br.step(forward_done=fwd_done, backward_ready=dl_ready)
+    copy.wait_event(fwd_done)
+    with torch.cuda.stream(copy):
+        got_img = [im.clone() for im in br.images]
+    torch.cuda.synchronize()
+    br.check()
+    assert fwd_done.query() and dl_ready.query()
+    for x, y in zip(got_img, want_img):
+        assert torch.equal(x, y)
+    for k in want_grad:
+        assert torch.equal(br.grad[k], want_grad[k]), k
