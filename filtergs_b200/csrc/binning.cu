@@ -26,7 +26,7 @@ namespace {
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;                        // keys per thread, at most
-constexpr int kSortItemsMin = 4;                      // keys per thread, at least
+constexpr int kSortItemsMin = 8;                      // keys per thread, at least
 constexpr int kSortTile = kSortThreads * kSortItems;  // largest chunk
 constexpr int kSortTileMin = kSortThreads * kSortItemsMin;
 constexpr int kRadix = 256;
