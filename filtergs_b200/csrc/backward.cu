@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(256, 4)
         e1 = max(e0, min(jj + 1 < V ? __ldg(pair_off + jj + 1) : K, rows));
         idx = (int)__ldg(visible_ids + jj);
     };
-    // sum of rows [e0, e1) on lanes 2q and 2q+1 (component q): 32 rows at a time in
+    // sum of rows [e0, e1), component sum9_component(lane) on each lane: 32 rows at a time in
     // emission order, each group through the same shuffle tree, added to 0 in turn
     auto sum_rows = [&](uint32_t e0, uint32_t e1) {
         const uint32_t ne = e1 - e0;
@@ -191,8 +191,8 @@ __global__ void __launch_bounds__(256, 4)
     };
     auto store = [&](int idx, float acc) {
         if (vis && lane == 0) atomicOr(vis + idx, vis_bit);  // this view sees Gaussian idx
-        if (lane < 18 && !(lane & 1)) {
-            const int q = lane >> 1;
+        const int q = sum9_component(lane);
+        if (q < 9 && !(lane & 1)) {
             float* dst = q < 3 ? dcolor + 3 * idx + q
                        : q < 5 ? dmean2D + 3 * idx + (q - 3)
                        : q == 7 ? dconic + 4 * idx + 3

@@ -265,36 +265,44 @@ __device__ __forceinline__ float3 ewa_cov2d_ref(const float3& mean, float fx, fl
 __device__ __forceinline__ float dilate_max(float c) { return (float)fmax((double)c, 0.3); }
 __device__ __forceinline__ float dilate_add(float c) { return (float)((double)c + 0.3); }
 
-// Reduce 9 per-lane values over the warp with 16 shuffles instead of 45:
-// a butterfly in which each level halves the values a lane keeps (the rest
-// go to the partner lane).  Lanes 2s and 2s+1 end with the warp total of
-// value s (s < 9; padded to 16 slots).
+// One level of warp_transpose_sum9: lanes with bit `o` clear keep values
+// [0, M) of the N they hold, the others keep [M, N) (padded with zeros to M),
+// each adding the partner lane's copy of what it keeps.
+template <int M, int N>
+__device__ __forceinline__ void sum9_level(const float (&in)[N], float (&out)[M], unsigned lane, int o)
+{
+    const bool hi = lane & o;
+#pragma unroll
+    for (int i = 0; i < M; i++) {
+        const float lo_v = in[i];
+        const float hi_v = i + M < N ? in[i + M] : 0.f;
+        const float send = hi ? lo_v : hi_v;
+        const float keep = hi ? hi_v : lo_v;
+        out[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+}
+
+// Reduce 9 per-lane values over the warp with 12 shuffles instead of 45: a
+// butterfly in which each level splits the values a lane holds as evenly as
+// it can (9 -> 5/4 -> 3/2 -> 2/1 -> 1) and sends the other part to the partner
+// lane, then one plain butterfly step.  Lanes 2s and 2s+1 end with the warp
+// total of value sum9_component(2s) (values past 8 are padding).
 __device__ __forceinline__ float warp_transpose_sum9(const float (&g)[9])
 {
     const unsigned lane = threadIdx.x & 31;
-    float v[8];
-    {
-        const bool hi = lane & 16;
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const float lo_v = g[i];
-            const float hi_v = (i + 8 < 9) ? g[i + 8] : 0.f;
-            const float send = hi ? lo_v : hi_v;
-            const float keep = hi ? hi_v : lo_v;
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-        }
-    }
-#pragma unroll
-    for (int w = 4, o = 8; w >= 1; w >>= 1, o >>= 1) {
-        const bool hi = lane & o;
-#pragma unroll
-        for (int i = 0; i < w; i++) {
-            const float send = hi ? v[i] : v[i + w];
-            const float keep = hi ? v[i + w] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
-        }
-    }
-    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+    float v5[5], v3[3], v2[2], v1[1];
+    sum9_level<5, 9>(g, v5, lane, 16);
+    sum9_level<3, 5>(v5, v3, lane, 8);
+    sum9_level<2, 3>(v3, v2, lane, 4);
+    sum9_level<1, 2>(v2, v1, lane, 2);
+    return v1[0] + __shfl_xor_sync(0xffffffffu, v1[0], 1);
+}
+
+// Which of the nine values warp_transpose_sum9 leaves on `lane` (15: padding).
+// Lane bits 4, 3, 2, 1 pick offsets 5, 3, 2, 1 inside the split at that level.
+__device__ __forceinline__ int sum9_component(unsigned lane)
+{
+    return (int)((0xfff8f765ff43f210ull >> (4 * ((lane & 31) >> 1))) & 15u);
 }
 
 // ---------------------------------------------------------------- SH (forward.cu:48-99)

@@ -867,11 +867,11 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
     const float ry0 = (float)(by * kTileY + (tid >> 5) * 2 * PPT), ry1 = ry0 + (2 * PPT - 1);
     const float ddelx_dx = 0.5 * W;
     const float ddely_dy = 0.5 * H;
-    // The per-pixel loop sums the mean and conic gradients without their constant
-    // factors (-W/2, -H/2 and -1/2, backward.cu:545-551); each warp total is scaled
-    // once, on the lanes that hold it (value q on lanes 2q and 2q+1).
-    const unsigned q_lane = (tid & 31) >> 1;
-    const float gscale = q_lane == 3 ? -ddelx_dx : (q_lane == 4 ? -ddely_dy : (q_lane >= 5 && q_lane <= 7 ? -0.5f : 1.f));
+    // The per-pixel loop sums w = G dL/dalpha and its products with dx, dy; the
+    // factors common to all of a pair's pixels (opacity, conic, -W/2, -H/2, -1/2 of
+    // backward.cu:537-551) are applied once per pair when the batch is flushed.
+    // Each warp total sits on the lanes of its component.
+    const int q_lane = (tid & 1) ? 15 : sum9_component((unsigned)tid);
 
     if (tid == 0) sm.max_last = 0;
     __syncthreads();
@@ -947,30 +947,30 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
                     // background term; exactly zero (and skipped) for a black background
                     if (bgT[k] != 0.f) dL_dalpha += bgT[k] * inv_1ma;
                     if (kConsistent && oG > 0.99f) dL_dalpha = 0.f;
-                    // s = G dL/dG; the sums below, times gscale, are dL/dmean2D
-                    // (G (a dx + b dy), G (b dx + c dy)) and dL/dconic (G dx dx, G dx dy,
-                    // G dy dy) of the reference's atomics
-                    const float s = G * (rb.y * dL_dalpha);
-                    const float u = s * dx, v = s * dy;
-                    gr[3] += u * ra.z + v * ra.w;
-                    gr[4] += v * rb.x + u * ra.w;
+                    // w = G dL/dalpha = dL/dopacity; w dx and w dy give dL/dmean2D,
+                    // w dx dx, w dx dy and w dy dy dL/dconic (times the pair's factors)
+                    const float w = G * dL_dalpha;
+                    const float u = w * dx, v = w * dy;
+                    gr[3] += u;
+                    gr[4] += v;
                     gr[5] += u * dx;
                     gr[6] += u * dy;
                     gr[7] += v * dy;
-                    gr[8] += G * dL_dalpha;
+                    gr[8] += w;
                     any = true;
                 }
                 if (__any_sync(0xffffffffu, any)) {
-                    const float tot = warp_transpose_sum9(gr) * gscale;
-                    const unsigned lane = tid & 31;
-                    if (!(lane & 1) && (lane >> 1) < NG) atomicAdd(&sm.acc[(tid >> 5) >> 1][lane >> 1][j], tot);
+                    const float tot = warp_transpose_sum9(gr);
+                    if (q_lane < NG) atomicAdd(&sm.acc[(tid >> 5) >> 1][q_lane][j], tot);
                 }
             }
         }
         __syncthreads();
-        // this batch's per-pair gradients, at each pair's emission index
+        // this batch's per-pair gradients, at each pair's emission index: the slot
+        // sums times the pair's own factors
         for (uint32_t e = tid; e < cnt; e += NT) {
             float* dst = a.pgrad + (size_t)__float_as_uint(R[e].c.w) * NG;
+            float sum[NG];
 #pragma unroll
             for (int q = 0; q < NG; q++) {
                 float v = 0.f;
@@ -979,8 +979,19 @@ __device__ __forceinline__ void render_bwd_tile(BwdSmem<kBatch, bwd_slots<PPT>()
                     v += sm.acc[sl][q][e];
                     sm.acc[sl][q][e] = 0.f;
                 }
-                dst[q] = v;
+                sum[q] = v;
             }
+            const float4 ea = R[e].a, eb = R[e].b;  // conic (ea.z, ea.w, eb.x), opacity eb.y
+            const float o = eb.y;
+            dst[0] = sum[0];
+            dst[1] = sum[1];
+            dst[2] = sum[2];
+            dst[3] = -ddelx_dx * (o * (ea.z * sum[3] + ea.w * sum[4]));
+            dst[4] = -ddely_dy * (o * (eb.x * sum[4] + ea.w * sum[3]));
+            dst[5] = -0.5f * (o * sum[5]);
+            dst[6] = -0.5f * (o * sum[6]);
+            dst[7] = -0.5f * (o * sum[7]);
+            dst[8] = sum[8];
         }
         if (tid == 0 && b + 2 < nb) {
             const int nbuf = (int)((g + 2) % kBufs);
