@@ -480,8 +480,14 @@ def measure_batched(args, scene, views, bg, dev, dist, rank, clocks=None, profil
 
 
 def roofline(prof, P, views, K, vis, batched):
-    """Roofline of the dominant kernel: algorithmic bytes per launch / its mean CUDA-event duration."""
-    dom = max(prof, key=lambda k: prof[k][0])
+    """Roofline of the dominant kernel: algorithmic bytes per launch / its mean CUDA-event duration.
+
+    In the batched path the per-view front-end stages (preprocess, sorts, pair emission, ranges) run
+    on concurrent streams, so their event times overlap one another and their sums overstate their
+    device time; the dominant kernel is then taken among the launches that have the device to
+    themselves, which is also the ranking of the serialised ncu launch list."""
+    alone = [k for k in prof if not batched or k in ("render_fwd", "render_bwd", "preprocess_bwd")]
+    dom = max(alone or list(prof), key=lambda k: prof[k][0])
     calls = max(1, prof[dom][1])
     per_call_ms = prof[dom][0] / calls
 
