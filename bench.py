@@ -236,7 +236,7 @@ def algo_bytes(stage, P, V, K, N, T, M=16, tile_passes=2):
     if stage == "render_fwd":
         return 40 * K + 28 * N
     if stage == "render_bwd":
-        # the survey's algorithmic bytes: records 40 B per pair; dL/dpix, T, n_contrib per pixel; the 44-byte
+        # the algorithm's own bytes: records 40 B per pair; dL/dpix, T, n_contrib per pixel; the 44-byte
         # screen-space gradient accumulators written once per visible Gaussian
         return 40 * K + 20 * N + 44 * V
     if stage == "render_bwd_design":
@@ -510,7 +510,7 @@ def roofline(prof, P, views, K, vis, batched):
     traffic, traffic_src = ncu_traffic(key, pairs)
     return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
-            "algorithmic_bytes_per_launch": ab, "bytes_formula": "survey 8(d) per view, summed over the views",
+            "algorithmic_bytes_per_launch": ab, "bytes_formula": "per view (render bwd: 40 K + 20 N + 44 V), summed over the views",
             "design_bytes_per_launch": db, "design_frac": db / (per_call_ms / 1000.0) / 1e9 / peak,
             "launch_ms": per_call_ms, "peak_source": f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured"
             else "fallback 6650 GB/s",
