@@ -64,8 +64,19 @@
 #define FMA(a, b, c) fmaf(a, b, c)
 #endif
 
+/* The reference's binning tile (config.h:16-17).  A build with other -DBLOCK_X /
+   -DBLOCK_Y serves the tile-shape study of tests/test_tile_shape_cpu.py only;
+   OGFS_LAMBDA_PIXELS is lambda_G's exponent (BLOCK_X*BLOCK_Y in the reference,
+   forward.cu:348), which that study keeps at 256 while the tile changes. */
+#ifndef BLOCK_X
 #define BLOCK_X 16
+#endif
+#ifndef BLOCK_Y
 #define BLOCK_Y 16
+#endif
+#ifndef OGFS_LAMBDA_PIXELS
+#define OGFS_LAMBDA_PIXELS (BLOCK_X * BLOCK_Y)
+#endif
 #define BLOCK_SIZE (BLOCK_X * BLOCK_Y)
 
 typedef REAL real;
@@ -322,10 +333,10 @@ void SFX(orc_preprocess)(const SFX(orc_pre_args) * a, int *radii, real *means2D,
     const int P = a->P;
     const real fy = a->H / (LIT(2.0) * a->tany), fx = a->W / (LIT(2.0) * a->tanx);
     const int gx = (a->W + BLOCK_X - 1) / BLOCK_X, gy = (a->H + BLOCK_Y - 1) / BLOCK_Y;
-    /* lambda_G (forward.cu:346-351); 256 = BLOCK_X*BLOCK_Y of the reference. */
+    /* lambda_G (forward.cu:346-351); OGFS_LAMBDA_PIXELS = 256 = BLOCK_X*BLOCK_Y of the reference. */
     const real eps_pix = LIT(1.0) / LIT(255.0);
     const real eps_base = FMAXR(LIT(0.0), LIT(1.0) - eps_pix);
-    const real lg_raw = LIT(1.0) - POWR(eps_base, (real)(BLOCK_X * BLOCK_Y));
+    const real lg_raw = LIT(1.0) - POWR(eps_base, (real)(OGFS_LAMBDA_PIXELS));
     real lg = eps_pix + a->eps_scale * (lg_raw - eps_pix);
     lg = FMINR(FMAXR(lg, eps_pix), a->eps_max);
     const real log_lg = LOGR(lg);

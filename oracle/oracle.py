@@ -34,6 +34,17 @@ def build(force=False):
         subprocess.check_call(cmd)
 
 
+def build_tile_variant(block_x, block_y, out_dir):
+    """FP32 oracle binning into block_x x block_y tiles, lambda_G's exponent kept at the reference's 256
+    (the tile-shape study; the reference itself bins into 16 x 16).  Returns the loaded library, to be
+    passed as `lib=` with `tile=(block_x, block_y)` to bin_pairs and as `lib=` to preprocess and render."""
+    out = os.path.join(out_dir, f"libfgs_oracle_f32_{block_x}x{block_y}.so")
+    subprocess.check_call(["gcc", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-shared", "-fPIC",
+                           "-o", out, SRC, "-lm", f"-DBLOCK_X={int(block_x)}", f"-DBLOCK_Y={int(block_y)}",
+                           "-DOGFS_LAMBDA_PIXELS=256"])
+    return C.CDLL(out)
+
+
 _libs = {}
 
 
@@ -109,8 +120,8 @@ class Scene:
         self.scale_modifier, self.use_filter, self.ogfs, self.filter3d = float(scale_modifier), bool(use_filter), ogfs, float(filter3d)
 
 
-def preprocess(sc, dtype=np.float32):
-    lib = _lib(dtype)
+def preprocess(sc, dtype=np.float32, lib=None):
+    lib = lib or _lib(dtype)
     f = getattr(lib, "orc_preprocess" + _sfx(dtype))
     P = int(np.asarray(sc.means3D).shape[0])
     A = {k: _arr(getattr(sc, k), dtype) for k in ("means3D", "scales", "rotations", "opacities", "shs",
@@ -153,11 +164,12 @@ def mark_visible(means, view, dtype=np.float32):
     return out.astype(bool)
 
 
-def bin_pairs(pre, W, H, dtype=np.float32):
-    """Duplicate + stable sort + tile ranges: (sorted keys u64, sorted values u32, ranges [T,2] u32)."""
-    lib = _lib(dtype)
+def bin_pairs(pre, W, H, dtype=np.float32, lib=None, tile=(16, 16)):
+    """Duplicate + stable sort + tile ranges: (sorted keys u64, sorted values u32, ranges [T,2] u32).
+    `tile` is the binning tile the library was built with (build_tile_variant)."""
+    lib = lib or _lib(dtype)
     K = int(pre["tiles_touched"].astype(np.int64).sum())
-    gx, gy = (W + 15) // 16, (H + 15) // 16
+    gx, gy = (W + tile[0] - 1) // tile[0], (H + tile[1] - 1) // tile[1]
     keys = np.zeros(max(K, 1), np.uint64)
     vals = np.zeros(max(K, 1), np.uint32)
     ranges = np.zeros((gx * gy, 2), np.uint32)
@@ -169,8 +181,8 @@ def bin_pairs(pre, W, H, dtype=np.float32):
     return keys[:K], vals[:K], ranges
 
 
-def render(sc, pre, vals, ranges, dtype=np.float32, stats=False, tile_range=(-1, -1)):
-    lib = _lib(dtype)
+def render(sc, pre, vals, ranges, dtype=np.float32, stats=False, tile_range=(-1, -1), lib=None):
+    lib = lib or _lib(dtype)
     W, H = sc.W, sc.H
     P = len(pre["radii"])
     feat = _arr(sc.colors_precomp, dtype) if sc.colors_precomp is not None else pre["rgb"]
