@@ -266,10 +266,10 @@ def kernel_source_digest():
     return h.hexdigest()[:12]
 
 
-def ncu_traffic(key, pairs):
-    """DRAM bytes of one launch of `key` from the committed ncu summary of the CURRENT render kernels:
-    per-pair traffic x pairs.  (None, reason) when the summary has no figure for this key or was captured
-    from other kernel sources than the ones built now."""
+def ncu_per_pair(field, key, pairs, what):
+    """`field`[key] per pair from the committed ncu summary of the CURRENT render kernels, times pairs.
+    (None, reason) when the summary has no figure for this key or was captured from other kernel sources
+    than the ones built now."""
     p = os.path.join(ROOT, "profiles", "render_traffic_urban1080.md")
     digest, per_pair = None, None
     try:
@@ -277,7 +277,7 @@ def ncu_traffic(key, pairs):
             for ln in f:
                 if ln.startswith("source_digest ="):
                     digest = ln.split("=")[1].strip()
-                if ln.startswith("traffic_per_pair[") and ln.split("[")[1].split("]")[0] == key:
+                if ln.startswith(field + "[") and ln.split("[")[1].split("]")[0] == key:
                     per_pair = float(ln.split("=")[1].strip().split()[0])
     except OSError:
         return None, "no ncu summary"
@@ -285,7 +285,33 @@ def ncu_traffic(key, pairs):
         return None, f"no ncu figure for {key}"
     if digest != kernel_source_digest():
         return None, "ncu summary is of other kernel sources"
-    return per_pair * pairs, f"ncu dram bytes per pair x pairs ({os.path.relpath(p, ROOT)})"
+    return per_pair * pairs, f"ncu {what} per pair x pairs ({os.path.relpath(p, ROOT)})"
+
+
+def ncu_traffic(key, pairs):
+    """DRAM bytes of one launch of `key`: the captured bytes per pair x pairs."""
+    return ncu_per_pair("traffic_per_pair", key, pairs, "dram bytes")
+
+
+# Warp instructions an SM can issue per cycle (four schedulers, one each), and the B200's maximum SM
+# clock: the issue roof of a kernel bound by instruction issue rather than by memory.
+ISSUE_PER_SM_CYCLE = 4
+SM_MAX_GHZ = 1.965
+
+
+def issue_roof(key, pairs, launch_ms):
+    """Warp instructions of one launch (captured per pair x pairs) / its duration, against the issue roof
+    of all SMs at the maximum clock; None when the ncu summary has no current figure for `key`."""
+    inst, src = ncu_per_pair("inst_per_pair", key, pairs, "warp instructions")
+    if inst is None:
+        return {"frac": None, "source": src}
+    n_sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count \
+        if torch.cuda.is_available() else 148
+    peak = n_sm * ISSUE_PER_SM_CYCLE * SM_MAX_GHZ  # G warp instructions / s
+    achieved = inst / (launch_ms / 1000.0) / 1e9
+    return {"warp_inst_per_launch": inst, "achieved": achieved, "peak": peak, "unit": "G warp inst/s",
+            "frac": achieved / peak, "sms": n_sm, "source": src,
+            "peak_source": f"{ISSUE_PER_SM_CYCLE} warp instructions per SM per cycle at {SM_MAX_GHZ * 1000:.0f} MHz"}
 
 
 def torch_cpu_baseline(sc, cam, threads):
@@ -508,6 +534,7 @@ def roofline(prof, P, views, K, vis, batched):
     peak, kind = measured_peak()
     achieved = ab / (per_call_ms / 1000.0) / 1e9
     traffic, traffic_src = ncu_traffic(key, pairs)
+    issue = issue_roof(key, pairs, per_call_ms)
     return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
             "algorithmic_bytes_per_launch": ab, "bytes_formula": "per view (render bwd: 40 K + 20 N + 44 V), summed over the views",
@@ -516,7 +543,9 @@ def roofline(prof, P, views, K, vis, batched):
             else "fallback 6650 GB/s",
             "timing": "CUDA events around each launch, eager pass of the same K steps" if batched
             else "CUDA events around each launch over the timed steps",
-            "note": "the compositing kernels are FP32/SFU issue-bound (exp per pixel-splat pair), not DRAM-bound"}
+            "issue": issue,
+            "note": "the compositing kernels are FP32/SFU issue-bound (exp per pixel-splat pair), not DRAM-bound: "
+                    "`issue` is the same launch against the instruction-issue roof"}
 
 
 def stages_of(prof):
